@@ -1,0 +1,31 @@
+"""ctypes signatures of every symbol include/gprtcu.h and include/gprt_compat.h declare."""
+import ctypes
+
+vp = ctypes.c_void_p
+u32 = ctypes.c_uint32
+u64 = ctypes.c_uint64
+i64 = ctypes.c_int64
+sz = ctypes.c_size_t
+i32 = ctypes.c_int
+st = ctypes.c_int  # gprtcuStatus
+
+SIGNATURES = {
+    "gprtcuStatusString": ([i32], ctypes.c_char_p),
+    "gprtcuVersion": ([], i32),
+    "gprtcuScratchStatus": ([vp, vp, ctypes.POINTER(i32)], st),
+    "gprtcuScanScratchSize": ([u64], sz),
+    "gprtcuExclusiveSumU32": ([vp, vp, u64, vp, vp, sz, vp], st),
+    "gprtcuInclusiveSumU32": ([vp, vp, u64, vp, vp, sz, vp], st),
+    "gprtcuPartitionI32": ([vp, vp, u64, i32, vp, vp, sz, vp], st),
+    "gprtcuSelectI32": ([vp, vp, u64, i32, vp, vp, sz, vp], st),
+    "gprtcuDebugSetSpinBudget": ([u32], None),
+    "gprtcuDebugScanSkipTile": ([i64], None),
+    "gprtcuDebugScanImpl": ([i32], None),
+}
+
+
+def declare(L):
+    for name, (args, res) in SIGNATURES.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res

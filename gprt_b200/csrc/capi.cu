@@ -1,0 +1,41 @@
+// capi.cu -- library-wide C entry points: status strings, version, and the
+// read-back of a scratch buffer's device-side status word.
+#include "common.cuh"
+
+using namespace gprtcu;
+
+extern "C" GPRTCU_API const char *gprtcuStatusString(int status) {
+  switch (status) {
+    case GPRTCU_OK: return "ok";
+    case GPRTCU_ERR_INVALID_ARG: return "invalid argument";
+    case GPRTCU_ERR_SIZE_MISMATCH: return "keys and values differ in size";
+    case GPRTCU_ERR_SCRATCH_TOO_SMALL: return "scratch buffer too small";
+    case GPRTCU_ERR_TIMEOUT: return "device-side wait exceeded its budget";
+    case GPRTCU_ERR_CUDA: return "CUDA runtime error";
+    case GPRTCU_ERR_TOO_LARGE: return "size beyond the supported maximum";
+    default: return "unknown status";
+  }
+}
+
+extern "C" GPRTCU_API int gprtcuVersion(void) { return 100; }
+
+extern "C" GPRTCU_API gprtcuStatus gprtcuScratchStatus(const void *scratch, gprtcuStream stream, int *deviceStatus) {
+  if (!scratch || !deviceStatus) return GPRTCU_ERR_INVALID_ARG;
+  uint32_t v = 0;
+  GPRTCU_TRY(cudaMemcpyAsync(&v, scratch, sizeof(v), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+  GPRTCU_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  *deviceStatus = (int)v;
+  return GPRTCU_OK;
+}
+
+int gprtcu_num_sms() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (cached[dev] == 0) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+    cached[dev] = v;
+  }
+  return cached[dev];
+}

@@ -1,0 +1,574 @@
+// scan.cu -- single-pass uint32 prefix sum with decoupled look-back.
+//
+// Replaces gprtBufferExclusiveSum (gprt/gprt_host.h:2246), whose host entry
+// is a stub in the reference (gprt/gprt.cpp:8739-8743) and whose intended
+// kernel is the chained scan of gprt/gprt_scan.slang:105-392.  Same single
+// pass structure (tile ticket, tile aggregate, look-back over predecessors,
+// inclusive publish), re-laid out for B200:
+//   * 8192 elements per 256-thread tile, each warp owning 1024 contiguous
+//     elements loaded as 8 coalesced 512-byte warp-wide 128-bit loads;
+//   * 64-bit status words {flag:32 | value:32}, so the aggregate is not
+//     capped at 2^30 as it is with the reference's 2-bit-flag packing
+//     (gprt/gprt_scan.slang:60-63, gprt/gprt_host.h:2231);
+//   * warp-wide look-back over 32 predecessors per probe, with a bounded
+//     wait that poisons the chain instead of hanging.
+// Traffic: 4 B read + 4 B written per element; HBM-bound.
+#include "common.cuh"
+
+namespace gprtcu {
+
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_VECS = 8;                                  // uint4 per thread
+constexpr int SCAN_WARP_ELEMS = SCAN_VECS * 4 * 32;           // 1024
+constexpr int SCAN_TILE = SCAN_WARP_ELEMS * (SCAN_THREADS / 32);  // 8192
+
+constexpr uint64_t ST_AGG = 1ull << 32;
+constexpr uint64_t ST_INC = 2ull << 32;
+constexpr uint64_t ST_POISON = 3ull << 32;
+
+// Warp 0 of tile `tile` (>= 1) sums the aggregates of its predecessors back to
+// the nearest inclusive prefix.  Returns false if the chain is poisoned or the
+// wait budget ran out.
+__device__ __forceinline__ bool scan_lookback(const uint64_t *status, uint64_t tile, int lane, uint32_t budget,
+                                              uint32_t &excl_out) {
+  uint32_t excl = 0;
+  int64_t base = (int64_t)tile - 1;
+  uint32_t spins = 0;
+  while (true) {
+    int64_t idx = base - lane;
+    uint64_t s = idx >= 0 ? ld_relaxed_u64(&status[idx]) : ST_INC;
+    // Wait only for the lanes up to the nearest inclusive (or poisoned)
+    // predecessor: the ones beyond it are not needed.
+    unsigned stopm;
+    while (true) {
+      unsigned ready = __ballot_sync(FULL_MASK, (s >> 32) != 0);
+      stopm = __ballot_sync(FULL_MASK, (s >> 32) >= 2);
+      unsigned need = stopm ? (2u << (__ffs(stopm) - 1)) - 1u : FULL_MASK;
+      if ((ready & need) == need) break;
+      if (++spins > budget) return false;
+      if ((s >> 32) == 0) s = ld_relaxed_u64(&status[idx]);
+    }
+    int stop = stopm ? __ffs(stopm) - 1 : 31;
+    uint32_t flag = (uint32_t)(s >> 32);
+    if (__shfl_sync(FULL_MASK, flag, stop) == 3) return false;
+    uint32_t v = lane <= stop ? (uint32_t)s : 0u;
+    excl += warp_sum(v);
+    if (stopm) break;
+    base -= 32;
+  }
+  excl_out = excl;
+  return true;
+}
+
+// MODE: 0 exclusive, 1 inclusive.  VEC: input/output 16-byte aligned.
+// NC: input does not alias output (read through the non-coherent path).
+template <int MODE, bool VEC, bool NC>
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_u32(const uint32_t *__restrict__ in, uint32_t *out, uint64_t n,
+                                                          uint64_t num_tiles, ScratchHeader *hdr, uint64_t *status,
+                                                          uint32_t *d_total, uint32_t budget, int64_t skip_tile) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_warp[SCAN_THREADS / 32];
+  __shared__ uint32_t s_prefix;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_tile = atomicAdd(&hdr->ticket[0], 1u);
+  __syncthreads();
+  const uint64_t tile = s_tile;
+  const uint64_t warp_start = tile * SCAN_TILE + (uint64_t)warp * SCAN_WARP_ELEMS;
+  const bool full = VEC && (tile + 1) * SCAN_TILE <= n;
+
+  uint4 v[SCAN_VECS];
+  if (full) {
+    const uint4 *src = reinterpret_cast<const uint4 *>(in + warp_start);
+#pragma unroll
+    for (int j = 0; j < SCAN_VECS; ++j) v[j] = NC ? ldg_stream(src + j * 32 + lane) : ldg_coherent(src + j * 32 + lane);
+  } else {
+#pragma unroll
+    for (int j = 0; j < SCAN_VECS; ++j) {
+      uint64_t e = warp_start + (uint64_t)(j * 32 + lane) * 4;
+      v[j].x = e + 0 < n ? in[e + 0] : 0u;
+      v[j].y = e + 1 < n ? in[e + 1] : 0u;
+      v[j].z = e + 2 < n ? in[e + 2] : 0u;
+      v[j].w = e + 3 < n ? in[e + 3] : 0u;
+    }
+  }
+
+  // Position order inside a warp is (j, lane, component): scan each 128-
+  // element row j across lanes and carry row totals forward.
+  uint32_t pre[SCAN_VECS];
+  uint32_t carry = 0;
+#pragma unroll
+  for (int j = 0; j < SCAN_VECS; ++j) {
+    uint32_t s = v[j].x + v[j].y + v[j].z + v[j].w;
+    uint32_t inc = warp_incl_scan(s, lane);
+    pre[j] = carry + inc - s;
+    carry += __shfl_sync(FULL_MASK, inc, 31);
+  }
+  if (lane == 0) s_warp[warp] = carry;
+  __syncthreads();
+
+  if (warp == 0) {
+    uint32_t wt = lane < SCAN_THREADS / 32 ? s_warp[lane] : 0u;
+    uint32_t wi = warp_incl_scan(wt, lane);
+    uint32_t agg = __shfl_sync(FULL_MASK, wi, SCAN_THREADS / 32 - 1);
+    if (lane < SCAN_THREADS / 32) s_warp[lane] = wi - wt;
+    uint32_t excl = 0;
+    bool ok = true;
+    if ((int64_t)tile == skip_tile) {
+      // Fault injection for tests: this tile never publishes.
+      ok = false;
+    } else if (tile == 0) {
+      if (lane == 0) st_relaxed_u64(&status[0], ST_INC | agg);
+    } else {
+      if (lane == 0) st_relaxed_u64(&status[tile], ST_AGG | agg);
+      ok = scan_lookback(status, tile, lane, budget, excl);
+      if (lane == 0) st_relaxed_u64(&status[tile], ok ? (ST_INC | (uint32_t)(excl + agg)) : ST_POISON);
+    }
+    if (!ok && lane == 0) record_error(hdr, GPRTCU_ERR_TIMEOUT);
+    if (lane == 0) {
+      s_prefix = excl;
+      if (tile == num_tiles - 1) {
+        hdr->total = excl + agg;
+        if (d_total) *d_total = excl + agg;
+      }
+    }
+  }
+  __syncthreads();
+
+  const uint32_t base = s_prefix + s_warp[warp];
+#pragma unroll
+  for (int j = 0; j < SCAN_VECS; ++j) {
+    uint32_t p = base + pre[j];
+    uint4 o;
+    if (MODE == 0) {
+      o.x = p;
+      o.y = o.x + v[j].x;
+      o.z = o.y + v[j].y;
+      o.w = o.z + v[j].z;
+    } else {
+      o.x = p + v[j].x;
+      o.y = o.x + v[j].y;
+      o.z = o.y + v[j].z;
+      o.w = o.z + v[j].w;
+    }
+    if (full) {
+      stg_v4(reinterpret_cast<uint4 *>(out + warp_start) + j * 32 + lane, o);
+    } else {
+      uint64_t e = warp_start + (uint64_t)(j * 32 + lane) * 4;
+      if (e + 0 < n) out[e + 0] = o.x;
+      if (e + 1 < n) out[e + 1] = o.y;
+      if (e + 2 < n) out[e + 2] = o.z;
+      if (e + 3 < n) out[e + 3] = o.w;
+    }
+  }
+}
+
+
+// Persistent, TMA-pipelined form of the same scan (16-byte aligned in/out).
+// Each CTA keeps PS_STAGES tiles in flight: thread 0 takes tile tickets ahead
+// and streams each full tile global->shared with one bulk async copy
+// (completion counted on a per-stage mbarrier); all warps scan the tile out
+// of shared memory, write the results back in place and thread 0 sends them
+// to global memory with one bulk async store.  Loads of the next tiles
+// therefore overlap the current tile's look-back and store.
+// Forward progress: a CTA processes its tickets in increasing order and a
+// tile waits only on smaller tickets, so the smallest unfinished ticket can
+// always proceed.
+constexpr int PS_STAGES = 3;
+constexpr int PS_TILE_BYTES = SCAN_TILE * 4;
+constexpr size_t PS_SMEM = (size_t)PS_STAGES * PS_TILE_BYTES + PS_STAGES * 8 + PS_STAGES * 4;
+
+template <int MODE>
+__global__ void __launch_bounds__(SCAN_THREADS, 2)
+    k_scan_pipe(const uint32_t *__restrict__ in, uint32_t *out, uint64_t n, uint64_t num_tiles, ScratchHeader *hdr,
+                uint64_t *status, uint32_t *d_total, uint32_t budget, int64_t skip_tile) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint4 *buf = reinterpret_cast<uint4 *>(smem);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (size_t)PS_STAGES * PS_TILE_BYTES);
+  uint32_t *stage_tile = reinterpret_cast<uint32_t *>(bars + PS_STAGES);
+  __shared__ uint32_t s_warp[SCAN_THREADS / 32];
+  __shared__ uint32_t s_prefix;
+  __shared__ uint32_t s_abort;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  auto issue = [&](int s) {  // thread 0 only
+    uint32_t t = atomicAdd(&hdr->ticket[0], 1u);
+    stage_tile[s] = t;
+    uint64_t start = (uint64_t)t * SCAN_TILE;
+    if (t < num_tiles && start + SCAN_TILE <= n) {
+      mbar_arrive_expect_tx(&bars[s], PS_TILE_BYTES);
+      bulk_g2s(buf + (size_t)s * (SCAN_TILE / 4), in + start, PS_TILE_BYTES, &bars[s]);
+    } else {
+      mbar_arrive(&bars[s]);  // past the end, or the ragged last tile (loaded directly)
+    }
+  };
+
+  if (tid == 0) {
+    for (int s = 0; s < PS_STAGES; ++s) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+    s_abort = 0;
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int s = 0; s < PS_STAGES; ++s) issue(s);
+
+  for (uint32_t k = 0;; ++k) {
+    const int s = k % PS_STAGES;
+    if (!mbar_wait(&bars[s], (k / PS_STAGES) & 1u, MBAR_WAIT_BUDGET)) s_abort = 1;
+    __syncthreads();
+    if (s_abort) {
+      if (tid == 0) record_error(hdr, GPRTCU_ERR_TIMEOUT);
+      break;
+    }
+    const uint32_t tile = stage_tile[s];
+    if (tile >= num_tiles) break;
+    const uint64_t tile_start = (uint64_t)tile * SCAN_TILE;
+    const uint64_t warp_start = tile_start + (uint64_t)warp * SCAN_WARP_ELEMS;
+    const bool full = tile_start + SCAN_TILE <= n;
+    uint4 *sb = buf + (size_t)s * (SCAN_TILE / 4) + warp * (SCAN_WARP_ELEMS / 4);
+
+    uint4 v[SCAN_VECS];
+    if (full) {
+#pragma unroll
+      for (int j = 0; j < SCAN_VECS; ++j) v[j] = sb[j * 32 + lane];
+    } else {
+#pragma unroll
+      for (int j = 0; j < SCAN_VECS; ++j) {
+        uint64_t e = warp_start + (uint64_t)(j * 32 + lane) * 4;
+        v[j].x = e + 0 < n ? in[e + 0] : 0u;
+        v[j].y = e + 1 < n ? in[e + 1] : 0u;
+        v[j].z = e + 2 < n ? in[e + 2] : 0u;
+        v[j].w = e + 3 < n ? in[e + 3] : 0u;
+      }
+    }
+    uint32_t pre[SCAN_VECS];
+    uint32_t carry = 0;
+#pragma unroll
+    for (int j = 0; j < SCAN_VECS; ++j) {
+      uint32_t sum = v[j].x + v[j].y + v[j].z + v[j].w;
+      uint32_t inc = warp_incl_scan(sum, lane);
+      pre[j] = carry + inc - sum;
+      carry += __shfl_sync(FULL_MASK, inc, 31);
+    }
+    if (lane == 0) s_warp[warp] = carry;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t wt = lane < SCAN_THREADS / 32 ? s_warp[lane] : 0u;
+      uint32_t wi = warp_incl_scan(wt, lane);
+      uint32_t agg = __shfl_sync(FULL_MASK, wi, SCAN_THREADS / 32 - 1);
+      if (lane < SCAN_THREADS / 32) s_warp[lane] = wi - wt;
+      uint32_t excl = 0;
+      bool ok = true;
+      if ((int64_t)tile == skip_tile) {
+        ok = false;  // fault injection: this tile never publishes
+      } else if (tile == 0) {
+        if (lane == 0) st_relaxed_u64(&status[0], ST_INC | agg);
+      } else {
+        if (lane == 0) st_relaxed_u64(&status[tile], ST_AGG | agg);
+        ok = scan_lookback(status, tile, lane, budget, excl);
+        if (lane == 0) st_relaxed_u64(&status[tile], ok ? (ST_INC | (uint32_t)(excl + agg)) : ST_POISON);
+      }
+      if (!ok && lane == 0) record_error(hdr, GPRTCU_ERR_TIMEOUT);
+      if (lane == 0) {
+        s_prefix = excl;
+        if (tile == num_tiles - 1) {
+          hdr->total = excl + agg;
+          if (d_total) *d_total = excl + agg;
+        }
+      }
+    }
+    __syncthreads();
+    const uint32_t base = s_prefix + s_warp[warp];
+#pragma unroll
+    for (int j = 0; j < SCAN_VECS; ++j) {
+      uint32_t p = base + pre[j];
+      uint4 o;
+      if (MODE == 0) {
+        o.x = p;
+        o.y = o.x + v[j].x;
+        o.z = o.y + v[j].y;
+        o.w = o.z + v[j].z;
+      } else {
+        o.x = p + v[j].x;
+        o.y = o.x + v[j].y;
+        o.z = o.y + v[j].z;
+        o.w = o.z + v[j].w;
+      }
+      if (full) {
+        sb[j * 32 + lane] = o;
+      } else {
+        uint64_t e = warp_start + (uint64_t)(j * 32 + lane) * 4;
+        if (e + 0 < n) out[e + 0] = o.x;
+        if (e + 1 < n) out[e + 1] = o.y;
+        if (e + 2 < n) out[e + 2] = o.z;
+        if (e + 3 < n) out[e + 3] = o.w;
+      }
+    }
+    if (full) fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      if (full) bulk_s2g(out + tile_start, buf + (size_t)s * (SCAN_TILE / 4), PS_TILE_BYTES);
+      bulk_commit();
+      // The stage used one iteration ago is free once its store has read it.
+      if (k > 0) {
+        bulk_wait_read<1>();
+        issue((k + PS_STAGES - 1) % PS_STAGES);
+      }
+    }
+  }
+  if (tid == 0) bulk_wait<0>();
+}
+
+// Partition / select by sign (gprt/gprt_scan.slang:118-133,270-283;
+// known-answer layout tests/t03-bufferScans/hostCode.cpp:98-160,172-241).
+// The scan runs over the 0/1 selection flags; each tile then stages its
+// selected items (in order) at the bottom of a shared buffer and, for a
+// partition, its unselected items (in reverse order) at the top, so both
+// groups leave the tile as contiguous, coalesced runs:
+//   selected   : out[excl + k]
+//   unselected : out[(n-1) - (tile_start - excl) - k']   (reverse order)
+template <bool PARTITION, bool VEC>
+__global__ void __launch_bounds__(SCAN_THREADS) k_partition_i32(const int32_t *__restrict__ in, int32_t *__restrict__ out,
+                                                               uint64_t n, uint64_t num_tiles, int select_positive,
+                                                               ScratchHeader *hdr, uint64_t *status, uint32_t *d_count,
+                                                               uint32_t budget) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_warp[SCAN_THREADS / 32];
+  __shared__ uint32_t s_prefix, s_tile_sel;
+  __shared__ int32_t s_buf[SCAN_TILE];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_tile = atomicAdd(&hdr->ticket[0], 1u);
+  __syncthreads();
+  const uint64_t tile = s_tile;
+  const uint64_t tile_start = tile * SCAN_TILE;
+  const uint64_t warp_start = tile_start + (uint64_t)warp * SCAN_WARP_ELEMS;
+  const bool full = VEC && (tile + 1) * SCAN_TILE <= n;
+  const uint32_t tile_count = (uint32_t)min((uint64_t)SCAN_TILE, n - tile_start);
+  const uint32_t want_neg = select_positive ? 0u : 1u;
+
+  int4 v[SCAN_VECS];
+  uint32_t fl[SCAN_VECS];  // 4 flag bits per vector, bit c = component c selected
+  if (full) {
+    const uint4 *src = reinterpret_cast<const uint4 *>(in + warp_start);
+#pragma unroll
+    for (int j = 0; j < SCAN_VECS; ++j) {
+      uint4 u = ldg_stream(src + j * 32 + lane);
+      v[j] = make_int4((int)u.x, (int)u.y, (int)u.z, (int)u.w);
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < SCAN_VECS; ++j) {
+      uint64_t e = warp_start + (uint64_t)(j * 32 + lane) * 4;
+      v[j].x = e + 0 < n ? in[e + 0] : 0;
+      v[j].y = e + 1 < n ? in[e + 1] : 0;
+      v[j].z = e + 2 < n ? in[e + 2] : 0;
+      v[j].w = e + 3 < n ? in[e + 3] : 0;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < SCAN_VECS; ++j) {
+    uint64_t e = warp_start + (uint64_t)(j * 32 + lane) * 4;
+    uint32_t f = 0;
+    f |= ((((uint32_t)v[j].x >> 31) == want_neg) && e + 0 < n) ? 1u : 0u;
+    f |= ((((uint32_t)v[j].y >> 31) == want_neg) && e + 1 < n) ? 2u : 0u;
+    f |= ((((uint32_t)v[j].z >> 31) == want_neg) && e + 2 < n) ? 4u : 0u;
+    f |= ((((uint32_t)v[j].w >> 31) == want_neg) && e + 3 < n) ? 8u : 0u;
+    fl[j] = f;
+  }
+  uint32_t pre[SCAN_VECS];
+  uint32_t carry = 0;
+#pragma unroll
+  for (int j = 0; j < SCAN_VECS; ++j) {
+    uint32_t s = __popc(fl[j]);
+    uint32_t inc = warp_incl_scan(s, lane);
+    pre[j] = carry + inc - s;
+    carry += __shfl_sync(FULL_MASK, inc, 31);
+  }
+  if (lane == 0) s_warp[warp] = carry;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t wt = lane < SCAN_THREADS / 32 ? s_warp[lane] : 0u;
+    uint32_t wi = warp_incl_scan(wt, lane);
+    uint32_t agg = __shfl_sync(FULL_MASK, wi, SCAN_THREADS / 32 - 1);
+    if (lane < SCAN_THREADS / 32) s_warp[lane] = wi - wt;
+    uint32_t excl = 0;
+    bool ok = true;
+    if (tile == 0) {
+      if (lane == 0) st_relaxed_u64(&status[0], ST_INC | agg);
+    } else {
+      if (lane == 0) st_relaxed_u64(&status[tile], ST_AGG | agg);
+      ok = scan_lookback(status, tile, lane, budget, excl);
+      if (lane == 0) st_relaxed_u64(&status[tile], ok ? (ST_INC | (uint32_t)(excl + agg)) : ST_POISON);
+    }
+    if (!ok && lane == 0) record_error(hdr, GPRTCU_ERR_TIMEOUT);
+    if (lane == 0) {
+      s_prefix = excl;
+      s_tile_sel = agg;
+      if (tile == num_tiles - 1) {
+        hdr->total = excl + agg;
+        if (d_count) *d_count = excl + agg;
+      }
+    }
+  }
+  __syncthreads();
+  // Stage: selected at local rank ls, unselected at SCAN_TILE-1-lu.
+  const uint32_t wbase = s_warp[warp];
+#pragma unroll
+  for (int j = 0; j < SCAN_VECS; ++j) {
+    uint32_t local0 = (uint32_t)(warp * SCAN_WARP_ELEMS + (j * 32 + lane) * 4);
+    uint32_t ls = wbase + pre[j];
+    int32_t vals[4] = {v[j].x, v[j].y, v[j].z, v[j].w};
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      uint32_t local = local0 + c;
+      if (local >= tile_count) continue;
+      if (fl[j] & (1u << c)) {
+        s_buf[ls] = vals[c];
+        ++ls;
+      } else if (PARTITION) {
+        uint32_t lu = local - ls;
+        s_buf[SCAN_TILE - 1 - lu] = vals[c];
+      }
+    }
+  }
+  __syncthreads();
+  const uint32_t tsel = s_tile_sel, excl = s_prefix;
+  for (uint32_t p = tid; p < tsel; p += SCAN_THREADS) out[(uint64_t)excl + p] = s_buf[p];
+  if (PARTITION) {
+    const uint32_t tunsel = tile_count - tsel;
+    // element at staging slot p has local unselected rank lu = SCAN_TILE-1-p
+    const uint64_t top = (n - 1) - (tile_start - excl);
+    for (uint32_t q = tid; q < tunsel; q += SCAN_THREADS) {
+      uint32_t p = SCAN_TILE - tunsel + q;
+      out[top - (SCAN_TILE - 1 - p)] = s_buf[p];
+    }
+  }
+}
+
+}  // namespace gprtcu
+
+using namespace gprtcu;
+
+static uint32_t g_spin_budget = DEFAULT_SPIN_BUDGET;
+static int64_t g_skip_tile = -1;
+// 0: persistent TMA-pipelined scan when aligned; 1: one-tile-per-CTA scan.
+static int g_scan_impl = 0;
+extern "C" GPRTCU_API void gprtcuDebugScanImpl(int impl) { g_scan_impl = impl; }
+
+extern "C" GPRTCU_API void gprtcuDebugSetSpinBudget(uint32_t polls) { g_spin_budget = polls ? polls : DEFAULT_SPIN_BUDGET; }
+extern "C" GPRTCU_API void gprtcuDebugScanSkipTile(int64_t tile) { g_skip_tile = tile; }
+uint32_t gprtcu_spin_budget(void) { return g_spin_budget; }
+
+static const uint64_t kScanMaxN = 1ull << 40;
+
+extern "C" GPRTCU_API size_t gprtcuScanScratchSize(uint64_t n) {
+  uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+  return sizeof(ScratchHeader) + gprtcu_align256(tiles * sizeof(uint64_t));
+}
+
+static gprtcuStatus scan_launch(const uint32_t *in, uint32_t *out, uint64_t n, int inclusive, uint32_t *d_total,
+                                void *scratch, size_t scratch_bytes, cudaStream_t stream) {
+  if (n > kScanMaxN) return GPRTCU_ERR_TOO_LARGE;
+  if (n > 0 && (!in || !out)) return GPRTCU_ERR_INVALID_ARG;
+  if (!scratch) return GPRTCU_ERR_INVALID_ARG;
+  if (((uintptr_t)scratch & 255) != 0) return GPRTCU_ERR_INVALID_ARG;
+  size_t need = gprtcuScanScratchSize(n);
+  if (scratch_bytes < need) return GPRTCU_ERR_SCRATCH_TOO_SMALL;
+  ScratchHeader *hdr = (ScratchHeader *)scratch;
+  uint64_t *status = (uint64_t *)((char *)scratch + sizeof(ScratchHeader));
+  uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+  GPRTCU_TRY(cudaMemsetAsync(scratch, 0, sizeof(ScratchHeader) + tiles * sizeof(uint64_t), stream));
+  if (n == 0) {
+    if (d_total) GPRTCU_TRY(cudaMemsetAsync(d_total, 0, sizeof(uint32_t), stream));
+    return GPRTCU_OK;
+  }
+  const bool vec = (((uintptr_t)in | (uintptr_t)out) & 15) == 0;
+  const bool nc = (const void *)in != (const void *)out;
+  if (vec && g_scan_impl == 0) {
+    // Persistent, TMA-pipelined kernel: as many CTAs as are co-resident.
+    static bool attr_set = false;
+    if (!attr_set) {
+      GPRTCU_TRY(cudaFuncSetAttribute(k_scan_pipe<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PS_SMEM));
+      GPRTCU_TRY(cudaFuncSetAttribute(k_scan_pipe<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PS_SMEM));
+      attr_set = true;
+    }
+    int per_sm = 0;
+    GPRTCU_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scan_pipe<0>, SCAN_THREADS, PS_SMEM));
+    uint64_t ctas = (uint64_t)gprtcu_num_sms() * (uint64_t)(per_sm > 0 ? per_sm : 1);
+    if (ctas > tiles) ctas = tiles;
+    if (inclusive)
+      k_scan_pipe<1><<<(unsigned)ctas, SCAN_THREADS, PS_SMEM, stream>>>(in, out, n, tiles, hdr, status, d_total,
+                                                                         g_spin_budget, g_skip_tile);
+    else
+      k_scan_pipe<0><<<(unsigned)ctas, SCAN_THREADS, PS_SMEM, stream>>>(in, out, n, tiles, hdr, status, d_total,
+                                                                         g_spin_budget, g_skip_tile);
+    GPRTCU_TRY(cudaGetLastError());
+    return GPRTCU_OK;
+  }
+  dim3 grid((unsigned)tiles), block(SCAN_THREADS);
+#define GPRTCU_SCAN_LAUNCH(M, V, N) \
+  k_scan_u32<M, V, N><<<grid, block, 0, stream>>>(in, out, n, tiles, hdr, status, d_total, g_spin_budget, g_skip_tile)
+  if (inclusive) {
+    if (vec && nc) GPRTCU_SCAN_LAUNCH(1, true, true);
+    else if (vec) GPRTCU_SCAN_LAUNCH(1, true, false);
+    else GPRTCU_SCAN_LAUNCH(1, false, false);
+  } else {
+    if (vec && nc) GPRTCU_SCAN_LAUNCH(0, true, true);
+    else if (vec) GPRTCU_SCAN_LAUNCH(0, true, false);
+    else GPRTCU_SCAN_LAUNCH(0, false, false);
+  }
+#undef GPRTCU_SCAN_LAUNCH
+  GPRTCU_TRY(cudaGetLastError());
+  return GPRTCU_OK;
+}
+
+extern "C" GPRTCU_API gprtcuStatus gprtcuExclusiveSumU32(const uint32_t *in, uint32_t *out, uint64_t n,
+                                                         uint32_t *d_total, void *scratch, size_t scratchBytes,
+                                                         gprtcuStream stream) {
+  return scan_launch(in, out, n, 0, d_total, scratch, scratchBytes, (cudaStream_t)stream);
+}
+
+extern "C" GPRTCU_API gprtcuStatus gprtcuInclusiveSumU32(const uint32_t *in, uint32_t *out, uint64_t n,
+                                                         uint32_t *d_total, void *scratch, size_t scratchBytes,
+                                                         gprtcuStream stream) {
+  return scan_launch(in, out, n, 1, d_total, scratch, scratchBytes, (cudaStream_t)stream);
+}
+
+static gprtcuStatus partition_launch(const int32_t *in, int32_t *out, uint64_t n, int select_positive, int partition,
+                                     uint32_t *d_count, void *scratch, size_t scratch_bytes, cudaStream_t stream) {
+  if (n > 0xFFFFFFFFull) return GPRTCU_ERR_TOO_LARGE;  // the count is a uint32, as in the reference
+  if (n > 0 && (!in || !out)) return GPRTCU_ERR_INVALID_ARG;
+  if (n > 0 && (const void *)in == (const void *)out) return GPRTCU_ERR_INVALID_ARG;
+  if (!scratch || ((uintptr_t)scratch & 255) != 0) return GPRTCU_ERR_INVALID_ARG;
+  if (scratch_bytes < gprtcuScanScratchSize(n)) return GPRTCU_ERR_SCRATCH_TOO_SMALL;
+  ScratchHeader *hdr = (ScratchHeader *)scratch;
+  uint64_t *status = (uint64_t *)((char *)scratch + sizeof(ScratchHeader));
+  uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+  GPRTCU_TRY(cudaMemsetAsync(scratch, 0, sizeof(ScratchHeader) + tiles * sizeof(uint64_t), stream));
+  if (n == 0) {
+    if (d_count) GPRTCU_TRY(cudaMemsetAsync(d_count, 0, sizeof(uint32_t), stream));
+    return GPRTCU_OK;
+  }
+  const bool vec = ((uintptr_t)in & 15) == 0;
+  dim3 grid((unsigned)tiles), block(SCAN_THREADS);
+  if (partition) {
+    if (vec) k_partition_i32<true, true><<<grid, block, 0, stream>>>(in, out, n, tiles, select_positive, hdr, status, d_count, g_spin_budget);
+    else k_partition_i32<true, false><<<grid, block, 0, stream>>>(in, out, n, tiles, select_positive, hdr, status, d_count, g_spin_budget);
+  } else {
+    if (vec) k_partition_i32<false, true><<<grid, block, 0, stream>>>(in, out, n, tiles, select_positive, hdr, status, d_count, g_spin_budget);
+    else k_partition_i32<false, false><<<grid, block, 0, stream>>>(in, out, n, tiles, select_positive, hdr, status, d_count, g_spin_budget);
+  }
+  GPRTCU_TRY(cudaGetLastError());
+  return GPRTCU_OK;
+}
+
+extern "C" GPRTCU_API gprtcuStatus gprtcuPartitionI32(const int32_t *in, int32_t *out, uint64_t n, int selectPositive,
+                                                      uint32_t *d_count, void *scratch, size_t scratchBytes,
+                                                      gprtcuStream stream) {
+  return partition_launch(in, out, n, selectPositive, 1, d_count, scratch, scratchBytes, (cudaStream_t)stream);
+}
+
+extern "C" GPRTCU_API gprtcuStatus gprtcuSelectI32(const int32_t *in, int32_t *out, uint64_t n, int selectPositive,
+                                                   uint32_t *d_count, void *scratch, size_t scratchBytes,
+                                                   gprtcuStream stream) {
+  return partition_launch(in, out, n, selectPositive, 0, d_count, scratch, scratchBytes, (cudaStream_t)stream);
+}

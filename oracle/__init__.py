@@ -1,0 +1,214 @@
+"""ctypes bindings for the CPU oracle (oracle/oracle.cpp) and, when built,
+the reference-compiled checker (oracle/_ref/libgprtref.so).
+
+TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg (and its reference arm) may import this package.  The product
+(gprt_b200) never imports it, and nothing here is a fallback for the CUDA path.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libgprtref.so")
+
+_lib = None
+_ref = None
+
+HIT_DTYPE = np.dtype([("prim", np.uint32), ("t", np.float32)])
+
+
+def build(ref=None):
+    """Compile the oracle (and the reference checker when the reference sources exist)."""
+    subprocess.check_call(["make", "-s", "-C", HERE])
+    if ref is None:
+        ref = os.path.isdir("/root/reference/gprt")
+    if ref:
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build(ref=False)
+        L = ctypes.CDLL(LIB_PATH)
+        vp, u32, u64, sz, i32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_size_t, ctypes.c_int
+        L.orc_sort.argtypes = [vp, i32, vp, i32, sz]
+        L.orc_scan_u32.argtypes = [vp, vp, sz, i32]
+        L.orc_scan_u32.restype = u32
+        L.orc_partition_i32.argtypes = [vp, vp, sz, i32, i32]
+        L.orc_partition_i32.restype = u32
+        L.orc_morton3d.argtypes = [u32, u32, u32]
+        L.orc_morton3d.restype = u32
+        L.orc_hilbert3d.argtypes = [u32, u32, u32]
+        L.orc_hilbert3d.restype = u32
+        L.orc_tri_bounds.argtypes = [vp, vp, u32, vp]
+        L.orc_tri_codes.argtypes = [vp, vp, u32, vp, i32, vp, vp]
+        L.orc_point_bounds.argtypes = [vp, u32, vp]
+        L.orc_point_codes.argtypes = [vp, u32, vp, i32, vp, vp]
+        L.orc_karras.argtypes = [vp, u32, vp]
+        L.orc_refit_tri.argtypes = [vp, vp, vp, u32, vp, vp]
+        L.orc_lbvh_build_tri.argtypes = [vp, vp, u32, i32, vp, vp, vp, vp, vp]
+        L.orc_lbvh_build_points.argtypes = [vp, u32, i32, vp, vp, vp, vp, vp]
+        L.orc_isect_tri32.argtypes = [vp, vp, vp, vp, vp]
+        L.orc_isect_tri32.restype = i32
+        L.orc_refine_t32.argtypes = [vp, vp, vp, vp]
+        L.orc_refine_t32.restype = ctypes.c_float
+        L.orc_t64.argtypes = [vp, vp, vp, vp]
+        L.orc_t64.restype = ctypes.c_double
+        L.orc_trace_brute.argtypes = [vp, vp, u32, vp, u64, vp]
+        L.orc_trace_lbvh.argtypes = [vp, vp, u32, vp, vp, vp, u64, i32, vp]
+        L.orc_num_threads.restype = i32
+        _lib = L
+    return _lib
+
+
+def ref_available():
+    return os.path.exists(REF_PATH)
+
+
+def ref():
+    """The reference's own LBVH programs and Hilbert encoder, compiled from its sources."""
+    global _ref
+    if _ref is None:
+        R = ctypes.CDLL(REF_PATH)
+        vp, u32, i32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int
+        R.ref_lbvh_build.argtypes = [i32, vp, u32, vp, u32, vp, vp, vp, vp, vp]
+        R.ref_hilbert3d.argtypes = [u32, u32, u32]
+        R.ref_hilbert3d.restype = u32
+        _ref = R
+    return _ref
+
+
+# ----------------------------------------------------------------------------
+# numpy-level helpers
+# ----------------------------------------------------------------------------
+def sort(keys, vals=None):
+    """Stable ascending sort; returns new arrays."""
+    k = np.ascontiguousarray(keys).copy()
+    v = None if vals is None else np.ascontiguousarray(vals).copy()
+    lib().orc_sort(_p(k), k.itemsize, _p(v), 0 if v is None else v.itemsize, k.size)
+    return k if v is None else (k, v)
+
+
+def scan(x, inclusive=False):
+    x = np.ascontiguousarray(x, dtype=np.uint32)
+    out = np.empty_like(x)
+    total = lib().orc_scan_u32(_p(x), _p(out), x.size, 1 if inclusive else 0)
+    return out, int(total)
+
+
+def partition(x, select_positive=True, partition=True):
+    x = np.ascontiguousarray(x, dtype=np.int32)
+    out = np.zeros_like(x)
+    total = lib().orc_partition_i32(_p(x), _p(out), x.size, 1 if select_positive else 0, 1 if partition else 0)
+    return out, int(total)
+
+
+def morton3d(x, y, z):
+    return lib().orc_morton3d(int(x), int(y), int(z))
+
+
+def hilbert3d(x, y, z):
+    return lib().orc_hilbert3d(int(x), int(y), int(z))
+
+
+def lbvh_build_tri(pos, tri, kind=0):
+    """Full CPU LBVH build.  Returns dict(scene, codes, ids, nodes, aabbs)."""
+    pos = np.ascontiguousarray(pos, dtype=np.float32)
+    tri = np.ascontiguousarray(tri, dtype=np.uint32)
+    n = tri.shape[0]
+    scene = np.zeros(6, np.float32)
+    codes = np.zeros(n, np.uint32)
+    ids = np.zeros(n, np.uint32)
+    nn = max(2 * n - 1, 0)
+    nodes = np.full((nn, 4), -1, np.int32)
+    aabbs = np.zeros((nn, 6), np.float32)
+    lib().orc_lbvh_build_tri(_p(pos), _p(tri), n, kind, _p(scene), _p(codes), _p(ids), _p(nodes), _p(aabbs))
+    return dict(scene=scene, codes=codes, ids=ids, nodes=nodes, aabbs=aabbs)
+
+
+def lbvh_build_points(pos, kind=0):
+    pos = np.ascontiguousarray(pos, dtype=np.float32)
+    n = pos.shape[0]
+    scene = np.zeros(6, np.float32)
+    codes = np.zeros(n, np.uint32)
+    ids = np.zeros(n, np.uint32)
+    nn = max(2 * n - 1, 0)
+    nodes = np.full((nn, 4), -1, np.int32)
+    aabbs = np.zeros((nn, 6), np.float32)
+    lib().orc_lbvh_build_points(_p(pos), n, kind, _p(scene), _p(codes), _p(ids), _p(nodes), _p(aabbs))
+    return dict(scene=scene, codes=codes, ids=ids, nodes=nodes, aabbs=aabbs)
+
+
+def karras(codes):
+    codes = np.ascontiguousarray(codes, dtype=np.uint32)
+    n = codes.size
+    nodes = np.full((max(2 * n - 1, 0), 4), -1, np.int32)
+    lib().orc_karras(_p(codes), n, _p(nodes))
+    return nodes
+
+
+def ref_lbvh_build(pos, tri=None):
+    """The reference's programs run serially (kind: triangles if tri given, else points)."""
+    pos = np.ascontiguousarray(pos, dtype=np.float32)
+    if tri is not None:
+        tri = np.ascontiguousarray(tri, dtype=np.uint32)
+        n = tri.shape[0]
+        kind = 0
+    else:
+        n = pos.shape[0]
+        kind = 1
+    scene = np.zeros(6, np.float32)
+    codes = np.zeros(n, np.uint32)
+    ids = np.zeros(n, np.uint32)
+    nodes = np.full((2 * n - 1, 4), -1, np.int32)
+    aabbs = np.zeros((2 * n - 1, 6), np.float32)
+    ref().ref_lbvh_build(kind, _p(pos), pos.shape[0], _p(tri), n, _p(scene), _p(codes), _p(ids), _p(nodes),
+                         _p(aabbs))
+    return dict(scene=scene, codes=codes, ids=ids, nodes=nodes, aabbs=aabbs)
+
+
+def trace_brute(pos, tri, rays):
+    pos = np.ascontiguousarray(pos, dtype=np.float32)
+    tri = np.ascontiguousarray(tri, dtype=np.uint32)
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    hits = np.zeros(rays.shape[0], HIT_DTYPE)
+    lib().orc_trace_brute(_p(pos), _p(tri), tri.shape[0], _p(rays), rays.shape[0], _p(hits))
+    return hits
+
+
+def trace_lbvh(pos, tri, bvh, rays, anyhit=False):
+    pos = np.ascontiguousarray(pos, dtype=np.float32)
+    tri = np.ascontiguousarray(tri, dtype=np.uint32)
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    nodes = np.ascontiguousarray(bvh["nodes"], dtype=np.int32)
+    aabbs = np.ascontiguousarray(bvh["aabbs"], dtype=np.float32)
+    hits = np.zeros(rays.shape[0], HIT_DTYPE)
+    lib().orc_trace_lbvh(_p(pos), _p(tri), tri.shape[0], _p(nodes), _p(aabbs), _p(rays), rays.shape[0],
+                         1 if anyhit else 0, _p(hits))
+    return hits
+
+
+def t64(ray, v0, v1, v2):
+    a = [np.ascontiguousarray(v, dtype=np.float32) for v in (ray, v0, v1, v2)]
+    return lib().orc_t64(*[_p(v) for v in a])
+
+
+def isect32(ray, v0, v1, v2):
+    a = [np.ascontiguousarray(v, dtype=np.float32) for v in (ray, v0, v1, v2)]
+    t = np.zeros(1, np.float32)
+    hit = lib().orc_isect_tri32(*[_p(v) for v in a], _p(t))
+    return bool(hit), float(t[0])
+
+
+def num_threads():
+    return lib().orc_num_threads()

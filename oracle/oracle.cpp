@@ -1,0 +1,612 @@
+// oracle.cpp -- CPU restatement of GPRT's acceleration-structure path.
+//
+// TEST INFRASTRUCTURE ONLY: the parity tests, the smoke check and the bench's
+// CPU-baseline leg use this library as the checker.  The product library never
+// links, loads or calls it.  Build: oracle/Makefile (g++ -O2 -fopenmp
+// -ffp-contract=off; the ray math relies on every float operation being a
+// separately rounded IEEE operation, exactly as the CUDA kernels issue them).
+//
+// Parity pins are listed per function in oracle.h.
+#include "oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+// ============================================================================
+// sort
+// ============================================================================
+// gprtBufferSort / gprtBufferSortPayload (gprt/gprt.cpp:8821-9073) run a stable
+// least-significant-digit radix sort in place; every pass is a stable split by
+// one digit (gprt/gprt_sort.slang:353-489).  The net effect is a stable
+// ascending sort, which is what the reference test checks with std::sort
+// (tests/t02-bufferSort/hostCode.cpp:59,115).  Restated as std::stable_sort of
+// (key, original position) so payload order within equal keys is preserved.
+template <typename K, typename V>
+static void sort_kv(K *keys, V *vals, size_t n) {
+  std::vector<std::pair<K, V>> kv(n);
+  for (size_t i = 0; i < n; ++i) kv[i] = {keys[i], vals[i]};
+  std::stable_sort(kv.begin(), kv.end(), [](const std::pair<K, V> &a, const std::pair<K, V> &b) {
+    return a.first < b.first;
+  });
+  for (size_t i = 0; i < n; ++i) {
+    keys[i] = kv[i].first;
+    vals[i] = kv[i].second;
+  }
+}
+
+extern "C" void orc_sort(void *keys, int kw, void *vals, int vw, size_t n) {
+  if (n == 0) return;
+  if (vw == 0 || vals == nullptr) {
+    if (kw == 4) std::sort((uint32_t *)keys, (uint32_t *)keys + n);
+    else std::sort((uint64_t *)keys, (uint64_t *)keys + n);
+    return;
+  }
+  if (kw == 4 && vw == 4) sort_kv((uint32_t *)keys, (uint32_t *)vals, n);
+  else if (kw == 4 && vw == 8) sort_kv((uint32_t *)keys, (uint64_t *)vals, n);
+  else if (kw == 8 && vw == 4) sort_kv((uint64_t *)keys, (uint32_t *)vals, n);
+  else sort_kv((uint64_t *)keys, (uint64_t *)vals, n);
+}
+
+// ============================================================================
+// scan / partition / select
+// ============================================================================
+// Exclusive sum as the t03 host loop computes it
+// (tests/t03-bufferScans/hostCode.cpp:53-58), uint32 wraparound; inclusive is
+// the same with the element added first.  The total is returned the way
+// bufferScan returns state[0] (gprt/gprt_scan.slang:290-297).
+extern "C" uint32_t orc_scan_u32(const uint32_t *in, uint32_t *out, size_t n, int inclusive) {
+  uint32_t sum = 0;
+  for (size_t i = 0; i < n; ++i) {
+    uint32_t v = in[i];
+    if (inclusive) {
+      sum += v;
+      out[i] = sum;
+    } else {
+      out[i] = sum;
+      sum += v;
+    }
+  }
+  return sum;
+}
+
+// Selected items (sign bit clear when selectPositive, set otherwise) go to
+// out[excl[i]] (getForwardAddr, gprt/gprt_scan.slang:84-87); with partition the
+// rest go to out[(n-1) - (i - excl[i])] (getReverseAddr, :89-92), i.e. to the
+// back in reverse order.  Known-answer layout:
+// tests/t03-bufferScans/hostCode.cpp:98-160 (partition), 172-241 (select).
+extern "C" uint32_t orc_partition_i32(const int32_t *in, int32_t *out, size_t n, int selectPositive, int partition) {
+  uint32_t excl = 0;
+  for (size_t i = 0; i < n; ++i) {
+    int32_t v = in[i];
+    bool neg = ((uint32_t)v >> 31) != 0;
+    bool sel = selectPositive ? !neg : neg;
+    if (sel) {
+      out[excl] = v;
+      ++excl;
+    } else if (partition) {
+      out[(n - 1) - (i - excl)] = v;
+    }
+  }
+  return excl;
+}
+
+// ============================================================================
+// Morton / Hilbert
+// ============================================================================
+// 10-bit spread: separate_bits (gprt/development/gprt_lbvh.hlsl:25-32).
+static inline uint32_t spread10(uint32_t v) {
+  v &= 0x3FFu;
+  v = (v | (v << 16)) & 0xFF0000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+// morton_encode3D (gprt/development/gprt_lbvh.hlsl:34-37): x in bit 0.
+extern "C" uint32_t orc_morton3d(uint32_t x, uint32_t y, uint32_t z) {
+  return spread10(x) | (spread10(y) << 1) | (spread10(z) << 2);
+}
+
+// 3-D, 10-bit Hilbert index with the orientation conventions of Moore's
+// hilbert_c2i as used by gprt/hilbert.h:179-235 (nDims=3, nBits=10).
+// Restated level by level: the coordinate bits of one level form a 3-bit cell
+// (x in bit 0), each cell is Gray-differenced against the level above, rotated
+// by the running rotation after XOR with the entry flip, and the rotation
+// advances by one plus the position of the cell's lowest set bit among bits
+// 0..1.  The concatenated digits are then XORed with 0b010 in every level
+// except the top, and Gray-decoded (prefix XOR over the whole index).
+extern "C" uint32_t orc_hilbert3d(uint32_t x, uint32_t y, uint32_t z) {
+  uint32_t cell[10];
+  for (int L = 0; L < 10; ++L) cell[L] = ((x >> L) & 1u) | (((y >> L) & 1u) << 1) | (((z >> L) & 1u) << 2);
+  uint32_t g[10];
+  for (int L = 0; L < 10; ++L) g[L] = cell[L] ^ (L < 9 ? cell[L + 1] : 0u);
+  uint32_t index = 0, rotation = 0, flip = 0;
+  for (int L = 9; L >= 0; --L) {
+    uint32_t b = flip ^ g[L];
+    b = ((b >> rotation) | (b << (3 - rotation))) & 7u;
+    index = (index << 3) | b;
+    flip = 1u << rotation;
+    uint32_t low = b & (0u - b) & 3u;
+    rotation += (low == 1u) ? 1u : (low == 2u) ? 2u : 0u;
+    rotation += 1u;
+    if (rotation >= 3u) rotation -= 3u;
+  }
+  index ^= 0x04924924u;  // bits 2,5,...,26
+  for (int d = 1; d < 30; d *= 2) index ^= index >> d;
+  return index;
+}
+
+// ============================================================================
+// bounds and codes
+// ============================================================================
+struct f3 {
+  float x, y, z;
+};
+static inline f3 ld3(const float *p, uint32_t i) { return {p[3 * (size_t)i], p[3 * (size_t)i + 1], p[3 * (size_t)i + 2]}; }
+
+// getTriangleBounds (gprt/development/gprt_lbvh.hlsl:121-129): min/max of the
+// three vertices, min(p1, min(p2, p3)).
+static inline void tri_box(const float *pos, const uint32_t *tri, uint32_t id, float b[6]) {
+  f3 p1 = ld3(pos, tri[3 * (size_t)id]), p2 = ld3(pos, tri[3 * (size_t)id + 1]), p3 = ld3(pos, tri[3 * (size_t)id + 2]);
+  b[0] = std::fmin(p1.x, std::fmin(p2.x, p3.x));
+  b[1] = std::fmin(p1.y, std::fmin(p2.y, p3.y));
+  b[2] = std::fmin(p1.z, std::fmin(p2.z, p3.z));
+  b[3] = std::fmax(p1.x, std::fmax(p2.x, p3.x));
+  b[4] = std::fmax(p1.y, std::fmax(p2.y, p3.y));
+  b[5] = std::fmax(p1.z, std::fmax(p2.z, p3.z));
+}
+
+// ComputeTriangleBounds (gprt/development/gprt_lbvh.hlsl:215-226): the scene
+// AABB, seeded with +-FLT_MAX by the host (gprt/development/gprt_lbvh.h:174-178).
+extern "C" void orc_tri_bounds(const float *pos, const uint32_t *tri, uint32_t n, float out[6]) {
+  const float M = 3.402823466e38f;
+  float s[6] = {M, M, M, -M, -M, -M};
+  for (uint32_t i = 0; i < n; ++i) {
+    float b[6];
+    tri_box(pos, tri, i, b);
+    for (int k = 0; k < 3; ++k) {
+      s[k] = std::fmin(s[k], b[k]);
+      s[3 + k] = std::fmax(s[3 + k], b[3 + k]);
+    }
+  }
+  std::memcpy(out, s, sizeof(s));
+}
+
+extern "C" void orc_point_bounds(const float *pos, uint32_t n, float out[6]) {
+  const float M = 3.402823466e38f;
+  float s[6] = {M, M, M, -M, -M, -M};
+  for (uint32_t i = 0; i < n; ++i) {
+    f3 p = ld3(pos, i);
+    float v[3] = {p.x, p.y, p.z};
+    for (int k = 0; k < 3; ++k) {
+      s[k] = std::fmin(s[k], v[k]);
+      s[3 + k] = std::fmax(s[3 + k], v[k]);
+    }
+  }
+  std::memcpy(out, s, sizeof(s));
+}
+
+// Normalise to the scene box, scale by 1024, clamp to [0,1023], truncate:
+// gprt/development/gprt_lbvh.hlsl:268-274.  The operation order is fixed:
+// (p - min), (max - min), IEEE divide, *1024, max with 0, min with 1023.
+// NaN (a zero-extent axis gives 0/0) clamps to 0, as maxNum semantics give;
+// an infinite extent (tests/t04-swBVH: coordinates near +-1e38) gives 0.
+static inline uint32_t quant10(float p, float lo, float hi) {
+  float v = (p - lo) / (hi - lo);
+  v = v * 1024.0f;
+  v = std::fmax(v, 0.0f);
+  v = std::fmin(v, 1023.0f);
+  return (uint32_t)v;
+}
+
+static inline uint32_t code_of(f3 c, const float b[6], int kind) {
+  uint32_t x = quant10(c.x, b[0], b[3]), y = quant10(c.y, b[1], b[4]), z = quant10(c.z, b[2], b[5]);
+  return kind == 0 ? orc_morton3d(x, y, z) : orc_hilbert3d(x, y, z);
+}
+
+// Centroid (p1 + p2 + p3) / 3 (gprt/development/gprt_lbvh.hlsl:139-146),
+// evaluated left to right.
+extern "C" void orc_tri_codes(const float *pos, const uint32_t *tri, uint32_t n, const float bounds[6], int kind,
+                              uint32_t *codes, uint32_t *ids) {
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)n; ++i) {
+    f3 p1 = ld3(pos, tri[3 * i]), p2 = ld3(pos, tri[3 * i + 1]), p3 = ld3(pos, tri[3 * i + 2]);
+    f3 c = {((p1.x + p2.x) + p3.x) / 3.0f, ((p1.y + p2.y) + p3.y) / 3.0f, ((p1.z + p2.z) + p3.z) / 3.0f};
+    codes[i] = code_of(c, bounds, kind);
+    ids[i] = (uint32_t)i;
+  }
+}
+
+extern "C" void orc_point_codes(const float *pos, uint32_t n, const float bounds[6], int kind, uint32_t *codes,
+                                uint32_t *ids) {
+  for (uint32_t i = 0; i < n; ++i) {
+    codes[i] = code_of(ld3(pos, i), bounds, kind);
+    ids[i] = i;
+  }
+}
+
+// ============================================================================
+// Karras topology
+// ============================================================================
+static inline int clz32(uint32_t v) { return v ? __builtin_clz(v) : 32; }
+
+// delta(i,j) (gprt/development/gprt_lbvh.hlsl:45-61): longest common prefix of
+// codes i and j, extended by the index bits when the codes are equal; -1 when j
+// is outside [0,n).
+static inline int kdelta(const uint32_t *c, int64_t n, int64_t i, int64_t j) {
+  if (j < 0 || j >= n) return -1;
+  uint32_t x = c[i] ^ c[j];
+  if (x == 0) return clz32((uint32_t)i ^ (uint32_t)j) + 32;
+  return clz32(x);
+}
+
+// determine_range + SplitNodes (gprt/development/gprt_lbvh.hlsl:64-103,287-338).
+// The split search uses t = ceil(l / 2^k) in integers.  The reference forms it
+// as ceil(l / divf) in fp32 and keeps iterating with t = 1 until divf
+// overflows, which lands on the same (maximal) split.
+extern "C" void orc_karras(const uint32_t *codes, uint32_t n, int32_t *nodes) {
+  const int64_t N = n;
+  for (int64_t k = 0; k < 4 * (2 * N - 1); ++k) nodes[k] = -1;
+  if (n < 2) return;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < N - 1; ++i) {
+    int d = kdelta(codes, N, i, i + 1) >= kdelta(codes, N, i, i - 1) ? 1 : -1;
+    int dmin = kdelta(codes, N, i, i - d);
+    int64_t lmax = 2;
+    while (kdelta(codes, N, i, i + lmax * d) > dmin) lmax *= 2;
+    int64_t l = 0;
+    for (int64_t t = lmax >> 1; t >= 1; t >>= 1)
+      if (kdelta(codes, N, i, i + (l + t) * d) > dmin) l += t;
+    int64_t j = i + l * d;
+    int dnode = kdelta(codes, N, i, j);
+    int64_t s = 0;
+    for (int64_t k = 1;; ++k) {
+      int64_t t = (l + ((int64_t)1 << k) - 1) >> k;
+      if (kdelta(codes, N, i, i + (s + t) * d) > dnode) s += t;
+      if (t == 1) break;
+    }
+    int64_t split = i + s * d + std::min(d, 0);
+    int64_t first = d == 1 ? i : j, last = d == 1 ? j : i;
+    int64_t left = split, right = split + 1;
+    int64_t lc = (left == first) ? (N - 1) + left : left;
+    int64_t rc = (right == last) ? (N - 1) + right : right;
+    nodes[4 * i + 0] = (int32_t)lc;
+    nodes[4 * i + 1] = (int32_t)rc;
+    nodes[4 * lc + 2] = (int32_t)i;
+    nodes[4 * rc + 2] = (int32_t)i;
+  }
+}
+
+// BuildTriangleHierarchy (gprt/development/gprt_lbvh.hlsl:400-428): leaf
+// n-1+i holds triangle ids[i] and its box; every inner box is the min/max of
+// the leaves below it, starting from MakeNodes' +-1e38 (:279-285).  min/max
+// are exact, so evaluating it bottom-up as the union of the two children gives
+// the identical bits.
+extern "C" void orc_refit_tri(const float *pos, const uint32_t *tri, const uint32_t *ids, uint32_t n,
+                              int32_t *nodes, float *aabbs) {
+  if (n == 0) return;
+  const int64_t N = n, inner = N - 1;
+  for (int64_t k = 0; k < 2 * N - 1; ++k) {
+    for (int a = 0; a < 3; ++a) {
+      aabbs[6 * k + a] = 1e38f;
+      aabbs[6 * k + 3 + a] = -1e38f;
+    }
+  }
+  for (int64_t i = 0; i < N; ++i) {
+    int64_t leaf = inner + i;
+    tri_box(pos, tri, ids[i], &aabbs[6 * leaf]);
+    nodes[4 * leaf + 3] = (int32_t)ids[i];
+  }
+  // Children of inner nodes are not index-ordered, so walk up from each leaf
+  // with a visit counter: the second arrival computes the union.
+  std::vector<uint8_t> seen(inner > 0 ? inner : 1, 0);
+  for (int64_t i = 0; i < N; ++i) {
+    int64_t cur = nodes[4 * (inner + i) + 2];
+    while (cur >= 0) {
+      if (seen[cur]++ == 0) break;
+      int64_t l = nodes[4 * cur], r = nodes[4 * cur + 1];
+      float *b = &aabbs[6 * cur];
+      for (int a = 0; a < 3; ++a) {
+        b[a] = std::fmin(b[a], std::fmin(aabbs[6 * l + a], aabbs[6 * r + a]));
+        b[3 + a] = std::fmax(b[3 + a], std::fmax(aabbs[6 * l + 3 + a], aabbs[6 * r + 3 + a]));
+      }
+      cur = nodes[4 * cur + 2];
+    }
+  }
+}
+
+// Point variant: ComputePointBounds / ComputePointMortonCodes /
+// BuildPointHierarchy (gprt/development/gprt_lbvh.hlsl:188-199,228-243,340-368):
+// a leaf box is the point itself.
+extern "C" void orc_lbvh_build_points(const float *pos, uint32_t n, int kind, float scene[6], uint32_t *codes,
+                                      uint32_t *ids, int32_t *nodes, float *aabbs) {
+  orc_point_bounds(pos, n, scene);
+  orc_point_codes(pos, n, scene, kind, codes, ids);
+  orc_sort(codes, 4, ids, 4, n);
+  orc_karras(codes, n, nodes);
+  if (n == 0) return;
+  // Leaf box (p, p); reuse the triangle refit with a degenerate index triple.
+  std::vector<uint32_t> tri(3 * (size_t)n);
+  for (uint32_t i = 0; i < n; ++i) tri[3 * i] = tri[3 * i + 1] = tri[3 * i + 2] = i;
+  orc_refit_tri(pos, tri.data(), ids, n, nodes, aabbs);
+}
+
+extern "C" void orc_lbvh_build_tri(const float *pos, const uint32_t *tri, uint32_t n, int kind, float scene[6],
+                                   uint32_t *codes, uint32_t *ids, int32_t *nodes, float *aabbs) {
+  orc_tri_bounds(pos, tri, n, scene);
+  orc_tri_codes(pos, tri, n, scene, kind, codes, ids);
+  orc_sort(codes, 4, ids, 4, n);
+  orc_karras(codes, n, nodes);
+  orc_refit_tri(pos, tri, ids, n, nodes, aabbs);
+}
+
+// ============================================================================
+// ray / triangle
+// ============================================================================
+// Kahan's 2x2 determinant a*d - b*c with one fused correction; its sign is
+// exact (relative error <= 2u, Jeannerod-Louvet-Muller 2013), which is what
+// makes the edge tests below watertight without a higher-precision retry.
+static inline float det2(float a, float b, float c, float d) {
+  float w = b * c;
+  float e = std::fma(-b, c, w);
+  float f = std::fma(a, d, -w);
+  return f + e;
+}
+
+struct RayPre {
+  float o[3], d[3], tmin, tmax;
+  int kx, ky, kz;
+  float Sx, Sy, Sz;
+  float inv[3];
+};
+
+// Per-ray set-up of Woop et al. 2013, section 3: kz is the axis of the
+// largest |d| (lowest index on ties), kx/ky follow cyclically and swap when
+// d[kz] < 0 to keep the winding.
+static inline void ray_pre(const float *r, RayPre &p) {
+  p.o[0] = r[0]; p.o[1] = r[1]; p.o[2] = r[2]; p.tmin = r[3];
+  p.d[0] = r[4]; p.d[1] = r[5]; p.d[2] = r[6]; p.tmax = r[7];
+  float ax = std::fabs(p.d[0]), ay = std::fabs(p.d[1]), az = std::fabs(p.d[2]);
+  int kz = (ax >= ay) ? (ax >= az ? 0 : 2) : (ay >= az ? 1 : 2);
+  int kx = kz + 1 == 3 ? 0 : kz + 1;
+  int ky = kx + 1 == 3 ? 0 : kx + 1;
+  if (p.d[kz] < 0.0f) std::swap(kx, ky);
+  p.kx = kx; p.ky = ky; p.kz = kz;
+  p.Sx = p.d[kx] / p.d[kz];
+  p.Sy = p.d[ky] / p.d[kz];
+  p.Sz = 1.0f / p.d[kz];
+  for (int a = 0; a < 3; ++a) p.inv[a] = 1.0f / p.d[a];
+}
+
+// Watertight test, Woop et al. 2013 section 3 with the edge functions from
+// det2().  Returns the hit distance t = T / det in (*t) when the ray crosses
+// the triangle inside [tmin, tmax].
+static inline int isect32(const RayPre &p, const float *v0, const float *v1, const float *v2, float *tout) {
+  float A[3] = {v0[0] - p.o[0], v0[1] - p.o[1], v0[2] - p.o[2]};
+  float B[3] = {v1[0] - p.o[0], v1[1] - p.o[1], v1[2] - p.o[2]};
+  float C[3] = {v2[0] - p.o[0], v2[1] - p.o[1], v2[2] - p.o[2]};
+  float Ax = A[p.kx] - p.Sx * A[p.kz], Ay = A[p.ky] - p.Sy * A[p.kz];
+  float Bx = B[p.kx] - p.Sx * B[p.kz], By = B[p.ky] - p.Sy * B[p.kz];
+  float Cx = C[p.kx] - p.Sx * C[p.kz], Cy = C[p.ky] - p.Sy * C[p.kz];
+  float U = det2(Cx, Cy, Bx, By);  // Cx*By - Cy*Bx
+  float V = det2(Ax, Ay, Cx, Cy);  // Ax*Cy - Ay*Cx
+  float W = det2(Bx, By, Ax, Ay);  // Bx*Ay - By*Ax
+  if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return 0;
+  float det = (U + V) + W;
+  if (det == 0.0f) return 0;
+  float Az = p.Sz * A[p.kz], Bz = p.Sz * B[p.kz], Cz = p.Sz * C[p.kz];
+  float T = (U * Az + V * Bz) + W * Cz;
+  float t = T / det;
+  if (!(t >= p.tmin && t <= p.tmax)) return 0;
+  *tout = t;
+  return 1;
+}
+
+extern "C" int orc_isect_tri32(const float *ray, const float *v0, const float *v1, const float *v2, float *t) {
+  RayPre p;
+  ray_pre(ray, p);
+  return isect32(p, v0, v1, v2, t);
+}
+
+// ---- double-float (unevaluated pair of fp32) arithmetic: Dekker 1971,
+// Knuth TAOCP vol. 2 4.2.2 (TwoSum), FMA-based TwoProduct. ----
+struct df {
+  float hi, lo;
+};
+static inline df two_sum(float a, float b) {
+  float s = a + b;
+  float bb = s - a;
+  float e = (a - (s - bb)) + (b - bb);
+  return {s, e};
+}
+static inline df fast_two_sum(float a, float b) {
+  float s = a + b;
+  float e = b - (s - a);
+  return {s, e};
+}
+static inline df two_prod(float a, float b) {
+  float p = a * b;
+  return {p, std::fma(a, b, -p)};
+}
+static inline df df_add(df x, df y) {
+  df s = two_sum(x.hi, y.hi);
+  df t = two_sum(x.lo, y.lo);
+  s.lo = s.lo + t.hi;
+  s = fast_two_sum(s.hi, s.lo);
+  s.lo = s.lo + t.lo;
+  return fast_two_sum(s.hi, s.lo);
+}
+static inline df df_neg(df x) { return {-x.hi, -x.lo}; }
+static inline df df_mul(df x, df y) {
+  df p = two_prod(x.hi, y.hi);
+  p.lo = p.lo + (x.hi * y.lo + x.lo * y.hi);
+  return fast_two_sum(p.hi, p.lo);
+}
+static inline df df_mulf(df x, float y) {
+  df p = two_prod(x.hi, y);
+  p.lo = p.lo + x.lo * y;
+  return fast_two_sum(p.hi, p.lo);
+}
+static inline float df_div_to_f(df x, df y) {
+  float q1 = x.hi / y.hi;
+  df r = df_add(x, df_neg(df_mulf(y, q1)));
+  float q2 = r.hi / y.hi;
+  df q = fast_two_sum(q1, q2);
+  return q.hi + q.lo;
+}
+
+// Plane-equation distance t = ((v0 - o) . n) / (d . n), n = (v1-v0) x (v2-v0),
+// evaluated in double-float and rounded once to fp32.  Used only to report the
+// distance of the winning hit; which triangle wins is decided by isect32().
+extern "C" float orc_refine_t32(const float *ray, const float *v0, const float *v1, const float *v2) {
+  df e1[3], e2[3], w[3];
+  for (int a = 0; a < 3; ++a) {
+    e1[a] = two_sum(v1[a], -v0[a]);
+    e2[a] = two_sum(v2[a], -v0[a]);
+    w[a] = two_sum(v0[a], -ray[a]);
+  }
+  df n[3];
+  n[0] = df_add(df_mul(e1[1], e2[2]), df_neg(df_mul(e1[2], e2[1])));
+  n[1] = df_add(df_mul(e1[2], e2[0]), df_neg(df_mul(e1[0], e2[2])));
+  n[2] = df_add(df_mul(e1[0], e2[1]), df_neg(df_mul(e1[1], e2[0])));
+  df num = df_add(df_add(df_mul(n[0], w[0]), df_mul(n[1], w[1])), df_mul(n[2], w[2]));
+  df den = df_add(df_add(df_mulf(n[0], ray[4]), df_mulf(n[1], ray[5])), df_mulf(n[2], ray[6]));
+  return df_div_to_f(num, den);
+}
+
+extern "C" double orc_t64(const float *ray, const float *v0, const float *v1, const float *v2) {
+  double e1[3], e2[3], w[3];
+  for (int a = 0; a < 3; ++a) {
+    e1[a] = (double)v1[a] - (double)v0[a];
+    e2[a] = (double)v2[a] - (double)v0[a];
+    w[a] = (double)v0[a] - (double)ray[a];
+  }
+  double n0 = e1[1] * e2[2] - e1[2] * e2[1];
+  double n1 = e1[2] * e2[0] - e1[0] * e2[2];
+  double n2 = e1[0] * e2[1] - e1[1] * e2[0];
+  double num = n0 * w[0] + n1 * w[1] + n2 * w[2];
+  double den = n0 * (double)ray[4] + n1 * (double)ray[5] + n2 * (double)ray[6];
+  return num / den;
+}
+
+// ============================================================================
+// ray / box and traversal
+// ============================================================================
+// Slab test, Ize 2013: per-axis (b - o) * (1/d); NaN slabs (0 * inf, a ray in
+// a face plane) impose no bound because fmin/fmax return the other operand.
+// The entry is scaled down and the exit up by 2^-18 so that a triangle hit the
+// watertight test reports is never pruned by a box that contains it.
+static const float kBoxLo = 1.0f - 1.0f / 262144.0f;
+static const float kBoxHi = 1.0f + 1.0f / 262144.0f;
+
+static inline int ray_box(const RayPre &p, const float *b, float tmax, float *tnear_out) {
+  float t0x = (b[0] - p.o[0]) * p.inv[0], t1x = (b[3] - p.o[0]) * p.inv[0];
+  float t0y = (b[1] - p.o[1]) * p.inv[1], t1y = (b[4] - p.o[1]) * p.inv[1];
+  float t0z = (b[2] - p.o[2]) * p.inv[2], t1z = (b[5] - p.o[2]) * p.inv[2];
+  float tn = std::fmax(std::fmax(std::fmin(t0x, t1x), std::fmin(t0y, t1y)), std::fmax(std::fmin(t0z, t1z), p.tmin));
+  float tf = std::fmin(std::fmin(std::fmax(t0x, t1x), std::fmax(t0y, t1y)), std::fmin(std::fmax(t0z, t1z), tmax));
+  tn = tn * kBoxLo;
+  tf = tf * kBoxHi;
+  *tnear_out = tn;
+  return tn <= tf;
+}
+
+static inline void tri_verts(const float *pos, const uint32_t *tri, uint32_t id, const float *&a, const float *&b,
+                             const float *&c) {
+  a = pos + 3 * (size_t)tri[3 * (size_t)id];
+  b = pos + 3 * (size_t)tri[3 * (size_t)id + 1];
+  c = pos + 3 * (size_t)tri[3 * (size_t)id + 2];
+}
+
+extern "C" void orc_trace_brute(const float *pos, const uint32_t *tri, uint32_t n, const float *rays, uint64_t nrays,
+                                orc_hit *hits) {
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t r = 0; r < (int64_t)nrays; ++r) {
+    RayPre p;
+    ray_pre(rays + 8 * r, p);
+    uint32_t best = 0xFFFFFFFFu;
+    float bt = 0.0f;
+    for (uint32_t i = 0; i < n; ++i) {
+      const float *a, *b, *c;
+      tri_verts(pos, tri, i, a, b, c);
+      float t;
+      if (isect32(p, a, b, c, &t) && (best == 0xFFFFFFFFu || t < bt)) {
+        best = i;
+        bt = t;
+      }
+    }
+    hits[r].prim = best;
+    if (best != 0xFFFFFFFFu) {
+      const float *a, *b, *c;
+      tri_verts(pos, tri, best, a, b, c);
+      hits[r].t = orc_refine_t32(rays + 8 * r, a, b, c);
+    } else {
+      hits[r].t = INFINITY;
+    }
+  }
+}
+
+// Depth-first traversal of the reference layout.  A node is entered when its
+// box passes ray_box and its entry distance does not exceed the best hit so
+// far (equal entry distance is entered, so that a tie can still be won by a
+// lower primitive id).  Closest hit = smallest (t, primID).
+extern "C" void orc_trace_lbvh(const float *pos, const uint32_t *tri, uint32_t n, const int32_t *nodes,
+                               const float *aabbs, const float *rays, uint64_t nrays, int anyhit, orc_hit *hits) {
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t r = 0; r < (int64_t)nrays; ++r) {
+    RayPre p;
+    ray_pre(rays + 8 * r, p);
+    uint32_t best = 0xFFFFFFFFu;
+    float bt = p.tmax;
+    if (n > 0) {
+      int32_t stack[128];
+      int sp = 0;
+      stack[sp++] = 0;
+      while (sp > 0) {
+        int32_t node = stack[--sp];
+        float tn;
+        if (!ray_box(p, &aabbs[6 * (size_t)node], bt, &tn)) continue;
+        if (tn > bt) continue;
+        int32_t leaf = nodes[4 * (size_t)node + 3];
+        if (leaf >= 0) {
+          const float *a, *b, *c;
+          tri_verts(pos, tri, (uint32_t)leaf, a, b, c);
+          float t;
+          if (isect32(p, a, b, c, &t)) {
+            if (best == 0xFFFFFFFFu || t < bt || (t == bt && (uint32_t)leaf < best)) {
+              best = (uint32_t)leaf;
+              bt = t;
+              if (anyhit) break;
+            }
+          }
+        } else {
+          stack[sp++] = nodes[4 * (size_t)node + 1];
+          stack[sp++] = nodes[4 * (size_t)node + 0];
+        }
+      }
+    }
+    hits[r].prim = best;
+    if (best != 0xFFFFFFFFu) {
+      const float *a, *b, *c;
+      tri_verts(pos, tri, best, a, b, c);
+      hits[r].t = orc_refine_t32(rays + 8 * r, a, b, c);
+    } else {
+      hits[r].t = INFINITY;
+    }
+  }
+}
+
+extern "C" int orc_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}

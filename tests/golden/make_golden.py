@@ -1,0 +1,108 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+    python tests/golden/make_golden.py      (needs the reference sources; run
+                                             where they are mounted)
+
+* lbvh_ref.npz   -- gprt/development/gprt_lbvh.hlsl compiled from the
+                    reference sources (oracle/Makefile target `ref`) and run
+                    serially in gprtLBVHBuild's order: scene box, Morton codes,
+                    sorted (code, id) pairs, int4 nodes, float3 box pairs, for
+                    seeded triangle soups and for a t04-style point set with
+                    coordinates in [-1e38, 1e38] (tests/t04-swBVH/hostCode.cpp:47-56).
+* hilbert_ref.npz -- gprt/hilbert.h hilbert_c2i(3, 10, .) on seeded and corner
+                    coordinates.
+* sortscan.npz   -- the reference tests' own host oracles restated with numpy:
+                    std::sort / std::sort-by-key (tests/t02-bufferSort/hostCode.cpp:59,115),
+                    the serial exclusive sum (tests/t03-bufferScans/hostCode.cpp:53-58)
+                    and the partition/select layouts (:98-160, :172-241), on
+                    small seeded inputs.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+import oracle  # noqa: E402
+
+
+def tri_soup(rng, n, sigma=0.002):
+    c = rng.random((n, 3), dtype=np.float32)
+    pos = (np.repeat(c, 3, axis=0) + rng.normal(0.0, sigma, (3 * n, 3))).astype(np.float32)
+    tri = np.arange(3 * n, dtype=np.uint32).reshape(n, 3)
+    return pos, tri
+
+
+def main():
+    oracle.build(ref=True)
+    rng = np.random.default_rng(20240601)
+    out = {}
+    cases = []
+    for n in (1, 2, 3, 7, 64, 1000, 4099):
+        cases.append(("tri%d" % n,) + tri_soup(rng, n))
+    # duplicate-heavy codes (equal Morton codes exercise the index tie-break)
+    n = 777
+    c = (np.floor(rng.random((n, 3)) * 3) / 3).astype(np.float32)
+    cases.append(("tridup", np.repeat(c, 3, axis=0).astype(np.float32), np.arange(3 * n, dtype=np.uint32).reshape(n, 3)))
+    # shared vertices (indexed mesh, not a soup)
+    grid = rng.random((200, 3), dtype=np.float32)
+    tri = rng.integers(0, 200, size=(500, 3)).astype(np.uint32)
+    cases.append(("trimesh", grid, tri))
+    for name, pos, tri in cases:
+        r = oracle.ref_lbvh_build(pos, tri)
+        out[name + "_pos"] = pos
+        out[name + "_tri"] = tri
+        for k, v in r.items():
+            out[name + "_" + k] = v
+    # t04: 42 points uniform in [-1e38, 1e38]^3 (max - min overflows to inf)
+    pts = rng.uniform(-1e38, 1e38, size=(42, 3)).astype(np.float32)
+    r = oracle.ref_lbvh_build(pts)
+    out["pts42_pos"] = pts
+    for k, v in r.items():
+        out["pts42_" + k] = v
+    np.savez_compressed(os.path.join(HERE, "lbvh_ref.npz"), **out)
+
+    R = oracle.ref()
+    co = rng.integers(0, 1024, size=(4096, 3)).astype(np.uint32)
+    corners = np.array([[x, y, z] for x in (0, 1, 511, 512, 1023) for y in (0, 1, 511, 512, 1023)
+                        for z in (0, 1, 511, 512, 1023)], np.uint32)
+    co = np.concatenate([co, corners])
+    h = np.array([R.ref_hilbert3d(int(a), int(b), int(c)) for a, b, c in co], np.uint32)
+    np.savez_compressed(os.path.join(HERE, "hilbert_ref.npz"), coords=co, codes=h)
+
+    # sort / scan / partition fixtures from numpy restatements of the tests' host oracles
+    k = rng.integers(0, 2 ** 32, size=5000, dtype=np.uint64).astype(np.uint32)
+    k[::7] = k[0]  # repeated keys so stability matters
+    v = np.arange(k.size, dtype=np.uint32)
+    order = np.argsort(k, kind="stable")
+    k64 = rng.integers(0, 2 ** 63, size=3000, dtype=np.uint64) | (rng.integers(0, 2, size=3000, dtype=np.uint64) << np.uint64(63))
+    k64[::5] = k64[1]
+    o64 = np.argsort(k64, kind="stable")
+    x = rng.integers(0, 256, size=9973 * 3, dtype=np.uint32)
+    excl = (np.concatenate([np.zeros(1, np.uint64), np.cumsum(x.astype(np.uint64))[:-1]]) & 0xFFFFFFFF).astype(np.uint32)
+    big = np.full(3000, 0xFFFFFFF0, np.uint32)  # forces uint32 wraparound
+    excl_big = (np.concatenate([np.zeros(1, np.uint64), np.cumsum(big.astype(np.uint64))[:-1]]) & 0xFFFFFFFF).astype(np.uint32)
+    nt = 9973 * 2
+    t03 = np.array([i * (1 if (i & 1) else -1) for i in range(nt)], np.int32)
+    sel = (t03 >= 0).astype(np.int64)
+    ex = np.concatenate([[0], np.cumsum(sel)[:-1]])
+    part = np.zeros(nt, np.int32)
+    selo = np.zeros(nt, np.int32)
+    for i in range(nt):
+        if t03[i] >= 0:
+            part[ex[i]] = t03[i]
+            selo[ex[i]] = t03[i]
+        else:
+            part[(nt - 1) - (i - ex[i])] = t03[i]
+    np.savez_compressed(os.path.join(HERE, "sortscan.npz"), keys=k, keys_sorted=k[order], vals_sorted=v[order],
+                        keys64=k64, keys64_sorted=k64[o64], vals64_sorted=o64.astype(np.uint32), scan_in=x,
+                        scan_excl=excl, scan_total=np.uint32(int(x.astype(np.uint64).sum()) & 0xFFFFFFFF),
+                        big_in=big, big_excl=excl_big, t03_in=t03, t03_partition=part, t03_select=selo,
+                        t03_total=np.uint32(sel.sum()))
+    print("wrote fixtures to", HERE)
+
+
+if __name__ == "__main__":
+    main()

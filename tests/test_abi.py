@@ -1,0 +1,47 @@
+"""The C-ABI library loads and exports every symbol the public headers declare.
+CPU only: no compute call is made."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared(header):
+    txt = open(os.path.join(ROOT, "include", header)).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    txt = "\n".join(l for l in txt.splitlines() if not l.lstrip().startswith("#"))
+    return sorted(set(re.findall(r"GPRT(?:CU)?_API\s+[^;(]*?\b(\w+)\s*\(", txt)))
+
+
+def test_headers_declare_entry_points():
+    names = _declared("gprtcu.h")
+    assert "gprtcuExclusiveSumU32" in names and "gprtcuScanScratchSize" in names
+
+
+@pytest.mark.parametrize("header", ["gprtcu.h", "gprt_compat.h"])
+def test_library_exports_every_declared_symbol(header):
+    if not os.path.exists(os.path.join(ROOT, "include", header)):
+        pytest.skip("header not present")
+    import gprt_b200
+    L = gprt_b200.lib()
+    missing = [n for n in _declared(header) if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_ctypes_signatures_cover_header():
+    from gprt_b200 import _sigs
+    names = set(_declared("gprtcu.h"))
+    assert names <= set(_sigs.SIGNATURES), sorted(names - set(_sigs.SIGNATURES))
+
+
+def test_host_side_argument_checks_without_gpu():
+    # Host-side validation returns before any CUDA call.
+    import gprt_b200
+    L = gprt_b200.lib()
+    assert L.gprtcuExclusiveSumU32(None, None, 10, None, None, 0, None) == 1  # INVALID_ARG
+    assert L.gprtcuScanScratchSize(0) == 256
+    assert L.gprtcuScanScratchSize(8192) == 256 + 256
+    assert L.gprtcuStatusString(4) == b"device-side wait exceeded its budget"

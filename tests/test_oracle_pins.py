@@ -1,0 +1,144 @@
+"""The oracle against the reference: golden fixtures made by the reference's
+own code (tests/golden/make_golden.py), the reference tests' known answers,
+and -- where the reference sources are mounted -- the reference-compiled
+checker directly.  CPU only."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _bits(a):
+    return a.view(np.uint32) if a.dtype == np.float32 else a
+
+
+@pytest.fixture(scope="module")
+def lbvh_gold():
+    return np.load(os.path.join(GOLD, "lbvh_ref.npz"))
+
+
+def _cases(g):
+    return sorted({k.rsplit("_", 1)[0] for k in g.files if k.endswith("_nodes")})
+
+
+def test_lbvh_matches_reference_fixtures(lbvh_gold):
+    g = lbvh_gold
+    cases = _cases(g)
+    assert len(cases) >= 9
+    for c in cases:
+        if c.startswith("pts"):
+            r = oracle.lbvh_build_points(g[c + "_pos"])
+        else:
+            r = oracle.lbvh_build_tri(g[c + "_pos"], g[c + "_tri"])
+        for k in ("scene", "codes", "ids", "nodes", "aabbs"):
+            exp = g[c + "_" + k].reshape(r[k].shape)
+            assert np.array_equal(_bits(r[k]), _bits(exp)), (c, k)
+
+
+def test_overflowing_extent_gives_zero_codes():
+    # tests/t04-swBVH draws coordinates from [-1e38, 1e38]; there the extent
+    # stays finite (< FLT_MAX).  Push it past FLT_MAX: max - min = inf, every
+    # normalised coordinate is 0 or inf/inf = NaN, both clamp to 0.
+    pts = np.array([[-3e38, 0, 0], [3e38, 1, 1], [1e38, 0.5, 0.25], [0, 1, 0]], np.float32)
+    r = oracle.lbvh_build_points(pts)
+    assert np.isinf(np.float32(r["scene"][3]) - np.float32(r["scene"][0]))
+    xs = [c & 0x09249249 for c in r["codes"]]  # x bits only
+    assert all(x == 0 for x in xs)
+    if oracle.ref_available():
+        b = oracle.ref_lbvh_build(pts)
+        assert np.array_equal(b["codes"], r["codes"]) and np.array_equal(b["nodes"], r["nodes"].reshape(b["nodes"].shape))
+
+
+def test_hilbert_matches_reference_fixture():
+    g = np.load(os.path.join(GOLD, "hilbert_ref.npz"))
+    got = np.array([oracle.hilbert3d(*c) for c in g["coords"]], np.uint32)
+    assert np.array_equal(got, g["codes"])
+
+
+def test_morton_known_answers():
+    assert oracle.morton3d(0, 0, 0) == 0
+    assert oracle.morton3d(1, 0, 0) == 1
+    assert oracle.morton3d(0, 1, 0) == 2
+    assert oracle.morton3d(0, 0, 1) == 4
+    assert oracle.morton3d(1023, 1023, 1023) == (1 << 30) - 1
+    assert oracle.morton3d(1023, 0, 0) == 0x09249249
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference sources not compiled here")
+def test_lbvh_matches_reference_compiled_random():
+    rng = np.random.default_rng(5)
+    for n in (5, 300, 20000):
+        c = rng.random((n, 3), dtype=np.float32)
+        pos = (np.repeat(c, 3, axis=0) + rng.normal(0, 0.01, (3 * n, 3))).astype(np.float32)
+        tri = rng.permutation(3 * n).astype(np.uint32).reshape(n, 3)
+        a = oracle.lbvh_build_tri(pos, tri)
+        b = oracle.ref_lbvh_build(pos, tri)
+        for k in a:
+            assert np.array_equal(_bits(a[k]), _bits(b[k].reshape(a[k].shape))), (n, k)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference sources not compiled here")
+def test_hilbert_matches_reference_compiled_exhaustive_slices():
+    R = oracle.ref()
+    L = oracle.lib()
+    for x in range(0, 1024, 31):
+        for y in range(0, 1024, 37):
+            for z in (0, 5, 1023, (x * 7 + y) & 1023):
+                assert L.orc_hilbert3d(x, y, z) == R.ref_hilbert3d(x, y, z)
+
+
+def test_sort_matches_t02_oracle_fixture():
+    g = np.load(os.path.join(GOLD, "sortscan.npz"))
+    k, v = oracle.sort(g["keys"], np.arange(g["keys"].size, dtype=np.uint32))
+    assert np.array_equal(k, g["keys_sorted"]) and np.array_equal(v, g["vals_sorted"])
+    k = oracle.sort(g["keys"])
+    assert np.array_equal(k, g["keys_sorted"])
+    k, v = oracle.sort(g["keys64"], np.arange(g["keys64"].size, dtype=np.uint32))
+    assert np.array_equal(k, g["keys64_sorted"]) and np.array_equal(v, g["vals64_sorted"])
+
+
+def test_scan_matches_t03_oracle_fixture():
+    g = np.load(os.path.join(GOLD, "sortscan.npz"))
+    out, total = oracle.scan(g["scan_in"])
+    assert np.array_equal(out, g["scan_excl"]) and total == int(g["scan_total"])
+    out, _ = oracle.scan(g["big_in"])
+    assert np.array_equal(out, g["big_excl"])
+    inc, total2 = oracle.scan(g["scan_in"], inclusive=True)
+    assert np.array_equal(inc, g["scan_excl"] + g["scan_in"]) and total2 == total
+
+
+def test_scan_t03_all_ones_known_answer():
+    # tests/t03-bufferScans/hostCode.cpp:38-81: all ones -> excl[i] = i, total N.
+    for k in (2, 3, 17, 101):
+        n = 9973 * k
+        out, total = oracle.scan(np.ones(n, np.uint32))
+        assert total == n and np.array_equal(out, np.arange(n, dtype=np.uint32))
+
+
+def test_partition_select_t03_known_answer():
+    g = np.load(os.path.join(GOLD, "sortscan.npz"))
+    p, t = oracle.partition(g["t03_in"], True, True)
+    assert np.array_equal(p, g["t03_partition"]) and t == int(g["t03_total"])
+    s, t2 = oracle.partition(g["t03_in"], True, False)
+    assert np.array_equal(s[:t2], g["t03_select"][:t2]) and t2 == t
+
+
+def test_karras_structure_invariants():
+    rng = np.random.default_rng(3)
+    for n in (2, 3, 10, 1000):
+        codes = np.sort(rng.integers(0, 1 << 30, size=n).astype(np.uint32))
+        codes[n // 2:n // 2 + n // 4] = codes[n // 2]
+        nodes = oracle.karras(codes)
+        inner = n - 1
+        parent_count = np.zeros(2 * n - 1, np.int64)
+        for i in range(inner):
+            l, r = nodes[i, 0], nodes[i, 1]
+            assert nodes[l, 2] == i and nodes[r, 2] == i
+            parent_count[l] += 1
+            parent_count[r] += 1
+        assert parent_count[0] == 0 and (parent_count[1:] == 1).all()
+        assert nodes[0, 2] == -1
