@@ -18,6 +18,18 @@ SIGNATURES = {
     "gprtcuInclusiveSumU32": ([vp, vp, u64, vp, vp, sz, vp], st),
     "gprtcuPartitionI32": ([vp, vp, u64, i32, vp, vp, sz, vp], st),
     "gprtcuSelectI32": ([vp, vp, u64, i32, vp, vp, sz, vp], st),
+    "gprtcuSortScratchSize": ([u64, i32, i32], sz),
+    "gprtcuSortKeysU32": ([vp, u64, i32, i32, vp, sz, vp], st),
+    "gprtcuSortPairsU32": ([vp, vp, u64, i32, i32, vp, sz, vp], st),
+    "gprtcuSortKeysU64": ([vp, u64, i32, i32, vp, sz, vp], st),
+    "gprtcuSortPairsU64": ([vp, vp, u64, i32, i32, vp, sz, vp], st),
+    "gprtcuSortPairsU64U64": ([vp, vp, u64, i32, i32, vp, sz, vp], st),
+    "gprtcuLbvhScratchSize": ([u32], sz),
+    "gprtcuLbvhBuildTriangles": ([vp, vp, u32, i32, vp, vp, sz, vp], st),
+    "gprtcuLbvhBuildPoints": ([vp, u32, i32, vp, vp, sz, vp], st),
+    "gprtcuTraceScratchSize": ([], sz),
+    "gprtcuTraceClosest": ([vp, vp, u64, vp, vp, sz, vp], st),
+    "gprtcuTraceAny": ([vp, vp, u64, vp, vp, sz, vp], st),
     "gprtcuDebugSetSpinBudget": ([u32], None),
     "gprtcuDebugScanSkipTile": ([i64], None),
     "gprtcuDebugScanImpl": ([i32], None),

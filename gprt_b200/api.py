@@ -87,3 +87,129 @@ def partition(inp, select_positive=True, out=None, count=None, scr=None, select_
 
 def select(inp, select_positive=True, out=None, count=None, scr=None):
     return partition(inp, select_positive, out, count, scr, select_only=True)
+
+
+# ---------------------------------------------------------------- sort
+_SORT_FN = {
+    (4, 0): "gprtcuSortKeysU32",
+    (4, 4): "gprtcuSortPairsU32",
+    (8, 0): "gprtcuSortKeysU64",
+    (8, 4): "gprtcuSortPairsU64",
+    (8, 8): "gprtcuSortPairsU64U64",
+}
+
+
+def sort_scratch_size(n, key_bytes, value_bytes):
+    return lib().gprtcuSortScratchSize(int(n), int(key_bytes), int(value_bytes))
+
+
+def sort(keys, values=None, begin_bit=0, end_bit=None, scr=None):
+    """Stable in-place radix sort of `keys` (int32/uint32 or int64/uint64
+    tensors, compared as unsigned) carrying `values` (optional, 4 or 8 bytes)."""
+    _need_cuda(keys, values)
+    kw = keys.element_size()
+    vw = 0 if values is None else values.element_size()
+    if values is not None and values.numel() != keys.numel():
+        raise ValueError("keys and values differ in size")
+    n = keys.numel()
+    if end_bit is None:
+        end_bit = 8 * kw
+    if scr is None:
+        scr = scratch(sort_scratch_size(n, kw, vw), keys.device)
+    name = _SORT_FN[(kw, vw)]
+    f = getattr(lib(), name)
+    if vw:
+        st = f(_ptr(keys), _ptr(values), n, begin_bit, end_bit, _ptr(scr), scr.numel(), _stream())
+    else:
+        st = f(_ptr(keys), n, begin_bit, end_bit, _ptr(scr), scr.numel(), _stream())
+    _check(st, name)
+    return keys, values
+
+
+# ---------------------------------------------------------------- LBVH + trace
+class LbvhDesc(ctypes.Structure):
+    """gprtcuLbvh (include/gprtcu.h)."""
+    _fields_ = [("numPrims", ctypes.c_uint32), ("codes", ctypes.c_void_p), ("ids", ctypes.c_void_p),
+                ("nodes", ctypes.c_void_p), ("aabbs", ctypes.c_void_p), ("sceneBounds", ctypes.c_void_p),
+                ("rootBox", ctypes.c_void_p), ("bvh2", ctypes.c_void_p), ("leafTris", ctypes.c_void_p)]
+
+
+class Lbvh:
+    """Device arrays of one LBVH (torch tensors) plus its C descriptor."""
+
+    def __init__(self, n, device="cuda", with_aabbs=True, with_traversal=True):
+        self.n = int(n)
+        nn = max(2 * self.n - 1, 1)
+        dev = torch.device(device)
+        self.codes = torch.empty(self.n, dtype=torch.int32, device=dev)
+        self.ids = torch.empty(self.n, dtype=torch.int32, device=dev)
+        self.nodes = torch.empty((nn, 4), dtype=torch.int32, device=dev)
+        self.aabbs = torch.empty((nn, 6), dtype=torch.float32, device=dev) if with_aabbs else None
+        self.scene = torch.empty(6, dtype=torch.float32, device=dev)
+        self.root = torch.empty(6, dtype=torch.float32, device=dev)
+        self.bvh2 = torch.empty((max(self.n - 1, 1), 16), dtype=torch.float32, device=dev) if with_traversal else None
+        self.leaf = torch.empty((self.n, 12), dtype=torch.float32, device=dev) if with_traversal else None
+        self.scratch = scratch(lib().gprtcuLbvhScratchSize(self.n), dev)
+        self.desc = LbvhDesc(0, _p(self.codes), _p(self.ids), _p(self.nodes), _p(self.aabbs), _p(self.scene),
+                             _p(self.root), _p(self.bvh2), _p(self.leaf))
+
+    def host(self):
+        """Copy the reference-layout arrays back (numpy dict, oracle layout)."""
+        import numpy as np
+        torch.cuda.synchronize()
+        d = dict(codes=self.codes.cpu().numpy().view(np.uint32), ids=self.ids.cpu().numpy().view(np.uint32),
+                 nodes=self.nodes.cpu().numpy(), scene=self.scene.cpu().numpy())
+        if self.aabbs is not None:
+            d["aabbs"] = self.aabbs.cpu().numpy()
+        return d
+
+
+def _p(t):
+    return t.data_ptr() if t is not None else None
+
+
+def lbvh_build_triangles(pos, tri, bvh=None, code_kind=0):
+    """Build over float32 positions [V,3] and uint32/int32 indices [N,3] (CUDA tensors)."""
+    _need_cuda(pos, tri)
+    n = tri.shape[0]
+    if bvh is None:
+        bvh = Lbvh(n, pos.device)
+    st = lib().gprtcuLbvhBuildTriangles(_ptr(pos), _ptr(tri), n, code_kind, ctypes.byref(bvh.desc), _ptr(bvh.scratch),
+                                        bvh.scratch.numel(), _stream())
+    _check(st, "gprtcuLbvhBuildTriangles")
+    return bvh
+
+
+def lbvh_build_points(pos, bvh=None, code_kind=0):
+    _need_cuda(pos)
+    n = pos.shape[0]
+    if bvh is None:
+        bvh = Lbvh(n, pos.device, with_traversal=False)
+    st = lib().gprtcuLbvhBuildPoints(_ptr(pos), n, code_kind, ctypes.byref(bvh.desc), _ptr(bvh.scratch),
+                                     bvh.scratch.numel(), _stream())
+    _check(st, "gprtcuLbvhBuildPoints")
+    return bvh
+
+
+def trace(bvh, rays, hits=None, anyhit=False, scr=None):
+    """rays: float32 [R, 8] {org.xyz, tmin, dir.xyz, tmax}; returns hits int32 [R, 2] {prim, t bits}."""
+    _need_cuda(rays)
+    nr = rays.shape[0]
+    if hits is None:
+        hits = torch.empty((nr, 2), dtype=torch.int32, device=rays.device)
+    if scr is None:
+        scr = scratch(lib().gprtcuTraceScratchSize(), rays.device)
+    f = lib().gprtcuTraceAny if anyhit else lib().gprtcuTraceClosest
+    _check(f(ctypes.byref(bvh.desc), _ptr(rays), nr, _ptr(hits), _ptr(scr), scr.numel(), _stream()),
+           "gprtcuTraceAny" if anyhit else "gprtcuTraceClosest")
+    return hits
+
+
+def hits_numpy(hits):
+    """Device hits -> numpy structured array {prim uint32, t float32}."""
+    import numpy as np
+    h = hits.cpu().numpy()
+    out = np.zeros(h.shape[0], dtype=[("prim", np.uint32), ("t", np.float32)])
+    out["prim"] = h[:, 0].view(np.uint32)
+    out["t"] = h[:, 1].view(np.float32)
+    return out

@@ -163,159 +163,184 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_u32(const uint32_t *__res
 }
 
 
-// Persistent, TMA-pipelined form of the same scan (16-byte aligned in/out).
-// Each CTA keeps PS_STAGES tiles in flight: thread 0 takes tile tickets ahead
-// and streams each full tile global->shared with one bulk async copy
-// (completion counted on a per-stage mbarrier); all warps scan the tile out
-// of shared memory, write the results back in place and thread 0 sends them
-// to global memory with one bulk async store.  Loads of the next tiles
-// therefore overlap the current tile's look-back and store.
-// Forward progress: a CTA processes its tickets in increasing order and a
-// tile waits only on smaller tickets, so the smallest unfinished ticket can
-// always proceed.
-constexpr int PS_STAGES = 3;
-constexpr int PS_TILE_BYTES = SCAN_TILE * 4;
-constexpr size_t PS_SMEM = (size_t)PS_STAGES * PS_TILE_BYTES + PS_STAGES * 8 + PS_STAGES * 4;
+// Look-back over 128 predecessors per probe (4 status words per lane, lane
+// l covering tiles base-4l .. base-4l-3, nearest first).  The inclusive
+// prefix can only travel as fast as one probe window per L2 round trip, so a
+// wide window keeps it ahead of the tile rate the HBM can feed.
+__device__ __forceinline__ bool scan_lookback128(const uint64_t *status, uint64_t tile, int lane, uint32_t budget,
+                                                 uint32_t &excl_out) {
+  uint32_t excl = 0;
+  int64_t base = (int64_t)tile - 1;
+  uint32_t spins = 0;
+  while (true) {
+    uint64_t s[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int64_t idx = base - 4 * lane - c;
+      s[c] = idx >= 0 ? ld_relaxed_u64(&status[idx]) : ST_INC;
+    }
+    unsigned stopm;
+    int cstop;
+    while (true) {
+      cstop = 4;
+#pragma unroll
+      for (int c = 3; c >= 0; --c)
+        if ((s[c] >> 32) >= 2) cstop = c;
+      stopm = __ballot_sync(FULL_MASK, cstop < 4);
+      const int stop_lane = stopm ? __ffs(stopm) - 1 : 32;
+      const int need = lane < stop_lane ? 4 : (lane == stop_lane ? cstop + 1 : 0);
+      bool ready = true;
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        if (c < need && (s[c] >> 32) == 0) ready = false;
+      if (__all_sync(FULL_MASK, ready)) break;
+      if (++spins > budget) return false;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int64_t idx = base - 4 * lane - c;
+        if (c < need && (s[c] >> 32) == 0) s[c] = ld_relaxed_u64(&status[idx]);
+      }
+    }
+    const int stop_lane = stopm ? __ffs(stopm) - 1 : 32;
+    const int use = lane < stop_lane ? 4 : (lane == stop_lane ? cstop + 1 : 0);
+    uint32_t v = 0;
+    bool poison = false;
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      if (c < use) {
+        v += (uint32_t)s[c];
+        poison |= (s[c] >> 32) == 3;
+      }
+    if (__any_sync(FULL_MASK, poison)) return false;
+    excl += warp_sum(v);
+    if (stopm) break;
+    base -= 128;
+  }
+  excl_out = excl;
+  return true;
+}
+
+// Tile-per-CTA scan with TMA staging (16-byte aligned in/out).  A 128-thread
+// CTA owns one 8192-element tile: thread 0 takes a ticket and brings the
+// whole 32 KB tile into shared memory with one bulk async copy; the four warps
+// reduce it (row sums), publish the tile aggregate, warp 0 looks back, then
+// the warps scan the tile row by row in shared memory and thread 0 writes it
+// out with one bulk async store.  32 KB of shared memory and few registers
+// per CTA let seven CTAs share an SM, so many tiles' loads are in flight while
+// other tiles wait on their look-back.
+constexpr int TS_THREADS = 128;
+constexpr int TS_WARPS = TS_THREADS / 32;
+constexpr int TS_ROWS = SCAN_TILE / (TS_WARPS * 128);  // 16 rows of 128 elements per warp
+constexpr size_t TS_SMEM = (size_t)SCAN_TILE * 4;
 
 template <int MODE>
-__global__ void __launch_bounds__(SCAN_THREADS, 2)
-    k_scan_pipe(const uint32_t *__restrict__ in, uint32_t *out, uint64_t n, uint64_t num_tiles, ScratchHeader *hdr,
-                uint64_t *status, uint32_t *d_total, uint32_t budget, int64_t skip_tile) {
+__global__ void __launch_bounds__(TS_THREADS) k_scan_tma(const uint32_t *in, uint32_t *out, uint64_t n,
+                                                        uint64_t num_tiles, ScratchHeader *hdr, uint64_t *status,
+                                                        uint32_t *d_total, uint32_t budget, int64_t skip_tile) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint4 *buf = reinterpret_cast<uint4 *>(smem);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (size_t)PS_STAGES * PS_TILE_BYTES);
-  uint32_t *stage_tile = reinterpret_cast<uint32_t *>(bars + PS_STAGES);
-  __shared__ uint32_t s_warp[SCAN_THREADS / 32];
-  __shared__ uint32_t s_prefix;
-  __shared__ uint32_t s_abort;
+  __shared__ uint64_t bar;
+  __shared__ uint32_t s_tile, s_abort, s_prefix;
+  __shared__ uint32_t s_warp[TS_WARPS];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-
-  auto issue = [&](int s) {  // thread 0 only
-    uint32_t t = atomicAdd(&hdr->ticket[0], 1u);
-    stage_tile[s] = t;
-    uint64_t start = (uint64_t)t * SCAN_TILE;
-    if (t < num_tiles && start + SCAN_TILE <= n) {
-      mbar_arrive_expect_tx(&bars[s], PS_TILE_BYTES);
-      bulk_g2s(buf + (size_t)s * (SCAN_TILE / 4), in + start, PS_TILE_BYTES, &bars[s]);
-    } else {
-      mbar_arrive(&bars[s]);  // past the end, or the ragged last tile (loaded directly)
-    }
-  };
-
   if (tid == 0) {
-    for (int s = 0; s < PS_STAGES; ++s) mbar_init(&bars[s], 1);
-    fence_mbar_init();
+    s_tile = atomicAdd(&hdr->ticket[0], 1u);
     s_abort = 0;
+    mbar_init(&bar, 1);
+    fence_mbar_init();
   }
   __syncthreads();
-  if (tid == 0)
-    for (int s = 0; s < PS_STAGES; ++s) issue(s);
-
-  for (uint32_t k = 0;; ++k) {
-    const int s = k % PS_STAGES;
-    if (!mbar_wait(&bars[s], (k / PS_STAGES) & 1u, MBAR_WAIT_BUDGET)) s_abort = 1;
-    __syncthreads();
-    if (s_abort) {
-      if (tid == 0) record_error(hdr, GPRTCU_ERR_TIMEOUT);
-      break;
-    }
-    const uint32_t tile = stage_tile[s];
-    if (tile >= num_tiles) break;
-    const uint64_t tile_start = (uint64_t)tile * SCAN_TILE;
-    const uint64_t warp_start = tile_start + (uint64_t)warp * SCAN_WARP_ELEMS;
-    const bool full = tile_start + SCAN_TILE <= n;
-    uint4 *sb = buf + (size_t)s * (SCAN_TILE / 4) + warp * (SCAN_WARP_ELEMS / 4);
-
-    uint4 v[SCAN_VECS];
-    if (full) {
-#pragma unroll
-      for (int j = 0; j < SCAN_VECS; ++j) v[j] = sb[j * 32 + lane];
-    } else {
-#pragma unroll
-      for (int j = 0; j < SCAN_VECS; ++j) {
-        uint64_t e = warp_start + (uint64_t)(j * 32 + lane) * 4;
-        v[j].x = e + 0 < n ? in[e + 0] : 0u;
-        v[j].y = e + 1 < n ? in[e + 1] : 0u;
-        v[j].z = e + 2 < n ? in[e + 2] : 0u;
-        v[j].w = e + 3 < n ? in[e + 3] : 0u;
-      }
-    }
-    uint32_t pre[SCAN_VECS];
-    uint32_t carry = 0;
-#pragma unroll
-    for (int j = 0; j < SCAN_VECS; ++j) {
-      uint32_t sum = v[j].x + v[j].y + v[j].z + v[j].w;
-      uint32_t inc = warp_incl_scan(sum, lane);
-      pre[j] = carry + inc - sum;
-      carry += __shfl_sync(FULL_MASK, inc, 31);
-    }
-    if (lane == 0) s_warp[warp] = carry;
-    __syncthreads();
-    if (warp == 0) {
-      uint32_t wt = lane < SCAN_THREADS / 32 ? s_warp[lane] : 0u;
-      uint32_t wi = warp_incl_scan(wt, lane);
-      uint32_t agg = __shfl_sync(FULL_MASK, wi, SCAN_THREADS / 32 - 1);
-      if (lane < SCAN_THREADS / 32) s_warp[lane] = wi - wt;
-      uint32_t excl = 0;
-      bool ok = true;
-      if ((int64_t)tile == skip_tile) {
-        ok = false;  // fault injection: this tile never publishes
-      } else if (tile == 0) {
-        if (lane == 0) st_relaxed_u64(&status[0], ST_INC | agg);
-      } else {
-        if (lane == 0) st_relaxed_u64(&status[tile], ST_AGG | agg);
-        ok = scan_lookback(status, tile, lane, budget, excl);
-        if (lane == 0) st_relaxed_u64(&status[tile], ok ? (ST_INC | (uint32_t)(excl + agg)) : ST_POISON);
-      }
-      if (!ok && lane == 0) record_error(hdr, GPRTCU_ERR_TIMEOUT);
-      if (lane == 0) {
-        s_prefix = excl;
-        if (tile == num_tiles - 1) {
-          hdr->total = excl + agg;
-          if (d_total) *d_total = excl + agg;
-        }
-      }
-    }
-    __syncthreads();
-    const uint32_t base = s_prefix + s_warp[warp];
-#pragma unroll
-    for (int j = 0; j < SCAN_VECS; ++j) {
-      uint32_t p = base + pre[j];
-      uint4 o;
-      if (MODE == 0) {
-        o.x = p;
-        o.y = o.x + v[j].x;
-        o.z = o.y + v[j].y;
-        o.w = o.z + v[j].z;
-      } else {
-        o.x = p + v[j].x;
-        o.y = o.x + v[j].y;
-        o.z = o.y + v[j].z;
-        o.w = o.z + v[j].w;
-      }
-      if (full) {
-        sb[j * 32 + lane] = o;
-      } else {
-        uint64_t e = warp_start + (uint64_t)(j * 32 + lane) * 4;
-        if (e + 0 < n) out[e + 0] = o.x;
-        if (e + 1 < n) out[e + 1] = o.y;
-        if (e + 2 < n) out[e + 2] = o.z;
-        if (e + 3 < n) out[e + 3] = o.w;
-      }
-    }
-    if (full) fence_proxy_async_smem();
-    __syncthreads();
+  const uint64_t tile = s_tile;
+  const uint64_t tile_start = tile * SCAN_TILE;
+  const bool full = tile_start + SCAN_TILE <= n;
+  if (full) {
     if (tid == 0) {
-      if (full) bulk_s2g(out + tile_start, buf + (size_t)s * (SCAN_TILE / 4), PS_TILE_BYTES);
-      bulk_commit();
-      // The stage used one iteration ago is free once its store has read it.
-      if (k > 0) {
-        bulk_wait_read<1>();
-        issue((k + PS_STAGES - 1) % PS_STAGES);
+      mbar_arrive_expect_tx(&bar, (uint32_t)TS_SMEM);
+      bulk_g2s(buf, in + tile_start, (uint32_t)TS_SMEM, &bar);
+    }
+    if (!mbar_wait(&bar, 0, MBAR_WAIT_BUDGET)) s_abort = 1;
+  } else {
+    uint32_t *sb = reinterpret_cast<uint32_t *>(buf);
+    for (int i = tid; i < SCAN_TILE; i += TS_THREADS) sb[i] = tile_start + i < n ? in[tile_start + i] : 0u;
+  }
+  __syncthreads();
+  if (s_abort) {
+    if (tid == 0) record_error(hdr, GPRTCU_ERR_TIMEOUT);
+    return;
+  }
+  // Warp w owns rows [w*TS_ROWS, (w+1)*TS_ROWS); row r is 32 lanes x uint4.
+  uint4 *wb = buf + warp * TS_ROWS * 32;
+  uint32_t part = 0;
+#pragma unroll
+  for (int r = 0; r < TS_ROWS; ++r) {
+    const uint4 v = wb[r * 32 + lane];
+    part += v.x + v.y + v.z + v.w;
+  }
+  part = warp_sum(part);
+  if (lane == 0) s_warp[warp] = part;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t wt = lane < TS_WARPS ? s_warp[lane] : 0u;
+    const uint32_t wi = warp_incl_scan(wt, lane);
+    const uint32_t agg = __shfl_sync(FULL_MASK, wi, TS_WARPS - 1);
+    if (lane < TS_WARPS) s_warp[lane] = wi - wt;
+    uint32_t excl = 0;
+    bool ok = true;
+    if ((int64_t)tile == skip_tile) {
+      ok = false;  // fault injection: this tile never publishes
+    } else if (tile == 0) {
+      if (lane == 0) st_relaxed_u64(&status[0], ST_INC | agg);
+    } else {
+      if (lane == 0) st_relaxed_u64(&status[tile], ST_AGG | agg);
+      ok = scan_lookback128(status, tile, lane, budget, excl);
+      if (lane == 0) st_relaxed_u64(&status[tile], ok ? (ST_INC | (uint32_t)(excl + agg)) : ST_POISON);
+    }
+    if (!ok && lane == 0) record_error(hdr, GPRTCU_ERR_TIMEOUT);
+    if (lane == 0) {
+      s_prefix = excl;
+      if (tile == num_tiles - 1) {
+        hdr->total = excl + agg;
+        if (d_total) *d_total = excl + agg;
       }
     }
   }
-  if (tid == 0) bulk_wait<0>();
+  __syncthreads();
+  uint32_t carry = s_prefix + s_warp[warp];
+#pragma unroll 4
+  for (int r = 0; r < TS_ROWS; ++r) {
+    const uint4 v = wb[r * 32 + lane];
+    const uint32_t sum = v.x + v.y + v.z + v.w;
+    const uint32_t inc = warp_incl_scan(sum, lane);
+    const uint32_t p = carry + inc - sum;
+    uint4 o;
+    if (MODE == 0) {
+      o.x = p;
+      o.y = o.x + v.x;
+      o.z = o.y + v.y;
+      o.w = o.z + v.z;
+    } else {
+      o.x = p + v.x;
+      o.y = o.x + v.y;
+      o.z = o.y + v.z;
+      o.w = o.z + v.w;
+    }
+    wb[r * 32 + lane] = o;
+    carry += __shfl_sync(FULL_MASK, inc, 31);
+  }
+  if (full) {
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      bulk_s2g(out + tile_start, buf, (uint32_t)TS_SMEM);
+      bulk_commit();
+      bulk_wait_read<0>();  // shared memory must stay valid until the store has read it
+    }
+  } else {
+    __syncthreads();
+    const uint32_t *sb = reinterpret_cast<const uint32_t *>(buf);
+    for (int i = tid; i < SCAN_TILE; i += TS_THREADS)
+      if (tile_start + i < n) out[tile_start + i] = sb[i];
+  }
 }
 
 // Partition / select by sign (gprt/gprt_scan.slang:118-133,270-283;
@@ -450,7 +475,7 @@ using namespace gprtcu;
 
 static uint32_t g_spin_budget = DEFAULT_SPIN_BUDGET;
 static int64_t g_skip_tile = -1;
-// 0: persistent TMA-pipelined scan when aligned; 1: one-tile-per-CTA scan.
+// 0: TMA-staged tile-per-CTA scan when aligned; 1: register tile-per-CTA scan.
 static int g_scan_impl = 0;
 extern "C" GPRTCU_API void gprtcuDebugScanImpl(int impl) { g_scan_impl = impl; }
 
@@ -484,23 +509,13 @@ static gprtcuStatus scan_launch(const uint32_t *in, uint32_t *out, uint64_t n, i
   const bool vec = (((uintptr_t)in | (uintptr_t)out) & 15) == 0;
   const bool nc = (const void *)in != (const void *)out;
   if (vec && g_scan_impl == 0) {
-    // Persistent, TMA-pipelined kernel: as many CTAs as are co-resident.
-    static bool attr_set = false;
-    if (!attr_set) {
-      GPRTCU_TRY(cudaFuncSetAttribute(k_scan_pipe<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PS_SMEM));
-      GPRTCU_TRY(cudaFuncSetAttribute(k_scan_pipe<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PS_SMEM));
-      attr_set = true;
-    }
-    int per_sm = 0;
-    GPRTCU_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scan_pipe<0>, SCAN_THREADS, PS_SMEM));
-    uint64_t ctas = (uint64_t)gprtcu_num_sms() * (uint64_t)(per_sm > 0 ? per_sm : 1);
-    if (ctas > tiles) ctas = tiles;
+    // TMA-staged tile-per-CTA kernel (32 KB dynamic shared memory per CTA).
     if (inclusive)
-      k_scan_pipe<1><<<(unsigned)ctas, SCAN_THREADS, PS_SMEM, stream>>>(in, out, n, tiles, hdr, status, d_total,
-                                                                         g_spin_budget, g_skip_tile);
+      k_scan_tma<1><<<(unsigned)tiles, TS_THREADS, TS_SMEM, stream>>>(in, out, n, tiles, hdr, status, d_total,
+                                                                       g_spin_budget, g_skip_tile);
     else
-      k_scan_pipe<0><<<(unsigned)ctas, SCAN_THREADS, PS_SMEM, stream>>>(in, out, n, tiles, hdr, status, d_total,
-                                                                         g_spin_budget, g_skip_tile);
+      k_scan_tma<0><<<(unsigned)tiles, TS_THREADS, TS_SMEM, stream>>>(in, out, n, tiles, hdr, status, d_total,
+                                                                       g_spin_budget, g_skip_tile);
     GPRTCU_TRY(cudaGetLastError());
     return GPRTCU_OK;
   }

@@ -1,0 +1,167 @@
+// trace.cu -- closest-hit and any-hit traversal of the binary LBVH.
+//
+// One thread per ray, rays handed out to persistent warps in chunks of 32 by
+// an atomic counter (load balance across rays of very different cost).  Each
+// step loads one 64-byte node holding both child boxes, tests both boxes,
+// intersects leaf children on the spot (their triangles are stored in leaf
+// order), descends into the nearer inner child and pushes the farther one on
+// a per-thread stack of node indices.  A child is entered when its entry distance does
+// not exceed the best hit (equal distance still enters, so a tie can be won by
+// a lower primitive id).
+#include "common.cuh"
+#include "lbvh.cuh"
+#include "rtmath.cuh"
+
+namespace gprtcu {
+
+constexpr int kTraceThreads = 128;
+constexpr int kStack = 64;
+
+__device__ __forceinline__ void leaf_test(const float4 *leaf, uint32_t slot, const Ray &R, uint32_t &best,
+                                          uint32_t &best_slot, float &bt) {
+  const float4 a = __ldg(leaf + 3 * (size_t)slot), b = __ldg(leaf + 3 * (size_t)slot + 1),
+               c = __ldg(leaf + 3 * (size_t)slot + 2);
+  const float v0[3] = {a.x, a.y, a.z}, v1[3] = {b.x, b.y, b.z}, v2[3] = {c.x, c.y, c.z};
+  const uint32_t id = __float_as_uint(a.w);
+  float t;
+  if (isect_tri(R, v0, v1, v2, t)) {
+    if (best == kMiss || t < bt || (t == bt && id < best)) {
+      best = id;
+      best_slot = slot;
+      bt = t;
+    }
+  }
+}
+
+template <bool ANY>
+__device__ __forceinline__ void trace_one(const Bvh2Node *bvh, const float4 *leaf, uint32_t n, const float4 *rays,
+                                          uint64_t r, Hit *hits, uint32_t *err) {
+  const float4 ra = __ldg(rays + 2 * r), rb = __ldg(rays + 2 * r + 1);
+  Ray R;
+  ray_setup(ra, rb, R);
+  uint32_t best = kMiss, best_slot = 0;
+  float bt = R.tmax;
+  if (n == 1) {
+    const float4 a = __ldg(leaf), b = __ldg(leaf + 1), c = __ldg(leaf + 2);
+    float tn;
+    if (ray_box(R, fminf(a.x, fminf(b.x, c.x)), fminf(a.y, fminf(b.y, c.y)), fminf(a.z, fminf(b.z, c.z)),
+                fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y)), fmaxf(a.z, fmaxf(b.z, c.z)), bt, tn) &&
+        tn <= bt)
+      leaf_test(leaf, 0, R, best, best_slot, bt);
+  } else {
+    int st_node[kStack];  // inner nodes still to visit (4 B each: the hot top stays in L1)
+    int sp = 0;
+    int node = 0;
+    while (true) {
+      const float4 *np = reinterpret_cast<const float4 *>(bvh + node);
+      const float4 f0 = __ldg(np), f1 = __ldg(np + 1), f2 = __ldg(np + 2);
+      const int4 rf = __ldg(reinterpret_cast<const int4 *>(np + 3));
+      float tn0, tn1;
+      bool h0 = ray_box(R, f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, bt, tn0) && tn0 <= bt;
+      bool h1 = ray_box(R, f1.z, f1.w, f2.x, f2.y, f2.z, f2.w, bt, tn1) && tn1 <= bt;
+      if (h0 && rf.x < 0) {
+        leaf_test(leaf, (uint32_t)~rf.x, R, best, best_slot, bt);
+        h0 = false;
+        if (ANY && best != kMiss) break;
+      }
+      if (h1 && rf.y < 0) {
+        if (tn1 <= bt) leaf_test(leaf, (uint32_t)~rf.y, R, best, best_slot, bt);
+        h1 = false;
+        if (ANY && best != kMiss) break;
+      }
+      if (h1 && tn1 > bt) h1 = false;
+      if (h0 && h1) {
+        const bool first0 = tn0 <= tn1;
+        if (sp >= kStack) {
+          atomicCAS(err, 0u, 5u);  // traversal stack overflow
+          break;
+        }
+        st_node[sp] = first0 ? rf.y : rf.x;
+        ++sp;
+        node = first0 ? rf.x : rf.y;
+      } else if (h0) {
+        node = rf.x;
+      } else if (h1) {
+        node = rf.y;
+      } else {
+        if (sp == 0) break;
+        node = st_node[--sp];
+      }
+    }
+  }
+  Hit h;
+  h.prim = best;
+  h.t = __int_as_float(0x7f800000);
+  if (best != kMiss) {
+    const float4 a = __ldg(leaf + 3 * (size_t)best_slot), b = __ldg(leaf + 3 * (size_t)best_slot + 1),
+                 c = __ldg(leaf + 3 * (size_t)best_slot + 2);
+    const float v0[3] = {a.x, a.y, a.z}, v1[3] = {b.x, b.y, b.z}, v2[3] = {c.x, c.y, c.z};
+    h.t = refine_t(R, v0, v1, v2);
+  }
+  hits[r] = h;
+}
+
+template <bool ANY>
+__global__ void __launch_bounds__(kTraceThreads) k_trace_bin(const Bvh2Node *bvh, const float4 *leaf, uint32_t n,
+                                                            const float4 *rays, uint64_t nrays, Hit *hits,
+                                                            unsigned long long *counter, uint32_t *err) {
+  const int lane = threadIdx.x & 31;
+  while (true) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32ull);
+    base = __shfl_sync(FULL_MASK, base, 0);
+    if (base >= nrays) break;
+    const uint64_t r = base + lane;
+    if (r < nrays) trace_one<ANY>(bvh, leaf, n, rays, r, hits, err);
+  }
+}
+
+}  // namespace gprtcu
+
+using namespace gprtcu;
+
+namespace {
+
+gprtcuStatus trace_launch(const gprtcuLbvh *bvh, const float *rays, uint64_t nrays, gprtcuHit *hits, bool any,
+                          void *scratch, size_t scratch_bytes, cudaStream_t stream) {
+  if (!bvh || (!rays && nrays) || (!hits && nrays)) return GPRTCU_ERR_INVALID_ARG;
+  if (nrays == 0) return GPRTCU_OK;
+  if (bvh->numPrims == 0 || !bvh->leafTris || (bvh->numPrims > 1 && !bvh->bvh2)) return GPRTCU_ERR_INVALID_ARG;
+  if (((uintptr_t)rays & 15) || ((uintptr_t)bvh->leafTris & 15) || ((uintptr_t)bvh->bvh2 & 15))
+    return GPRTCU_ERR_INVALID_ARG;
+  if (!scratch || ((uintptr_t)scratch & 255)) return GPRTCU_ERR_INVALID_ARG;
+  if (scratch_bytes < sizeof(ScratchHeader)) return GPRTCU_ERR_SCRATCH_TOO_SMALL;
+  ScratchHeader *hdr = (ScratchHeader *)scratch;
+  unsigned long long *counter = reinterpret_cast<unsigned long long *>(&hdr->ticket[0]);
+  GPRTCU_TRY(cudaMemsetAsync(scratch, 0, sizeof(ScratchHeader), stream));
+  const int blocks = gprtcu_num_sms() * 8;
+  const uint64_t need = (nrays + kTraceThreads - 1) / kTraceThreads;
+  const int grid = (int)(need < (uint64_t)blocks ? need : blocks);
+  if (any)
+    k_trace_bin<true><<<grid, kTraceThreads, 0, stream>>>((const Bvh2Node *)bvh->bvh2, (const float4 *)bvh->leafTris,
+                                                          bvh->numPrims, (const float4 *)rays, nrays, (Hit *)hits,
+                                                          counter, &hdr->status);
+  else
+    k_trace_bin<false><<<grid, kTraceThreads, 0, stream>>>((const Bvh2Node *)bvh->bvh2,
+                                                           (const float4 *)bvh->leafTris, bvh->numPrims,
+                                                           (const float4 *)rays, nrays, (Hit *)hits, counter,
+                                                           &hdr->status);
+  GPRTCU_TRY(cudaGetLastError());
+  return GPRTCU_OK;
+}
+
+}  // namespace
+
+extern "C" GPRTCU_API size_t gprtcuTraceScratchSize(void) { return sizeof(ScratchHeader); }
+
+extern "C" GPRTCU_API gprtcuStatus gprtcuTraceClosest(const gprtcuLbvh *bvh, const float *rays, uint64_t numRays,
+                                                      gprtcuHit *hits, void *scratch, size_t scratchBytes,
+                                                      gprtcuStream stream) {
+  return trace_launch(bvh, rays, numRays, hits, false, scratch, scratchBytes, (cudaStream_t)stream);
+}
+
+extern "C" GPRTCU_API gprtcuStatus gprtcuTraceAny(const gprtcuLbvh *bvh, const float *rays, uint64_t numRays,
+                                                  gprtcuHit *hits, void *scratch, size_t scratchBytes,
+                                                  gprtcuStream stream) {
+  return trace_launch(bvh, rays, numRays, hits, true, scratch, scratchBytes, (cudaStream_t)stream);
+}

@@ -80,6 +80,98 @@ GPRTCU_API gprtcuStatus gprtcuSelectI32(const int32_t *in, int32_t *out, uint64_
                                         uint32_t *d_count, void *scratch, size_t scratchBytes, gprtcuStream stream);
 
 /* ------------------------------------------------------------------------
+ * Radix sort.  Replaces gprtBufferSort (gprt/gprt_host.h:2384) and
+ * gprtBufferSortPayload (gprt/gprt_host.h:2416); host driver
+ * gprt/gprt.cpp:8821-9073, kernels gprt/gprt_sort.slang:109-637.
+ * Stable ascending sort by the key bits [beginBit, endBit), in place: the
+ * result is in `keys` (and `values`) when the work completes, as in the
+ * reference.  The reference sorts 64-bit keys with 64-bit payloads over all
+ * 64 bits (gprt/gprt.cpp:8837,8966-8969); the 32-bit forms are what its
+ * typed shims and tests/t02-bufferSort use.  Key widths 4/8 bytes, payload
+ * widths 0/4/8 bytes.  Maximum n: 2^30 - 1.
+ * ------------------------------------------------------------------------ */
+GPRTCU_API size_t gprtcuSortScratchSize(uint64_t n, int keyBytes, int valueBytes);
+GPRTCU_API gprtcuStatus gprtcuSortKeysU32(uint32_t *keys, uint64_t n, int beginBit, int endBit, void *scratch,
+                                          size_t scratchBytes, gprtcuStream stream);
+GPRTCU_API gprtcuStatus gprtcuSortPairsU32(uint32_t *keys, uint32_t *values, uint64_t n, int beginBit, int endBit,
+                                           void *scratch, size_t scratchBytes, gprtcuStream stream);
+GPRTCU_API gprtcuStatus gprtcuSortKeysU64(uint64_t *keys, uint64_t n, int beginBit, int endBit, void *scratch,
+                                          size_t scratchBytes, gprtcuStream stream);
+GPRTCU_API gprtcuStatus gprtcuSortPairsU64(uint64_t *keys, uint32_t *values, uint64_t n, int beginBit, int endBit,
+                                           void *scratch, size_t scratchBytes, gprtcuStream stream);
+GPRTCU_API gprtcuStatus gprtcuSortPairsU64U64(uint64_t *keys, uint64_t *values, uint64_t n, int beginBit, int endBit,
+                                              void *scratch, size_t scratchBytes, gprtcuStream stream);
+
+/* ------------------------------------------------------------------------
+ * LBVH build.  Replaces gprtTriangleLBVHCreate / gprtPointsLBVHCreate +
+ * gprtLBVHBuild (gprt/development/gprt_lbvh.h:91-195; kernels
+ * gprt/development/gprt_lbvh.hlsl:188-428).  The caller owns every array of
+ * gprtcuLbvh; the build fills them (numPrims is set by the build):
+ *   codes       uint32[n]           sorted 30-bit codes
+ *   ids         uint32[n]           primitive id of leaf i (sorted order)
+ *   nodes       int32[2n-1][4]      {left,right,parent,leaf}; inner nodes
+ *                                   [0,n-1) with root 0, leaves [n-1,2n-1)
+ *   aabbs       float[2n-1][6]      {min.xyz,max.xyz} per node     (optional)
+ *   sceneBounds float[6]            scene box the codes were made in (opt.)
+ *   rootBox     float[6]            box of node 0                   (opt.)
+ *   bvh2        64 B x max(n-1,1)   traversal nodes: both child boxes and
+ *                                   child refs (needed by the traces)
+ *   leafTris    float[n][12]        leaf-order triangle vertices, w of the
+ *                                   first float4 = primitive id bits (needed
+ *                                   by the traces; triangles only)
+ * nodes, codes, ids and aabbs are bit-identical to the reference programs'
+ * output.  Either aabbs or bvh2 must be given.  codeKind: 0 Morton30
+ * (gprt/development/gprt_lbvh.hlsl:25-38), 1 Hilbert30 (gprt/hilbert.h:179-235).
+ * positions are float[3] per vertex (12-byte stride), triangles uint32[3].
+ * Maximum n: 2^30 - 1.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+  uint32_t numPrims;
+  uint32_t *codes;
+  uint32_t *ids;
+  int32_t *nodes;
+  float *aabbs;
+  float *sceneBounds;
+  float *rootBox;
+  void *bvh2;
+  void *leafTris;
+} gprtcuLbvh;
+
+GPRTCU_API size_t gprtcuLbvhScratchSize(uint32_t n);
+GPRTCU_API gprtcuStatus gprtcuLbvhBuildTriangles(const float *positions, const uint32_t *triangles,
+                                                 uint32_t numTriangles, int codeKind, gprtcuLbvh *bvh, void *scratch,
+                                                 size_t scratchBytes, gprtcuStream stream);
+GPRTCU_API gprtcuStatus gprtcuLbvhBuildPoints(const float *positions, uint32_t numPoints, int codeKind,
+                                              gprtcuLbvh *bvh, void *scratch, size_t scratchBytes,
+                                              gprtcuStream stream);
+
+/* ------------------------------------------------------------------------
+ * Trace.  Software replacement for the closest-hit / any-hit semantics of
+ * TraceRay (gprt/gprt_builtins.slang:105-124; RayDesc use
+ * samples/s2-hitPrograms/s2-0-triangles/deviceCode.slang:52-57), whose
+ * reference path is Vulkan hardware ray tracing (gprt/gprt.cpp:9404).
+ * rays: float[8] per ray {org.xyz, tmin, dir.xyz, tmax} (32 B, 16-B aligned).
+ * hits: {uint32 prim (0xFFFFFFFF = miss), float t} per ray.
+ * Closest hit: smallest fp32 watertight distance in [tmin, tmax], ties to the
+ * lowest primitive id; the reported t is the plane-equation distance of that
+ * triangle in double-float arithmetic, rounded once to fp32.
+ * Any hit: some triangle hit in [tmin, tmax] (prim) or a miss.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+  uint32_t prim;
+  float t;
+} gprtcuHit;
+
+/* scratch: at least gprtcuTraceScratchSize() bytes (the ray work counter and
+ * the status word; a stack overflow -- impossible for trees of depth <= 64,
+ * which 30-bit codes plus the index tie-break guarantee -- sets status 5). */
+GPRTCU_API size_t gprtcuTraceScratchSize(void);
+GPRTCU_API gprtcuStatus gprtcuTraceClosest(const gprtcuLbvh *bvh, const float *rays, uint64_t numRays,
+                                           gprtcuHit *hits, void *scratch, size_t scratchBytes, gprtcuStream stream);
+GPRTCU_API gprtcuStatus gprtcuTraceAny(const gprtcuLbvh *bvh, const float *rays, uint64_t numRays, gprtcuHit *hits,
+                                       void *scratch, size_t scratchBytes, gprtcuStream stream);
+
+/* ------------------------------------------------------------------------
  * Test hooks (fault injection without a GPU fault).  Process-wide settings
  * read at launch time by the look-back kernels.
  * gprtcuDebugSetSpinBudget: polls a look-back wait makes before it records
@@ -89,8 +181,8 @@ GPRTCU_API gprtcuStatus gprtcuSelectI32(const int32_t *in, int32_t *out, uint64_
  * ------------------------------------------------------------------------ */
 GPRTCU_API void gprtcuDebugSetSpinBudget(uint32_t polls);
 GPRTCU_API void gprtcuDebugScanSkipTile(int64_t tile);
-/* Scan kernel selection for tests: 0 = persistent TMA-pipelined kernel when
- * in/out are 16-byte aligned (default), 1 = one tile per CTA. */
+/* Scan kernel selection for tests: 0 = TMA-staged tile-per-CTA kernel when
+ * in/out are 16-byte aligned (default), 1 = register-staged tile per CTA. */
 GPRTCU_API void gprtcuDebugScanImpl(int impl);
 
 #ifdef __cplusplus

@@ -500,18 +500,24 @@ extern "C" double orc_t64(const float *ray, const float *v0, const float *v1, co
 // ray / box and traversal
 // ============================================================================
 // Slab test, Ize 2013: per-axis (b - o) * (1/d); NaN slabs (0 * inf, a ray in
-// a face plane) impose no bound because fmin/fmax return the other operand.
+// a face plane) impose no bound.
 // The entry is scaled down and the exit up by 2^-18 so that a triangle hit the
 // watertight test reports is never pruned by a box that contains it.
 static const float kBoxLo = 1.0f - 1.0f / 262144.0f;
 static const float kBoxHi = 1.0f + 1.0f / 262144.0f;
 
+// Per-axis min/max propagate NaN (a ray parallel to an axis lying in a face
+// plane gives 0 * inf); the accumulation below then drops that axis, so it
+// imposes no bound -- the conservative answer.
+static inline float nmin(float a, float b) { return (std::isnan(a) || std::isnan(b)) ? NAN : std::fmin(a, b); }
+static inline float nmax(float a, float b) { return (std::isnan(a) || std::isnan(b)) ? NAN : std::fmax(a, b); }
+
 static inline int ray_box(const RayPre &p, const float *b, float tmax, float *tnear_out) {
   float t0x = (b[0] - p.o[0]) * p.inv[0], t1x = (b[3] - p.o[0]) * p.inv[0];
   float t0y = (b[1] - p.o[1]) * p.inv[1], t1y = (b[4] - p.o[1]) * p.inv[1];
   float t0z = (b[2] - p.o[2]) * p.inv[2], t1z = (b[5] - p.o[2]) * p.inv[2];
-  float tn = std::fmax(std::fmax(std::fmin(t0x, t1x), std::fmin(t0y, t1y)), std::fmax(std::fmin(t0z, t1z), p.tmin));
-  float tf = std::fmin(std::fmin(std::fmax(t0x, t1x), std::fmax(t0y, t1y)), std::fmin(std::fmax(t0z, t1z), tmax));
+  float tn = std::fmax(std::fmax(nmin(t0x, t1x), nmin(t0y, t1y)), std::fmax(nmin(t0z, t1z), p.tmin));
+  float tf = std::fmin(std::fmin(nmax(t0x, t1x), nmax(t0y, t1y)), std::fmin(nmax(t0z, t1z), tmax));
   tn = tn * kBoxLo;
   tf = tf * kBoxHi;
   *tnear_out = tn;

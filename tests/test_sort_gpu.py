@@ -1,0 +1,150 @@
+"""Radix sort on the GPU through the C ABI, bit-exact against the oracle
+(std::stable_sort, the semantics of tests/t02-bufferSort's std::sort check)."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _zipf_u32(rng, n, s=1.1):
+    # rank r in [1, 2^32-1] by inverse-CDF of a continuous power law, key = r-1
+    u = rng.random(n)
+    r = np.floor((1 - u) ** (-1.0 / (s - 1.0)))
+    r = np.clip(r, 1, 2 ** 32 - 1)
+    return (r - 1).astype(np.uint64).astype(np.uint32)
+
+
+def _dists(rng, n, bits=32):
+    top = 2 ** bits
+    yield "uniform", rng.integers(0, top, size=n, dtype=np.uint64)
+    yield "equal", np.full(n, 12345 % top, np.uint64)
+    yield "sorted", np.sort(rng.integers(0, top, size=n, dtype=np.uint64))
+    yield "reverse", np.sort(rng.integers(0, top, size=n, dtype=np.uint64))[::-1].copy()
+    yield "fewdistinct", rng.choice(np.array([3, 77, 1 << (bits - 1), top - 1], np.uint64), size=n)
+
+
+def _sort_gpu(torch, keys_np, vals_np=None, begin=0, end=None):
+    from gprt_b200 import api
+    kt = torch.from_numpy(keys_np.view(np.int32 if keys_np.itemsize == 4 else np.int64).copy()).cuda()
+    vt = None
+    if vals_np is not None:
+        vt = torch.from_numpy(vals_np.view(np.int32 if vals_np.itemsize == 4 else np.int64).copy()).cuda()
+    api.sort(kt, vt, begin, end)
+    torch.cuda.synchronize()
+    k = kt.cpu().numpy().view(keys_np.dtype)
+    v = None if vt is None else vt.cpu().numpy().view(vals_np.dtype)
+    return k, v
+
+
+@pytest.mark.parametrize("n", [1, 2, 31, 32, 33, 4095, 4096, 4097, 8191, 8192, 8193, 100003, 1 << 20])
+def test_sort_pairs_u32_sizes(cuda, n):
+    import torch
+    rng = np.random.default_rng(n)
+    for name, k in _dists(rng, n):
+        k = k.astype(np.uint32)
+        v = np.arange(n, dtype=np.uint32)  # payload = original index: stability is visible
+        gk, gv = _sort_gpu(torch, k, v)
+        ek, ev = oracle.sort(k, v)
+        assert np.array_equal(gk, ek), (n, name)
+        assert np.array_equal(gv, ev), (n, name)
+
+
+def test_sort_keys_only_and_t02_shape(cuda):
+    import torch
+    rng = np.random.default_rng(7)
+    n = 3_000_017
+    k = rng.integers(0, 2 ** 32, size=n, dtype=np.uint64).astype(np.uint32)
+    gk, _ = _sort_gpu(torch, k)
+    assert np.array_equal(gk, np.sort(k))
+    # t02 key/value form: keys a shuffled permutation, values random
+    perm = rng.permutation(n).astype(np.uint32)
+    vals = rng.integers(0, 2 ** 32, size=n, dtype=np.uint64).astype(np.uint32)
+    gk, gv = _sort_gpu(torch, perm, vals)
+    order = np.argsort(perm, kind="stable")
+    assert np.array_equal(gk, perm[order]) and np.array_equal(gv, vals[order])
+
+
+def test_sort_zipf_pairs(cuda):
+    import torch
+    rng = np.random.default_rng(11)
+    n = 1 << 22
+    k = _zipf_u32(rng, n)
+    v = np.arange(n, dtype=np.uint32)
+    gk, gv = _sort_gpu(torch, k, v)
+    ek, ev = oracle.sort(k, v)
+    assert np.array_equal(gk, ek) and np.array_equal(gv, ev)
+
+
+def test_sort_bit_ranges(cuda):
+    import torch
+    rng = np.random.default_rng(5)
+    n = 200_001
+    k = rng.integers(0, 1 << 30, size=n, dtype=np.uint64).astype(np.uint32)  # Morton-like 30-bit
+    v = np.arange(n, dtype=np.uint32)
+    gk, gv = _sort_gpu(torch, k, v, 0, 30)
+    ek, ev = oracle.sort(k, v)
+    assert np.array_equal(gk, ek) and np.array_equal(gv, ev)
+    # a sub-range: stable sort by bits [8, 20) only
+    gk, gv = _sort_gpu(torch, k, v, 8, 20)
+    order = np.argsort((k >> 8) & 0xFFF, kind="stable")
+    assert np.array_equal(gk, k[order]) and np.array_equal(gv, v[order])
+
+
+@pytest.mark.parametrize("vw", [0, 4, 8])
+def test_sort_u64_keys(cuda, vw):
+    import torch
+    rng = np.random.default_rng(100 + vw)
+    for n in (1, 3, 4095, 4097, 65536 + 5, 1 << 20):
+        for name, k in _dists(rng, n, 64 if n < 70000 else 63):
+            v = None
+            if vw == 4:
+                v = np.arange(n, dtype=np.uint32)
+            elif vw == 8:
+                v = (np.arange(n, dtype=np.uint64) * np.uint64(0x9E3779B97F4A7C15))
+            gk, gv = _sort_gpu(torch, k, v)
+            if v is None:
+                assert np.array_equal(gk, np.sort(k)), (n, name)
+            else:
+                ek, ev = oracle.sort(k, v)
+                assert np.array_equal(gk, ek) and np.array_equal(gv, ev), (n, name)
+
+
+def test_sort_segmented_keys(cuda):
+    # meshID << 32 | morton30: the batched-build key (44 significant bits).
+    import torch
+    rng = np.random.default_rng(9)
+    n = 1_000_003
+    mesh = rng.integers(0, 4096, size=n, dtype=np.uint64)
+    code = rng.integers(0, 1 << 30, size=n, dtype=np.uint64)
+    k = (mesh << np.uint64(32)) | code
+    v = np.arange(n, dtype=np.uint32)
+    gk, gv = _sort_gpu(torch, k, v, 0, 44)
+    ek, ev = oracle.sort(k, v)
+    assert np.array_equal(gk, ek) and np.array_equal(gv, ev)
+
+
+def test_sort_golden_fixture(cuda):
+    import torch
+    g = np.load(os.path.join(GOLD, "sortscan.npz"))
+    gk, gv = _sort_gpu(torch, g["keys"], np.arange(g["keys"].size, dtype=np.uint32))
+    assert np.array_equal(gk, g["keys_sorted"]) and np.array_equal(gv, g["vals_sorted"])
+    gk, gv = _sort_gpu(torch, g["keys64"], np.arange(g["keys64"].size, dtype=np.uint32))
+    assert np.array_equal(gk, g["keys64_sorted"]) and np.array_equal(gv, g["vals64_sorted"])
+
+
+def test_sort_host_errors(cuda):
+    import torch
+    import gprt_b200
+    from gprt_b200 import api
+    L = gprt_b200.lib()
+    k = torch.zeros(100, dtype=torch.int32, device="cuda")
+    scr = api.scratch(16)
+    assert L.gprtcuSortKeysU32(api._ptr(k), 100, 0, 32, api._ptr(scr), scr.numel(), api._stream()) == 3
+    big = api.scratch(api.sort_scratch_size(100, 4, 0))
+    assert L.gprtcuSortKeysU32(api._ptr(k), 100, 0, 33, api._ptr(big), big.numel(), api._stream()) == 1
+    assert L.gprtcuSortKeysU32(api._ptr(k), 100, 5, 5, api._ptr(big), big.numel(), api._stream()) == 1
