@@ -33,74 +33,10 @@ __device__ __forceinline__ void leaf_test(const float4 *leaf, uint32_t slot, con
   }
 }
 
-template <bool ANY>
-__device__ __forceinline__ void trace_one(const Bvh2Node *bvh, const float4 *leaf, uint32_t n, const float4 *rays,
-                                          uint64_t r, Hit *hits, uint32_t *err) {
-  const float4 ra = __ldg(rays + 2 * r), rb = __ldg(rays + 2 * r + 1);
-  Ray R;
-  ray_setup(ra, rb, R);
-  uint32_t best = kMiss, best_slot = 0;
-  float bt = R.tmax;
-  if (n == 1) {
-    const float4 a = __ldg(leaf), b = __ldg(leaf + 1), c = __ldg(leaf + 2);
-    float tn;
-    if (ray_box(R, fminf(a.x, fminf(b.x, c.x)), fminf(a.y, fminf(b.y, c.y)), fminf(a.z, fminf(b.z, c.z)),
-                fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y)), fmaxf(a.z, fmaxf(b.z, c.z)), bt, tn) &&
-        tn <= bt)
-      leaf_test(leaf, 0, R, best, best_slot, bt);
-  } else {
-    int st_node[kStack];  // inner nodes still to visit (4 B each: the hot top stays in L1)
-    int sp = 0;
-    int node = 0;
-    while (true) {
-      const float4 *np = reinterpret_cast<const float4 *>(bvh + node);
-      const float4 f0 = __ldg(np), f1 = __ldg(np + 1), f2 = __ldg(np + 2);
-      const int4 rf = __ldg(reinterpret_cast<const int4 *>(np + 3));
-      float tn0, tn1;
-      bool h0 = ray_box(R, f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, bt, tn0) && tn0 <= bt;
-      bool h1 = ray_box(R, f1.z, f1.w, f2.x, f2.y, f2.z, f2.w, bt, tn1) && tn1 <= bt;
-      if (h0 && rf.x < 0) {
-        leaf_test(leaf, (uint32_t)~rf.x, R, best, best_slot, bt);
-        h0 = false;
-        if (ANY && best != kMiss) break;
-      }
-      if (h1 && rf.y < 0) {
-        if (tn1 <= bt) leaf_test(leaf, (uint32_t)~rf.y, R, best, best_slot, bt);
-        h1 = false;
-        if (ANY && best != kMiss) break;
-      }
-      if (h1 && tn1 > bt) h1 = false;
-      if (h0 && h1) {
-        const bool first0 = tn0 <= tn1;
-        if (sp >= kStack) {
-          atomicCAS(err, 0u, 5u);  // traversal stack overflow
-          break;
-        }
-        st_node[sp] = first0 ? rf.y : rf.x;
-        ++sp;
-        node = first0 ? rf.x : rf.y;
-      } else if (h0) {
-        node = rf.x;
-      } else if (h1) {
-        node = rf.y;
-      } else {
-        if (sp == 0) break;
-        node = st_node[--sp];
-      }
-    }
-  }
-  Hit h;
-  h.prim = best;
-  h.t = __int_as_float(0x7f800000);
-  if (best != kMiss) {
-    const float4 a = __ldg(leaf + 3 * (size_t)best_slot), b = __ldg(leaf + 3 * (size_t)best_slot + 1),
-                 c = __ldg(leaf + 3 * (size_t)best_slot + 2);
-    const float v0[3] = {a.x, a.y, a.z}, v1[3] = {b.x, b.y, b.z}, v2[3] = {c.x, c.y, c.z};
-    h.t = refine_t(R, v0, v1, v2);
-  }
-  hits[r] = h;
-}
-
+// One warp traces 32 rays; the loop over node visits is warp-uniform (a lane
+// that has finished idles until the warp's last ray is done), so the lanes
+// re-converge at every visit.  A loop with per-lane exits lets the lanes drift
+// apart and run one at a time.
 template <bool ANY>
 __global__ void __launch_bounds__(kTraceThreads) k_trace_bin(const Bvh2Node *bvh, const float4 *leaf, uint32_t n,
                                                             const float4 *rays, uint64_t nrays, Hit *hits,
@@ -112,7 +48,78 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace_bin(const Bvh2Node *bvh
     base = __shfl_sync(FULL_MASK, base, 0);
     if (base >= nrays) break;
     const uint64_t r = base + lane;
-    if (r < nrays) trace_one<ANY>(bvh, leaf, n, rays, r, hits, err);
+    const bool active = r < nrays;
+    Ray R;
+    ray_setup(active ? __ldg(rays + 2 * r) : make_float4(0.f, 0.f, 0.f, 1.f),
+              active ? __ldg(rays + 2 * r + 1) : make_float4(1.f, 0.f, 0.f, 0.f), R);
+    uint32_t best = kMiss, best_slot = 0;
+    float bt = R.tmax;
+    bool done = !active;
+    int st_node[kStack];  // inner nodes still to visit (4 B each: the hot top stays in L1)
+    int sp = 0;
+    int node = 0;
+    if (n == 1) {
+      if (active) {
+        const float4 a = __ldg(leaf), b = __ldg(leaf + 1), c = __ldg(leaf + 2);
+        float tn;
+        if (ray_box(R, fminf(a.x, fminf(b.x, c.x)), fminf(a.y, fminf(b.y, c.y)), fminf(a.z, fminf(b.z, c.z)),
+                    fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y)), fmaxf(a.z, fmaxf(b.z, c.z)), bt, tn) &&
+            tn <= bt)
+          leaf_test(leaf, 0, R, best, best_slot, bt);
+      }
+      done = true;
+    }
+    while (__any_sync(FULL_MASK, !done)) {
+      if (!done) {
+        const float4 *np = reinterpret_cast<const float4 *>(bvh + node);
+        const float4 f0 = __ldg(np), f1 = __ldg(np + 1), f2 = __ldg(np + 2);
+        const int4 rf = __ldg(reinterpret_cast<const int4 *>(np + 3));
+        float tn0, tn1;
+        bool h0 = ray_box(R, f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, bt, tn0) && tn0 <= bt;
+        bool h1 = ray_box(R, f1.z, f1.w, f2.x, f2.y, f2.z, f2.w, bt, tn1) && tn1 <= bt;
+        if (h0 && rf.x < 0) {
+          leaf_test(leaf, (uint32_t)~rf.x, R, best, best_slot, bt);
+          h0 = false;
+        }
+        if (h1 && rf.y < 0) {
+          if (tn1 <= bt) leaf_test(leaf, (uint32_t)~rf.y, R, best, best_slot, bt);
+          h1 = false;
+        }
+        if (h1 && tn1 > bt) h1 = false;
+        if (ANY && best != kMiss) {
+          done = true;
+        } else if (h0 && h1) {
+          const bool first0 = tn0 <= tn1;
+          if (sp < kStack) {
+            st_node[sp++] = first0 ? rf.y : rf.x;
+            node = first0 ? rf.x : rf.y;
+          } else {
+            atomicCAS(err, 0u, 5u);  // traversal stack overflow
+            done = true;
+          }
+        } else if (h0) {
+          node = rf.x;
+        } else if (h1) {
+          node = rf.y;
+        } else if (sp > 0) {
+          node = st_node[--sp];
+        } else {
+          done = true;
+        }
+      }
+    }
+    if (active) {
+      Hit h;
+      h.prim = best;
+      h.t = __int_as_float(0x7f800000);
+      if (best != kMiss) {
+        const float4 a = __ldg(leaf + 3 * (size_t)best_slot), b = __ldg(leaf + 3 * (size_t)best_slot + 1),
+                     c = __ldg(leaf + 3 * (size_t)best_slot + 2);
+        const float v0[3] = {a.x, a.y, a.z}, v1[3] = {b.x, b.y, b.z}, v2[3] = {c.x, c.y, c.z};
+        h.t = refine_t(R, v0, v1, v2);
+      }
+      hits[r] = h;
+    }
   }
 }
 
@@ -134,7 +141,7 @@ gprtcuStatus trace_launch(const gprtcuLbvh *bvh, const float *rays, uint64_t nra
   ScratchHeader *hdr = (ScratchHeader *)scratch;
   unsigned long long *counter = reinterpret_cast<unsigned long long *>(&hdr->ticket[0]);
   GPRTCU_TRY(cudaMemsetAsync(scratch, 0, sizeof(ScratchHeader), stream));
-  const int blocks = gprtcu_num_sms() * 8;
+  const int blocks = gprtcu_num_sms() * 10;  // 48 registers: 10 CTAs of 128 threads per SM
   const uint64_t need = (nrays + kTraceThreads - 1) / kTraceThreads;
   const int grid = (int)(need < (uint64_t)blocks ? need : blocks);
   if (any)
