@@ -16,6 +16,7 @@ SIGNATURES = {
     "gprtcuScanScratchSize": ([u64], sz),
     "gprtcuExclusiveSumU32": ([vp, vp, u64, vp, vp, sz, vp], st),
     "gprtcuInclusiveSumU32": ([vp, vp, u64, vp, vp, sz, vp], st),
+    "gprtcuExclusiveSumU32NoAlloc": ([vp, vp, u64, vp, vp], st),
     "gprtcuPartitionI32": ([vp, vp, u64, i32, vp, vp, sz, vp], st),
     "gprtcuSelectI32": ([vp, vp, u64, i32, vp, vp, sz, vp], st),
     "gprtcuSortScratchSize": ([u64, i32, i32], sz),

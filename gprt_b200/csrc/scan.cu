@@ -587,3 +587,65 @@ extern "C" GPRTCU_API gprtcuStatus gprtcuSelectI32(const int32_t *in, int32_t *o
                                                    gprtcuStream stream) {
   return partition_launch(in, out, n, selectPositive, 0, d_count, scratch, scratchBytes, (cudaStream_t)stream);
 }
+
+// ---------------------------------------------------------------------------
+// Exclusive sum that allocates nothing and takes no scratch argument.
+//
+// Some callers cannot allocate device memory for work space: a host
+// application that owns the whole device-memory budget and lends this library
+// only the input and output buffers (an engine that allocates everything up
+// front and forbids allocation while a frame is in flight, for instance), or a
+// foreign-language binding that has no way to keep a device allocation alive
+// between calls.  For them, gprtcuExclusiveSumU32NoAlloc keeps the look-back
+// state (the 256-byte header plus one 8-byte status word per 8192-element
+// tile) in the fixed array below, compiled into the library.
+//
+// * Size limit: n <= 2^28 (268,435,456) elements, which needs 262,400 bytes;
+//   larger n returns GPRTCU_ERR_TOO_LARGE.  Every GPU that loads the library
+//   holds these bytes until the process exits.
+// * Set-up: host code cannot use the array's name as a device address, so the
+//   first call on each device (with that device current) looks the address
+//   up with cudaGetSymbolAddress and caches it.  Make that first call before
+//   any stream capture on the device.
+// * Sharing: every call uses the same array.  Each call clears the part it
+//   uses (cudaMemsetAsync, which allocates nothing) before its kernel runs,
+//   so calls ordered on one stream are safe; calls whose work overlaps on the
+//   GPU (different streams, no ordering between them) race on the array and
+//   give wrong results.
+// * No cudaMalloc, cudaFree or allocating library routine is called.
+// ---------------------------------------------------------------------------
+static const uint64_t kNoAllocMaxN = 1ull << 28;
+static const size_t kNoAllocBytes = sizeof(ScratchHeader) + ((kNoAllocMaxN + SCAN_TILE - 1) / SCAN_TILE) * 8;
+static __device__ __align__(256) unsigned char g_scan_noalloc_state[kNoAllocBytes];
+
+#include <mutex>
+
+static void *noalloc_state_ptr(gprtcuStatus &st) {
+  static std::mutex mu;
+  static void *ptrs[64] = {nullptr};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    st = GPRTCU_ERR_CUDA;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!ptrs[dev]) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_scan_noalloc_state) != cudaSuccess || !p) {
+      st = GPRTCU_ERR_CUDA;
+      return nullptr;
+    }
+    ptrs[dev] = p;
+  }
+  st = GPRTCU_OK;
+  return ptrs[dev];
+}
+
+extern "C" GPRTCU_API gprtcuStatus gprtcuExclusiveSumU32NoAlloc(const uint32_t *in, uint32_t *out, uint64_t n,
+                                                                uint32_t *d_total, gprtcuStream stream) {
+  if (n > kNoAllocMaxN) return GPRTCU_ERR_TOO_LARGE;
+  gprtcuStatus st;
+  void *state = noalloc_state_ptr(st);
+  if (!state) return st;
+  return scan_launch(in, out, n, 0, d_total, state, kNoAllocBytes, (cudaStream_t)stream);
+}

@@ -66,6 +66,21 @@ GPRTCU_API gprtcuStatus gprtcuExclusiveSumU32(const uint32_t *in, uint32_t *out,
 GPRTCU_API gprtcuStatus gprtcuInclusiveSumU32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *d_total,
                                               void *scratch, size_t scratchBytes, gprtcuStream stream);
 
+/* Exclusive sum that allocates nothing and takes no scratch argument.  No
+ * counterpart in the reference: it is for callers that cannot allocate device
+ * work space -- a host application that owns the whole device-memory budget
+ * and lends this library only the input and output buffers, or a foreign-
+ * language binding that cannot keep a device allocation alive between calls.
+ * Same results as gprtcuExclusiveSumU32.  The look-back state lives in a
+ * fixed 262,400-byte array inside the library (held on every GPU that loads
+ * it until the process exits), so n is limited to 2^28 elements; larger n
+ * returns GPRTCU_ERR_TOO_LARGE.  The first call on a device resolves the
+ * array's device address (make it before any stream capture on that device).
+ * All calls share the array: calls ordered on one stream are fine, calls that
+ * overlap on the GPU race and give wrong results. */
+GPRTCU_API gprtcuStatus gprtcuExclusiveSumU32NoAlloc(const uint32_t *in, uint32_t *out, uint64_t n,
+                                                     uint32_t *d_total, gprtcuStream stream);
+
 /* Partition / select by sign.  Replaces gprtBufferPartition
  * (gprt/gprt_host.h:2295) and gprtBufferSelect (:2344); kernel modes
  * gprt/gprt_scan.slang:118-133,270-283.  Selected items (sign bit clear when
