@@ -60,109 +60,6 @@ __device__ __forceinline__ bool scan_lookback(const uint64_t *status, uint64_t t
   return true;
 }
 
-// MODE: 0 exclusive, 1 inclusive.  VEC: input/output 16-byte aligned.
-// NC: input does not alias output (read through the non-coherent path).
-template <int MODE, bool VEC, bool NC>
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_u32(const uint32_t *__restrict__ in, uint32_t *out, uint64_t n,
-                                                          uint64_t num_tiles, ScratchHeader *hdr, uint64_t *status,
-                                                          uint32_t *d_total, uint32_t budget, int64_t skip_tile) {
-  __shared__ uint32_t s_tile;
-  __shared__ uint32_t s_warp[SCAN_THREADS / 32];
-  __shared__ uint32_t s_prefix;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (tid == 0) s_tile = atomicAdd(&hdr->ticket[0], 1u);
-  __syncthreads();
-  const uint64_t tile = s_tile;
-  const uint64_t warp_start = tile * SCAN_TILE + (uint64_t)warp * SCAN_WARP_ELEMS;
-  const bool full = VEC && (tile + 1) * SCAN_TILE <= n;
-
-  uint4 v[SCAN_VECS];
-  if (full) {
-    const uint4 *src = reinterpret_cast<const uint4 *>(in + warp_start);
-#pragma unroll
-    for (int j = 0; j < SCAN_VECS; ++j) v[j] = NC ? ldg_stream(src + j * 32 + lane) : ldg_coherent(src + j * 32 + lane);
-  } else {
-#pragma unroll
-    for (int j = 0; j < SCAN_VECS; ++j) {
-      uint64_t e = warp_start + (uint64_t)(j * 32 + lane) * 4;
-      v[j].x = e + 0 < n ? in[e + 0] : 0u;
-      v[j].y = e + 1 < n ? in[e + 1] : 0u;
-      v[j].z = e + 2 < n ? in[e + 2] : 0u;
-      v[j].w = e + 3 < n ? in[e + 3] : 0u;
-    }
-  }
-
-  // Position order inside a warp is (j, lane, component): scan each 128-
-  // element row j across lanes and carry row totals forward.
-  uint32_t pre[SCAN_VECS];
-  uint32_t carry = 0;
-#pragma unroll
-  for (int j = 0; j < SCAN_VECS; ++j) {
-    uint32_t s = v[j].x + v[j].y + v[j].z + v[j].w;
-    uint32_t inc = warp_incl_scan(s, lane);
-    pre[j] = carry + inc - s;
-    carry += __shfl_sync(FULL_MASK, inc, 31);
-  }
-  if (lane == 0) s_warp[warp] = carry;
-  __syncthreads();
-
-  if (warp == 0) {
-    uint32_t wt = lane < SCAN_THREADS / 32 ? s_warp[lane] : 0u;
-    uint32_t wi = warp_incl_scan(wt, lane);
-    uint32_t agg = __shfl_sync(FULL_MASK, wi, SCAN_THREADS / 32 - 1);
-    if (lane < SCAN_THREADS / 32) s_warp[lane] = wi - wt;
-    uint32_t excl = 0;
-    bool ok = true;
-    if ((int64_t)tile == skip_tile) {
-      // Fault injection for tests: this tile never publishes.
-      ok = false;
-    } else if (tile == 0) {
-      if (lane == 0) st_relaxed_u64(&status[0], ST_INC | agg);
-    } else {
-      if (lane == 0) st_relaxed_u64(&status[tile], ST_AGG | agg);
-      ok = scan_lookback(status, tile, lane, budget, excl);
-      if (lane == 0) st_relaxed_u64(&status[tile], ok ? (ST_INC | (uint32_t)(excl + agg)) : ST_POISON);
-    }
-    if (!ok && lane == 0) record_error(hdr, GPRTCU_ERR_TIMEOUT);
-    if (lane == 0) {
-      s_prefix = excl;
-      if (tile == num_tiles - 1) {
-        hdr->total = excl + agg;
-        if (d_total) *d_total = excl + agg;
-      }
-    }
-  }
-  __syncthreads();
-
-  const uint32_t base = s_prefix + s_warp[warp];
-#pragma unroll
-  for (int j = 0; j < SCAN_VECS; ++j) {
-    uint32_t p = base + pre[j];
-    uint4 o;
-    if (MODE == 0) {
-      o.x = p;
-      o.y = o.x + v[j].x;
-      o.z = o.y + v[j].y;
-      o.w = o.z + v[j].z;
-    } else {
-      o.x = p + v[j].x;
-      o.y = o.x + v[j].y;
-      o.z = o.y + v[j].z;
-      o.w = o.z + v[j].w;
-    }
-    if (full) {
-      stg_v4(reinterpret_cast<uint4 *>(out + warp_start) + j * 32 + lane, o);
-    } else {
-      uint64_t e = warp_start + (uint64_t)(j * 32 + lane) * 4;
-      if (e + 0 < n) out[e + 0] = o.x;
-      if (e + 1 < n) out[e + 1] = o.y;
-      if (e + 2 < n) out[e + 2] = o.z;
-      if (e + 3 < n) out[e + 3] = o.w;
-    }
-  }
-}
-
-
 // Look-back over 128 predecessors per probe (4 status words per lane, lane
 // l covering tiles base-4l .. base-4l-3, nearest first).  The inclusive
 // prefix can only travel as fast as one probe window per L2 round trip, so a
@@ -220,6 +117,114 @@ __device__ __forceinline__ bool scan_lookback128(const uint64_t *status, uint64_
   return true;
 }
 
+// Register-staged tile per CTA.  MODE: 0 exclusive, 1 inclusive.  VEC:
+// input/output 16-byte aligned.  NC: input does not alias output (read
+// through the non-coherent path).  THREADS x VECS uint4 per tile; LBW is the
+// look-back window (32 or 128 predecessors per probe).
+template <int MODE, bool VEC, bool NC, int THREADS, int VECS, int LBW>
+__global__ void __launch_bounds__(THREADS) k_scan_u32(const uint32_t *__restrict__ in, uint32_t *out, uint64_t n,
+                                                          uint64_t num_tiles, ScratchHeader *hdr, uint64_t *status,
+                                                          uint32_t *d_total, uint32_t budget, int64_t skip_tile) {
+  constexpr int WARP_ELEMS = VECS * 4 * 32;
+  constexpr int TILE = WARP_ELEMS * (THREADS / 32);
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_warp[THREADS / 32];
+  __shared__ uint32_t s_prefix;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_tile = atomicAdd(&hdr->ticket[0], 1u);
+  __syncthreads();
+  const uint64_t tile = s_tile;
+  const uint64_t warp_start = tile * TILE + (uint64_t)warp * WARP_ELEMS;
+  const bool full = VEC && (tile + 1) * TILE <= n;
+
+  uint4 v[VECS];
+  if (full) {
+    const uint4 *src = reinterpret_cast<const uint4 *>(in + warp_start);
+#pragma unroll
+    for (int j = 0; j < VECS; ++j) v[j] = NC ? ldg_stream(src + j * 32 + lane) : ldg_coherent(src + j * 32 + lane);
+  } else {
+#pragma unroll
+    for (int j = 0; j < VECS; ++j) {
+      uint64_t e = warp_start + (uint64_t)(j * 32 + lane) * 4;
+      v[j].x = e + 0 < n ? in[e + 0] : 0u;
+      v[j].y = e + 1 < n ? in[e + 1] : 0u;
+      v[j].z = e + 2 < n ? in[e + 2] : 0u;
+      v[j].w = e + 3 < n ? in[e + 3] : 0u;
+    }
+  }
+
+  // Position order inside a warp is (j, lane, component): scan each 128-
+  // element row j across lanes and carry row totals forward.
+  uint32_t pre[VECS];
+  uint32_t carry = 0;
+#pragma unroll
+  for (int j = 0; j < VECS; ++j) {
+    uint32_t s = v[j].x + v[j].y + v[j].z + v[j].w;
+    uint32_t inc = warp_incl_scan(s, lane);
+    pre[j] = carry + inc - s;
+    carry += __shfl_sync(FULL_MASK, inc, 31);
+  }
+  if (lane == 0) s_warp[warp] = carry;
+  __syncthreads();
+
+  if (warp == 0) {
+    uint32_t wt = lane < THREADS / 32 ? s_warp[lane] : 0u;
+    uint32_t wi = warp_incl_scan(wt, lane);
+    uint32_t agg = __shfl_sync(FULL_MASK, wi, THREADS / 32 - 1);
+    if (lane < THREADS / 32) s_warp[lane] = wi - wt;
+    uint32_t excl = 0;
+    bool ok = true;
+    if ((int64_t)tile == skip_tile) {
+      // Fault injection for tests: this tile never publishes.
+      ok = false;
+    } else if (tile == 0) {
+      if (lane == 0) st_relaxed_u64(&status[0], ST_INC | agg);
+    } else {
+      if (lane == 0) st_relaxed_u64(&status[tile], ST_AGG | agg);
+      ok = LBW == 128 ? scan_lookback128(status, tile, lane, budget, excl)
+                      : scan_lookback(status, tile, lane, budget, excl);
+      if (lane == 0) st_relaxed_u64(&status[tile], ok ? (ST_INC | (uint32_t)(excl + agg)) : ST_POISON);
+    }
+    if (!ok && lane == 0) record_error(hdr, GPRTCU_ERR_TIMEOUT);
+    if (lane == 0) {
+      s_prefix = excl;
+      if (tile == num_tiles - 1) {
+        hdr->total = excl + agg;
+        if (d_total) *d_total = excl + agg;
+      }
+    }
+  }
+  __syncthreads();
+
+  const uint32_t base = s_prefix + s_warp[warp];
+#pragma unroll
+  for (int j = 0; j < VECS; ++j) {
+    uint32_t p = base + pre[j];
+    uint4 o;
+    if (MODE == 0) {
+      o.x = p;
+      o.y = o.x + v[j].x;
+      o.z = o.y + v[j].y;
+      o.w = o.z + v[j].z;
+    } else {
+      o.x = p + v[j].x;
+      o.y = o.x + v[j].y;
+      o.z = o.y + v[j].z;
+      o.w = o.z + v[j].w;
+    }
+    if (full) {
+      stg_v4(reinterpret_cast<uint4 *>(out + warp_start) + j * 32 + lane, o);
+    } else {
+      uint64_t e = warp_start + (uint64_t)(j * 32 + lane) * 4;
+      if (e + 0 < n) out[e + 0] = o.x;
+      if (e + 1 < n) out[e + 1] = o.y;
+      if (e + 2 < n) out[e + 2] = o.z;
+      if (e + 3 < n) out[e + 3] = o.w;
+    }
+  }
+}
+
+
 // Tile-per-CTA scan with TMA staging (16-byte aligned in/out).  A 128-thread
 // CTA owns one 8192-element tile: thread 0 takes a ticket and brings the
 // whole 32 KB tile into shared memory with one bulk async copy; the four warps
@@ -230,38 +235,43 @@ __device__ __forceinline__ bool scan_lookback128(const uint64_t *status, uint64_
 // other tiles wait on their look-back.
 constexpr int TS_THREADS = 128;
 constexpr int TS_WARPS = TS_THREADS / 32;
-constexpr int TS_ROWS = SCAN_TILE / (TS_WARPS * 128);  // 16 rows of 128 elements per warp
+constexpr int TS_ROWS = 16;  // rows of 128 elements per warp
 constexpr size_t TS_SMEM = (size_t)SCAN_TILE * 4;
 
-template <int MODE>
-__global__ void __launch_bounds__(TS_THREADS) k_scan_tma(const uint32_t *in, uint32_t *out, uint64_t n,
+// WARPS x 16 rows x 128 elements per tile.  TICKET: tile order from an atomic
+// ticket (dispatch-order independent) or from blockIdx.x.
+template <int MODE, int WARPS = 4, bool TICKET = true>
+__global__ void __launch_bounds__(WARPS * 32) k_scan_tma(const uint32_t *in, uint32_t *out, uint64_t n,
                                                         uint64_t num_tiles, ScratchHeader *hdr, uint64_t *status,
                                                         uint32_t *d_total, uint32_t budget, int64_t skip_tile) {
+  constexpr int THREADS = WARPS * 32;
+  constexpr int TILE = WARPS * TS_ROWS * 128;
+  constexpr uint32_t TILE_BYTES = TILE * 4;
   extern __shared__ __align__(128) unsigned char smem[];
   uint4 *buf = reinterpret_cast<uint4 *>(smem);
   __shared__ uint64_t bar;
   __shared__ uint32_t s_tile, s_abort, s_prefix;
-  __shared__ uint32_t s_warp[TS_WARPS];
+  __shared__ uint32_t s_warp[WARPS];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) {
-    s_tile = atomicAdd(&hdr->ticket[0], 1u);
+    s_tile = TICKET ? atomicAdd(&hdr->ticket[0], 1u) : blockIdx.x;
     s_abort = 0;
     mbar_init(&bar, 1);
     fence_mbar_init();
   }
   __syncthreads();
   const uint64_t tile = s_tile;
-  const uint64_t tile_start = tile * SCAN_TILE;
-  const bool full = tile_start + SCAN_TILE <= n;
+  const uint64_t tile_start = tile * TILE;
+  const bool full = tile_start + TILE <= n;
   if (full) {
     if (tid == 0) {
-      mbar_arrive_expect_tx(&bar, (uint32_t)TS_SMEM);
-      bulk_g2s(buf, in + tile_start, (uint32_t)TS_SMEM, &bar);
+      mbar_arrive_expect_tx(&bar, TILE_BYTES);
+      bulk_g2s(buf, in + tile_start, TILE_BYTES, &bar);
     }
     if (!mbar_wait(&bar, 0, MBAR_WAIT_BUDGET)) s_abort = 1;
   } else {
     uint32_t *sb = reinterpret_cast<uint32_t *>(buf);
-    for (int i = tid; i < SCAN_TILE; i += TS_THREADS) sb[i] = tile_start + i < n ? in[tile_start + i] : 0u;
+    for (int i = tid; i < TILE; i += THREADS) sb[i] = tile_start + i < n ? in[tile_start + i] : 0u;
   }
   __syncthreads();
   if (s_abort) {
@@ -280,10 +290,10 @@ __global__ void __launch_bounds__(TS_THREADS) k_scan_tma(const uint32_t *in, uin
   if (lane == 0) s_warp[warp] = part;
   __syncthreads();
   if (warp == 0) {
-    const uint32_t wt = lane < TS_WARPS ? s_warp[lane] : 0u;
+    const uint32_t wt = lane < WARPS ? s_warp[lane] : 0u;
     const uint32_t wi = warp_incl_scan(wt, lane);
-    const uint32_t agg = __shfl_sync(FULL_MASK, wi, TS_WARPS - 1);
-    if (lane < TS_WARPS) s_warp[lane] = wi - wt;
+    const uint32_t agg = __shfl_sync(FULL_MASK, wi, WARPS - 1);
+    if (lane < WARPS) s_warp[lane] = wi - wt;
     uint32_t excl = 0;
     bool ok = true;
     if ((int64_t)tile == skip_tile) {
@@ -331,17 +341,18 @@ __global__ void __launch_bounds__(TS_THREADS) k_scan_tma(const uint32_t *in, uin
     fence_proxy_async_smem();
     __syncthreads();
     if (tid == 0) {
-      bulk_s2g(out + tile_start, buf, (uint32_t)TS_SMEM);
+      bulk_s2g(out + tile_start, buf, TILE_BYTES);
       bulk_commit();
       bulk_wait_read<0>();  // shared memory must stay valid until the store has read it
     }
   } else {
     __syncthreads();
     const uint32_t *sb = reinterpret_cast<const uint32_t *>(buf);
-    for (int i = tid; i < SCAN_TILE; i += TS_THREADS)
+    for (int i = tid; i < TILE; i += THREADS)
       if (tile_start + i < n) out[tile_start + i] = sb[i];
   }
 }
+
 
 // Partition / select by sign (gprt/gprt_scan.slang:118-133,270-283;
 // known-answer layout tests/t03-bufferScans/hostCode.cpp:98-160,172-241).
@@ -479,6 +490,7 @@ static int64_t g_skip_tile = -1;
 static int g_scan_impl = 0;
 extern "C" GPRTCU_API void gprtcuDebugScanImpl(int impl) { g_scan_impl = impl; }
 
+
 extern "C" GPRTCU_API void gprtcuDebugSetSpinBudget(uint32_t polls) { g_spin_budget = polls ? polls : DEFAULT_SPIN_BUDGET; }
 extern "C" GPRTCU_API void gprtcuDebugScanSkipTile(int64_t tile) { g_skip_tile = tile; }
 uint32_t gprtcu_spin_budget(void) { return g_spin_budget; }
@@ -490,38 +502,14 @@ extern "C" GPRTCU_API size_t gprtcuScanScratchSize(uint64_t n) {
   return sizeof(ScratchHeader) + gprtcu_align256(tiles * sizeof(uint64_t));
 }
 
-static gprtcuStatus scan_launch(const uint32_t *in, uint32_t *out, uint64_t n, int inclusive, uint32_t *d_total,
-                                void *scratch, size_t scratch_bytes, cudaStream_t stream) {
-  if (n > kScanMaxN) return GPRTCU_ERR_TOO_LARGE;
-  if (n > 0 && (!in || !out)) return GPRTCU_ERR_INVALID_ARG;
-  if (!scratch) return GPRTCU_ERR_INVALID_ARG;
-  if (((uintptr_t)scratch & 255) != 0) return GPRTCU_ERR_INVALID_ARG;
-  size_t need = gprtcuScanScratchSize(n);
-  if (scratch_bytes < need) return GPRTCU_ERR_SCRATCH_TOO_SMALL;
-  ScratchHeader *hdr = (ScratchHeader *)scratch;
-  uint64_t *status = (uint64_t *)((char *)scratch + sizeof(ScratchHeader));
-  uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
-  GPRTCU_TRY(cudaMemsetAsync(scratch, 0, sizeof(ScratchHeader) + tiles * sizeof(uint64_t), stream));
-  if (n == 0) {
-    if (d_total) GPRTCU_TRY(cudaMemsetAsync(d_total, 0, sizeof(uint32_t), stream));
-    return GPRTCU_OK;
-  }
-  const bool vec = (((uintptr_t)in | (uintptr_t)out) & 15) == 0;
-  const bool nc = (const void *)in != (const void *)out;
-  if (vec && g_scan_impl == 0) {
-    // TMA-staged tile-per-CTA kernel (32 KB dynamic shared memory per CTA).
-    if (inclusive)
-      k_scan_tma<1><<<(unsigned)tiles, TS_THREADS, TS_SMEM, stream>>>(in, out, n, tiles, hdr, status, d_total,
-                                                                       g_spin_budget, g_skip_tile);
-    else
-      k_scan_tma<0><<<(unsigned)tiles, TS_THREADS, TS_SMEM, stream>>>(in, out, n, tiles, hdr, status, d_total,
-                                                                       g_spin_budget, g_skip_tile);
-    GPRTCU_TRY(cudaGetLastError());
-    return GPRTCU_OK;
-  }
-  dim3 grid((unsigned)tiles), block(SCAN_THREADS);
-#define GPRTCU_SCAN_LAUNCH(M, V, N) \
-  k_scan_u32<M, V, N><<<grid, block, 0, stream>>>(in, out, n, tiles, hdr, status, d_total, g_spin_budget, g_skip_tile)
+template <int THREADS, int VECS, int LBW>
+static void launch_reg_scan(const uint32_t *in, uint32_t *out, uint64_t n, int inclusive, bool vec, bool nc,
+                            ScratchHeader *hdr, uint64_t *status, uint32_t *d_total, uint64_t tiles,
+                            cudaStream_t stream) {
+  dim3 grid((unsigned)tiles), block(THREADS);
+#define GPRTCU_SCAN_LAUNCH(M, V, N)                                                                              \
+  k_scan_u32<M, V, N, THREADS, VECS, LBW><<<grid, block, 0, stream>>>(in, out, n, tiles, hdr, status, d_total, \
+                                                                     g_spin_budget, g_skip_tile)
   if (inclusive) {
     if (vec && nc) GPRTCU_SCAN_LAUNCH(1, true, true);
     else if (vec) GPRTCU_SCAN_LAUNCH(1, true, false);
@@ -532,6 +520,39 @@ static gprtcuStatus scan_launch(const uint32_t *in, uint32_t *out, uint64_t n, i
     else GPRTCU_SCAN_LAUNCH(0, false, false);
   }
 #undef GPRTCU_SCAN_LAUNCH
+}
+
+static gprtcuStatus scan_launch(const uint32_t *in, uint32_t *out, uint64_t n, int inclusive, uint32_t *d_total,
+                                void *scratch, size_t scratch_bytes, cudaStream_t stream) {
+  if (n > kScanMaxN) return GPRTCU_ERR_TOO_LARGE;
+  if (n > 0 && (!in || !out)) return GPRTCU_ERR_INVALID_ARG;
+  if (!scratch) return GPRTCU_ERR_INVALID_ARG;
+  if (((uintptr_t)scratch & 255) != 0) return GPRTCU_ERR_INVALID_ARG;
+  ScratchHeader *hdr = (ScratchHeader *)scratch;
+  uint64_t *status = (uint64_t *)((char *)scratch + sizeof(ScratchHeader));
+  const bool vec = (((uintptr_t)in | (uintptr_t)out) & 15) == 0;
+  const bool nc = (const void *)in != (const void *)out;
+  // Kernel choice: impl 0 = TMA-staged 8192-element tiles (aligned buffers),
+  // impl 1 = register-staged 8192-element tiles (any alignment).
+  const int impl = vec ? g_scan_impl : 1;
+  const uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+  if (scratch_bytes < sizeof(ScratchHeader) + tiles * sizeof(uint64_t)) return GPRTCU_ERR_SCRATCH_TOO_SMALL;
+  GPRTCU_TRY(cudaMemsetAsync(scratch, 0, sizeof(ScratchHeader) + tiles * sizeof(uint64_t), stream));
+  if (n == 0) {
+    if (d_total) GPRTCU_TRY(cudaMemsetAsync(d_total, 0, sizeof(uint32_t), stream));
+    return GPRTCU_OK;
+  }
+  if (impl == 0) {
+    // TMA-staged tile-per-CTA kernel (32 KB dynamic shared memory per CTA).
+    if (inclusive)
+      k_scan_tma<1><<<(unsigned)tiles, TS_THREADS, TS_SMEM, stream>>>(in, out, n, tiles, hdr, status, d_total,
+                                                                       g_spin_budget, g_skip_tile);
+    else
+      k_scan_tma<0><<<(unsigned)tiles, TS_THREADS, TS_SMEM, stream>>>(in, out, n, tiles, hdr, status, d_total,
+                                                                       g_spin_budget, g_skip_tile);
+  } else {
+    launch_reg_scan<256, 8, 32>(in, out, n, inclusive, vec, nc, hdr, status, d_total, tiles, stream);
+  }
   GPRTCU_TRY(cudaGetLastError());
   return GPRTCU_OK;
 }
