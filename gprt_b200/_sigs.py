@@ -31,6 +31,9 @@ SIGNATURES = {
     "gprtcuTraceScratchSize": ([], sz),
     "gprtcuTraceClosest": ([vp, vp, u64, vp, vp, sz, vp], st),
     "gprtcuTraceAny": ([vp, vp, u64, vp, vp, sz, vp], st),
+    "gprtcuBatchScratchSize": ([u32, u32], sz),
+    "gprtcuBatchBuildTriangles": ([vp, vp, vp, u32, u32, i32, vp, vp, sz, vp], st),
+    "gprtcuBatchTrace": ([vp, vp, vp, u32, vp, u64, i32, vp, vp, sz, vp], st),
     "gprtcuDebugSetSpinBudget": ([u32], None),
     "gprtcuDebugScanSkipTile": ([i64], None),
     "gprtcuDebugScanImpl": ([i32], None),

@@ -213,3 +213,65 @@ def hits_numpy(hits):
     out["prim"] = h[:, 0].view(np.uint32)
     out["t"] = h[:, 1].view(np.float32)
     return out
+
+
+# ---------------------------------------------------------------- batched
+class BatchLbvh:
+    """Concatenated per-mesh LBVHs of a batch (see gprtcuBatchBuildTriangles)."""
+
+    def __init__(self, tri_offsets_host, device="cuda", with_aabbs=True):
+        import numpy as np
+        off = np.asarray(tri_offsets_host, dtype=np.int64)
+        self.meshes = int(off.size - 1)
+        self.n = int(off[-1])
+        dev = torch.device(device)
+        self.tri_off = torch.from_numpy(off.astype(np.uint32).view(np.int32)).to(dev)
+        nn = 2 * self.n - self.meshes
+        ni = max(self.n - self.meshes, 1)
+        self.codes = torch.empty(self.n, dtype=torch.int32, device=dev)
+        self.ids = torch.empty(self.n, dtype=torch.int32, device=dev)
+        self.nodes = torch.empty((nn, 4), dtype=torch.int32, device=dev)
+        self.aabbs = torch.empty((nn, 6), dtype=torch.float32, device=dev) if with_aabbs else None
+        self.scene = torch.empty((self.meshes, 6), dtype=torch.float32, device=dev)
+        self.root = torch.empty((self.meshes, 6), dtype=torch.float32, device=dev)
+        self.bvh2 = torch.empty((ni, 16), dtype=torch.float32, device=dev)
+        self.leaf = torch.empty((self.n, 12), dtype=torch.float32, device=dev)
+        self.scratch = scratch(lib().gprtcuBatchScratchSize(self.meshes, self.n), dev)
+        self.desc = LbvhDesc(0, _p(self.codes), _p(self.ids), _p(self.nodes), _p(self.aabbs), _p(self.scene),
+                             _p(self.root), _p(self.bvh2), _p(self.leaf))
+        self.off_host = off
+
+    def mesh_host(self, m):
+        """Reference-layout arrays of mesh m (numpy), as a plain build of that mesh returns them."""
+        import numpy as np
+        torch.cuda.synchronize()
+        b, e = int(self.off_host[m]), int(self.off_host[m + 1])
+        nb, ne = 2 * b - m, 2 * e - (m + 1)
+        d = dict(codes=self.codes[b:e].cpu().numpy().view(np.uint32), ids=self.ids[b:e].cpu().numpy().view(np.uint32),
+                 nodes=self.nodes[nb:ne].cpu().numpy(), scene=self.scene[m].cpu().numpy())
+        if self.aabbs is not None:
+            d["aabbs"] = self.aabbs[nb:ne].cpu().numpy()
+        return d
+
+
+def batch_build_triangles(pos, tri, batch, code_kind=0):
+    _need_cuda(pos, tri)
+    st = lib().gprtcuBatchBuildTriangles(_ptr(pos), _ptr(tri), _ptr(batch.tri_off), batch.meshes, batch.n, code_kind,
+                                         ctypes.byref(batch.desc), _ptr(batch.scratch), batch.scratch.numel(),
+                                         _stream())
+    _check(st, "gprtcuBatchBuildTriangles")
+    return batch
+
+
+def batch_trace(batch, rays, ray_off, hits=None, anyhit=False, scr=None):
+    """rays float32 [R,8]; ray_off device int32/uint32 [meshes+1]."""
+    _need_cuda(rays, ray_off)
+    nr = rays.shape[0]
+    if hits is None:
+        hits = torch.empty((nr, 2), dtype=torch.int32, device=rays.device)
+    if scr is None:
+        scr = scratch(lib().gprtcuTraceScratchSize(), rays.device)
+    st = lib().gprtcuBatchTrace(ctypes.byref(batch.desc), _ptr(batch.tri_off), _ptr(ray_off), batch.meshes, _ptr(rays),
+                                nr, 1 if anyhit else 0, _ptr(hits), _ptr(scr), scr.numel(), _stream())
+    _check(st, "gprtcuBatchTrace")
+    return hits

@@ -47,51 +47,6 @@ __device__ __forceinline__ void tri_box(const float v[9], float b[6]) {
   }
 }
 
-// Scene box.  Slot words hold order-preserving images: max of f2ord for the
-// maxima, max of ~f2ord for the minima, so one zero fill initialises both.
-template <int KIND>  // 0 triangles, 1 points
-__global__ void __launch_bounds__(256) k_bounds(const float *pos, const uint32_t *tri, uint32_t n, uint32_t *slots) {
-  float b[6] = {3.402823466e38f, 3.402823466e38f, 3.402823466e38f, -3.402823466e38f, -3.402823466e38f,
-                -3.402823466e38f};
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    float t[6];
-    if (KIND == 0) {
-      float v[9];
-      load_tri(pos, tri, i, v);
-      tri_box(v, t);
-    } else {
-      const float *p = pos + 3 * (size_t)i;
-      t[0] = t[3] = p[0];
-      t[1] = t[4] = p[1];
-      t[2] = t[5] = p[2];
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      b[k] = fminf(b[k], t[k]);
-      b[3 + k] = fmaxf(b[3 + k], t[3 + k]);
-    }
-  }
-  uint32_t w[6];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    w[k] = ~f2ord(b[k]);
-    w[3 + k] = f2ord(b[3 + k]);
-  }
-#pragma unroll
-  for (int k = 0; k < 6; ++k)
-    for (int o = 16; o > 0; o >>= 1) w[k] = max(w[k], __shfl_xor_sync(FULL_MASK, w[k], o));
-  __shared__ uint32_t s[8][6];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0)
-    for (int k = 0; k < 6; ++k) s[warp][k] = w[k];
-  __syncthreads();
-  if (threadIdx.x < 6) {
-    uint32_t m = 0;
-    for (int j = 0; j < (int)(blockDim.x >> 5); ++j) m = max(m, s[j][threadIdx.x]);
-    atomicMax(&slots[threadIdx.x], m);
-  }
-}
-
 __device__ __forceinline__ uint32_t spread10(uint32_t v) {
   v &= 0x3FFu;
   v = (v | (v << 16)) & 0xFF0000FFu;
@@ -138,23 +93,141 @@ __device__ __forceinline__ uint32_t quant10(float p, float lo, float hi) {
   return (uint32_t)v;
 }
 
-// Codes of centroids (p1 + p2 + p3) / 3 (gprt/development/gprt_lbvh.hlsl:
-// 139-146, 262-277), or of the points themselves; ids[i] = i.
-template <int KIND>
-__global__ void __launch_bounds__(256) k_codes(const float *pos, const uint32_t *tri, uint32_t n, const uint32_t *slots,
-                                               int code_kind, uint32_t *codes, uint32_t *ids, float *scene_out) {
-  float lo[3], hi[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    lo[k] = fminf(3.402823466e38f, ord2f(~slots[k]));
-    hi[k] = fmaxf(-3.402823466e38f, ord2f(slots[3 + k]));
+// Meshes are consecutive primitive ranges [prim_off[m], prim_off[m+1]), each
+// with at least one primitive.  Mesh m's arrays sit at fixed offsets inside
+// the concatenated outputs, so every mesh's block is exactly what a build of
+// that mesh alone produces:
+//   codes, ids, leaves' triangles     at prim base b = prim_off[m]
+//   nodes, aabbs (2 n_m - 1 entries)  at node base  2b - m
+//   traversal nodes (n_m - 1)         at inner base  b - m
+// A plain build is the single mesh [0, n) (prim_off == nullptr).
+struct MeshMap {
+  const uint32_t *prim_off;
+  uint32_t meshes;
+  uint32_t n;
+  __device__ __forceinline__ uint32_t begin(uint32_t m) const { return prim_off ? __ldg(prim_off + m) : 0u; }
+  __device__ __forceinline__ uint32_t count(uint32_t m) const {
+    return prim_off ? __ldg(prim_off + m + 1) - __ldg(prim_off + m) : n;
   }
-  if (blockIdx.x == 0 && threadIdx.x < 6 && scene_out) scene_out[threadIdx.x] = threadIdx.x < 3 ? lo[threadIdx.x] : hi[threadIdx.x - 3];
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  // Mesh holding global primitive i: prim_off[m] <= i < prim_off[m+1].
+  __device__ __forceinline__ uint32_t mesh_of_prim(uint64_t i) const {
+    if (!prim_off) return 0;
+    uint32_t lo = 0, hi = meshes;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (__ldg(prim_off + mid) <= i) lo = mid;
+      else hi = mid;
+    }
+    return lo;
+  }
+  // Mesh holding global inner node g: (b_m - m) <= g < (b_{m+1} - m - 1).
+  __device__ __forceinline__ uint32_t mesh_of_inner(uint64_t g) const {
+    if (!prim_off) return 0;
+    uint32_t lo = 0, hi = meshes;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (__ldg(prim_off + mid) - mid <= g) lo = mid;
+      else hi = mid;
+    }
+    return lo;
+  }
+};
+
+template <int KIND>
+__device__ __forceinline__ void prim_box(const float *pos, const uint32_t *tri, uint64_t id, float v[9], float b[6]) {
+  if (KIND == 0) {
+    load_tri(pos, tri, (uint32_t)id, v);
+    tri_box(v, b);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) v[k] = v[3 + k] = v[6 + k] = b[k] = b[3 + k] = pos[3 * (size_t)id + k];
+  }
+}
+
+// Scene box of each mesh (ComputeTriangleBounds, gprt/development/
+// gprt_lbvh.hlsl:215-226).  Slot words hold order-preserving integer images:
+// max of f2ord for the maxima, max of ~f2ord for the minima, so one zero fill
+// initialises both.  One mesh: block reduction, one atomic per CTA and
+// component.  Many meshes: warp reduction when the warp's primitives share a
+// mesh, per-lane atomics at mesh boundaries.
+template <int KIND, bool BATCHED>
+__global__ void __launch_bounds__(256) k_bounds(const float *pos, const uint32_t *tri, MeshMap mm, uint32_t *slots) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t w[6] = {0, 0, 0, 0, 0, 0};
+  const uint64_t total = ((uint64_t)mm.n + 31) & ~31ull;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const bool valid = i < mm.n;
+    float v[9], t[6];
+    uint32_t tw[6] = {0, 0, 0, 0, 0, 0};
+    if (valid) {
+      prim_box<KIND>(pos, tri, i, v, t);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        tw[k] = ~f2ord(t[k]);
+        tw[3 + k] = f2ord(t[3 + k]);
+      }
+    }
+    if (!BATCHED) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) w[k] = max(w[k], tw[k]);
+    } else {
+      const uint32_t m = valid ? mm.mesh_of_prim(i) : 0xFFFFFFFFu;
+      const uint32_t m0 = __shfl_sync(FULL_MASK, m, 0);
+      if (__all_sync(FULL_MASK, m == m0)) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+          for (int o = 16; o > 0; o >>= 1) tw[k] = max(tw[k], __shfl_xor_sync(FULL_MASK, tw[k], o));
+        if (lane < 6 && m0 != 0xFFFFFFFFu) atomicMax(&slots[6 * (size_t)m0 + lane], tw[lane]);
+      } else if (valid) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) atomicMax(&slots[6 * (size_t)m + k], tw[k]);
+      }
+    }
+  }
+  if (!BATCHED) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+      for (int o = 16; o > 0; o >>= 1) w[k] = max(w[k], __shfl_xor_sync(FULL_MASK, w[k], o));
+    __shared__ uint32_t s[8][6];
+    if (lane == 0)
+      for (int k = 0; k < 6; ++k) s[warp][k] = w[k];
+    __syncthreads();
+    if (threadIdx.x < 6) {
+      uint32_t mx = 0;
+      for (int j = 0; j < (int)(blockDim.x >> 5); ++j) mx = max(mx, s[j][threadIdx.x]);
+      atomicMax(&slots[threadIdx.x], mx);
+    }
+  }
+}
+
+// Codes of centroids (p1 + p2 + p3) / 3 (gprt/development/gprt_lbvh.hlsl:
+// 139-146, 262-277), or of the points themselves, normalised to the mesh's
+// box.  One mesh: codes[i] and ids[i] = i.  Many meshes: 64-bit sort keys
+// (mesh << 32 | code) and mesh-local ids.
+template <int KIND, bool BATCHED>
+__global__ void __launch_bounds__(256) k_codes(const float *pos, const uint32_t *tri, MeshMap mm, const uint32_t *slots,
+                                               int code_kind, uint32_t *codes, uint64_t *keys, uint32_t *ids,
+                                               float *scene_out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < mm.n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t m = BATCHED ? mm.mesh_of_prim(i) : 0u;
+    const uint32_t *sl = slots + 6 * (size_t)m;
+    float lo[3], hi[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = fminf(3.402823466e38f, ord2f(~sl[k]));
+      hi[k] = fmaxf(-3.402823466e38f, ord2f(sl[3 + k]));
+    }
+    const uint32_t b = BATCHED ? mm.begin(m) : 0u;
+    if (scene_out && i == b)
+      for (int k = 0; k < 3; ++k) {
+        scene_out[6 * (size_t)m + k] = lo[k];
+        scene_out[6 * (size_t)m + 3 + k] = hi[k];
+      }
     float c[3];
     if (KIND == 0) {
       float v[9];
-      load_tri(pos, tri, i, v);
+      load_tri(pos, tri, (uint32_t)i, v);
 #pragma unroll
       for (int k = 0; k < 3; ++k) c[k] = __fdiv_rn(__fadd_rn(__fadd_rn(v[k], v[3 + k]), v[6 + k]), 3.0f);
     } else {
@@ -162,133 +235,150 @@ __global__ void __launch_bounds__(256) k_codes(const float *pos, const uint32_t 
       for (int k = 0; k < 3; ++k) c[k] = pos[3 * (size_t)i + k];
     }
     const uint32_t x = quant10(c[0], lo[0], hi[0]), y = quant10(c[1], lo[1], hi[1]), z = quant10(c[2], lo[2], hi[2]);
-    codes[i] = code_kind == 0 ? (spread10(x) | (spread10(y) << 1) | (spread10(z) << 2)) : hilbert3d(x, y, z);
-    ids[i] = i;
+    const uint32_t code = code_kind == 0 ? (spread10(x) | (spread10(y) << 1) | (spread10(z) << 2)) : hilbert3d(x, y, z);
+    if (BATCHED) {
+      keys[i] = ((uint64_t)m << 32) | code;
+      ids[i] = (uint32_t)(i - b);
+    } else {
+      codes[i] = code;
+      ids[i] = (uint32_t)i;
+    }
   }
 }
 
-// Karras 2012 delta with the index tie-break (gprt/development/gprt_lbvh.hlsl:45-61).
-__device__ __forceinline__ int kdelta(const uint32_t *codes, int64_t n, int64_t i, uint32_t ci, int64_t j) {
+// Karras 2012 delta with the index tie-break (gprt/development/gprt_lbvh.hlsl:45-61),
+// over one mesh's sorted codes (local indices; the 64-bit batched keys carry
+// the code in their low word).
+template <bool BATCHED>
+__device__ __forceinline__ uint32_t code_at(const uint32_t *codes, const uint64_t *keys, uint64_t j) {
+  return BATCHED ? (uint32_t)__ldg(reinterpret_cast<const unsigned long long *>(keys) + j) : __ldg(codes + j);
+}
+template <bool BATCHED>
+__device__ __forceinline__ int kdelta(const uint32_t *codes, const uint64_t *keys, uint64_t base, int64_t n, int64_t i,
+                                      uint32_t ci, int64_t j) {
   if (j < 0 || j >= n) return -1;
-  const uint32_t x = ci ^ __ldg(&codes[j]);
+  const uint32_t x = ci ^ code_at<BATCHED>(codes, keys, base + j);
   if (x == 0) return __clz((uint32_t)i ^ (uint32_t)j) + 32;
   return __clz(x);
 }
 
 // determine_range + SplitNodes (gprt/development/gprt_lbvh.hlsl:64-103,
-// 287-338), one thread per inner node.  Writes {left, right, -, -1} of the
-// node, the parent field of both children, and the child references of the
-// traversal node (inner child c -> c, leaf k -> ~k).
-__global__ void __launch_bounds__(256) k_karras(const uint32_t *codes, uint32_t n, int4 *nodes, Bvh2Node *bvh) {
-  const int64_t N = n;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N - 1; i += (int64_t)gridDim.x * blockDim.x) {
-    const uint32_t ci = codes[i];
-    const int d = kdelta(codes, N, i, ci, i + 1) >= kdelta(codes, N, i, ci, i - 1) ? 1 : -1;
-    const int dmin = kdelta(codes, N, i, ci, i - d);
+// 287-338), one thread per inner node, mesh-local indices.  Writes {left,
+// right, -, -1} of the node, the parent field of both children, and the child
+// references of the traversal node (inner child c -> c, leaf k -> ~k).
+template <bool BATCHED>
+__global__ void __launch_bounds__(256) k_karras(const uint32_t *codes, const uint64_t *keys, MeshMap mm, int4 *nodes,
+                                                Bvh2Node *bvh) {
+  const uint64_t total_inner = (uint64_t)mm.n - mm.meshes;
+  for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total_inner;
+       g += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t m = BATCHED ? mm.mesh_of_inner(g) : 0u;
+    const uint64_t b = BATCHED ? mm.begin(m) : 0;
+    const int64_t N = BATCHED ? mm.count(m) : mm.n;
+    const uint64_t inner_base = b - m, node_base = 2 * b - m;
+    const int64_t i = (int64_t)(g - inner_base);
+    const uint32_t ci = code_at<BATCHED>(codes, keys, b + i);
+#define KD(j) kdelta<BATCHED>(codes, keys, b, N, i, ci, (j))
+    const int d = KD(i + 1) >= KD(i - 1) ? 1 : -1;
+    const int dmin = KD(i - d);
     int64_t lmax = 2;
-    while (kdelta(codes, N, i, ci, i + lmax * d) > dmin) lmax *= 2;
+    while (KD(i + lmax * d) > dmin) lmax *= 2;
     int64_t l = 0;
     for (int64_t t = lmax >> 1; t >= 1; t >>= 1)
-      if (kdelta(codes, N, i, ci, i + (l + t) * d) > dmin) l += t;
+      if (KD(i + (l + t) * d) > dmin) l += t;
     const int64_t j = i + l * d;
-    const int dnode = kdelta(codes, N, i, ci, j);
+    const int dnode = KD(j);
     int64_t s = 0;
     for (int k = 1;; ++k) {
       const int64_t t = (l + ((int64_t)1 << k) - 1) >> k;
-      if (kdelta(codes, N, i, ci, i + (s + t) * d) > dnode) s += t;
+      if (KD(i + (s + t) * d) > dnode) s += t;
       if (t == 1) break;
     }
+#undef KD
     const int64_t split = i + s * d + min(d, 0);
     const int64_t first = d == 1 ? i : j, last = d == 1 ? j : i;
     const int64_t left = split, right = split + 1;
     const bool lleaf = left == first, rleaf = right == last;
     const int64_t lc = lleaf ? (N - 1) + left : left;
     const int64_t rc = rleaf ? (N - 1) + right : right;
-    int4 nd;
-    nd.x = (int)lc;
-    nd.y = (int)rc;
-    nd.z = -1;  // overwritten by the parent's thread (root stays -1)
-    nd.w = -1;
-    // x, y, w of this node; z belongs to the parent's thread.
-    reinterpret_cast<int *>(&nodes[i])[0] = nd.x;
-    reinterpret_cast<int *>(&nodes[i])[1] = nd.y;
-    reinterpret_cast<int *>(&nodes[i])[3] = -1;
-    if (i == 0) reinterpret_cast<int *>(&nodes[0])[2] = -1;
-    reinterpret_cast<int *>(&nodes[lc])[2] = (int)i;
-    reinterpret_cast<int *>(&nodes[rc])[2] = (int)i;
-    if (bvh) {
-      bvh[i].ref[0] = lleaf ? ~(int)left : (int)lc;
-      bvh[i].ref[1] = rleaf ? ~(int)right : (int)rc;
-    }
+    int *nd = reinterpret_cast<int *>(&nodes[node_base + i]);
+    nd[0] = (int)lc;
+    nd[1] = (int)rc;
+    nd[3] = -1;
+    if (i == 0) nd[2] = -1;  // root; other parents are written by the parent's thread
+    reinterpret_cast<int *>(&nodes[node_base + lc])[2] = (int)i;
+    reinterpret_cast<int *>(&nodes[node_base + rc])[2] = (int)i;
+    if (bvh)
+      *reinterpret_cast<int4 *>(bvh[inner_base + i].ref) = make_int4(lleaf ? ~(int)left : (int)lc,
+                                                                     rleaf ? ~(int)right : (int)rc, 0, 0);
   }
 }
 
 // Leaf boxes and the bottom-up union (BuildTriangleHierarchy,
 // gprt/development/gprt_lbvh.hlsl:400-428, with MakeNodes' +-1e38 start
 // :279-285).  One thread per leaf; the second arrival at a node forms it.
-template <int KIND>
-__global__ void __launch_bounds__(256) k_refit(const float *pos, const uint32_t *tri, const uint32_t *ids, uint32_t n,
-                                               int4 *nodes, float *aabbs, Bvh2Node *bvh, float4 *leaf_tris,
+template <int KIND, bool BATCHED>
+__global__ void __launch_bounds__(256) k_refit(const float *pos, const uint32_t *tri, const uint32_t *ids,
+                                               const uint64_t *keys, MeshMap mm, int4 *nodes, float *aabbs,
+                                               Bvh2Node *bvh, float4 *leaf_tris, uint32_t *codes_out,
                                                uint32_t *arrivals, float *root_box) {
-  const int64_t N = n, inner = N - 1;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
-    const uint32_t id = ids[i];
-    float v[9], b[6];
-    if (KIND == 0) {
-      load_tri(pos, tri, id, v);
-      tri_box(v, b);
-    } else {
-#pragma unroll
-      for (int k = 0; k < 3; ++k) v[k] = v[3 + k] = v[6 + k] = b[k] = b[3 + k] = pos[3 * (size_t)id + k];
-    }
-    const int64_t leaf = inner + i;
+  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < mm.n; s += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t m = BATCHED ? mm.mesh_of_prim(s) : 0u;
+    const uint64_t b = BATCHED ? mm.begin(m) : 0;
+    const int64_t N = BATCHED ? mm.count(m) : mm.n;
+    const uint64_t inner_base = b - m, node_base = 2 * b - m;
+    const int64_t i = (int64_t)(s - b);
+    const uint32_t id = ids[s];
+    float v[9], bx[6];
+    prim_box<KIND>(pos, tri, b + id, v, bx);
+    if (BATCHED && codes_out) codes_out[s] = (uint32_t)keys[s];
     if (leaf_tris) {
-      leaf_tris[3 * i + 0] = make_float4(v[0], v[1], v[2], __uint_as_float(id));
-      leaf_tris[3 * i + 1] = make_float4(v[3], v[4], v[5], 0.0f);
-      leaf_tris[3 * i + 2] = make_float4(v[6], v[7], v[8], 0.0f);
+      leaf_tris[3 * s + 0] = make_float4(v[0], v[1], v[2], __uint_as_float(id));
+      leaf_tris[3 * s + 1] = make_float4(v[3], v[4], v[5], 0.0f);
+      leaf_tris[3 * s + 2] = make_float4(v[6], v[7], v[8], 0.0f);
     }
-    int *nl = reinterpret_cast<int *>(&nodes[leaf]);
+    const int64_t leaf = (N - 1) + i;
+    int *nl = reinterpret_cast<int *>(&nodes[node_base + leaf]);
     nl[0] = -1;
     nl[1] = -1;
     nl[3] = (int)id;
     if (N == 1) nl[2] = -1;
     if (aabbs)
-      for (int k = 0; k < 6; ++k) aabbs[6 * leaf + k] = b[k];
+      for (int k = 0; k < 6; ++k) aabbs[6 * (node_base + leaf) + k] = bx[k];
     int64_t child = leaf;
-    int64_t p = N == 1 ? -1 : (int64_t)ld_relaxed_u32(reinterpret_cast<const uint32_t *>(nl + 2));
+    int64_t p = N == 1 ? -1 : (int64_t)nl[2];
     while (p >= 0) {
-      const int side = (ld_relaxed_u32(reinterpret_cast<const uint32_t *>(&nodes[p])) == (uint32_t)child) ? 0 : 1;
+      const int side = nodes[node_base + p].x == (int)child ? 0 : 1;
       // This child's box goes into its slot of the parent's traversal node
       // (or is already in the reference-layout array); publish it before
       // counting the arrival.
       if (bvh) {
-        float *cb = bvh[p].box + 6 * side;
+        float *cb = bvh[inner_base + p].box + 6 * side;
 #pragma unroll
-        for (int k = 0; k < 6; ++k) cb[k] = b[k];
+        for (int k = 0; k < 6; ++k) cb[k] = bx[k];
       }
       __threadfence();
-      if (atomicAdd(&arrivals[p], 1u) == 0) break;  // first arrival: the sibling finishes the node
+      if (atomicAdd(&arrivals[inner_base + p], 1u) == 0) break;  // first arrival: the sibling finishes the node
       __threadfence();
       // Second arrival: read the sibling's box (from L2) and form the union,
       // starting from +-1e38 exactly as MakeNodes initialises inner boxes.
+      const int64_t sib = side == 0 ? nodes[node_base + p].y : nodes[node_base + p].x;
+      const float *ob = bvh ? bvh[inner_base + p].box + 6 * (1 - side) : aabbs + 6 * (node_base + sib);
       float sb[6];
-      const float *ob = bvh ? bvh[p].box + 6 * (1 - side)
-                            : aabbs + 6 * (int64_t)(side == 0 ? nodes[p].y : nodes[p].x);
 #pragma unroll
       for (int k = 0; k < 6; ++k) sb[k] = __ldcg(ob + k);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        b[k] = fminf(1e38f, fminf(b[k], sb[k]));
-        b[3 + k] = fmaxf(-1e38f, fmaxf(b[3 + k], sb[3 + k]));
+        bx[k] = fminf(1e38f, fminf(bx[k], sb[k]));
+        bx[3 + k] = fmaxf(-1e38f, fmaxf(bx[3 + k], sb[3 + k]));
       }
       if (aabbs)
-        for (int k = 0; k < 6; ++k) aabbs[6 * p + k] = b[k];
+        for (int k = 0; k < 6; ++k) aabbs[6 * (node_base + p) + k] = bx[k];
       child = p;
-      p = (int64_t)(int)ld_relaxed_u32(reinterpret_cast<const uint32_t *>(&nodes[p]) + 2);
+      p = nodes[node_base + p].z;
     }
-    if (p < 0 && child == 0 && root_box) {
-      for (int k = 0; k < 6; ++k) root_box[k] = b[k];
-    }
+    if (p < 0 && child == 0 && root_box)
+      for (int k = 0; k < 6; ++k) root_box[6 * (size_t)m + k] = bx[k];
   }
 }
 
@@ -298,23 +388,6 @@ using namespace gprtcu;
 
 namespace {
 
-struct LbvhScratch {
-  size_t slots, arrivals, sort, total;
-};
-
-LbvhScratch lbvh_scratch_layout(uint32_t n) {
-  LbvhScratch L;
-  size_t off = sizeof(ScratchHeader);
-  L.slots = off;
-  off += 256;
-  L.arrivals = off;
-  off += gprtcu_align256((size_t)(n > 1 ? n - 1 : 1) * 4);
-  L.sort = off;
-  off += gprtcuSortScratchSize(n, 4, 4);
-  L.total = off;
-  return L;
-}
-
 int grid_for(uint64_t n, int threads, int per_sm) {
   uint64_t g = (n + threads - 1) / threads;
   uint64_t cap = (uint64_t)gprtcu_num_sms() * per_sm;
@@ -322,65 +395,116 @@ int grid_for(uint64_t n, int threads, int per_sm) {
   return (int)(g ? g : 1);
 }
 
-gprtcuStatus lbvh_build(int kind, const float *pos, const uint32_t *tri, uint32_t n, int codeKind, gprtcuLbvh *out,
-                        void *scratch, size_t scratchBytes, cudaStream_t stream) {
+struct LbvhScratch {
+  size_t slots, arrivals, keys, sort, total;
+};
+
+LbvhScratch lbvh_scratch_layout(uint64_t n, uint32_t meshes) {
+  LbvhScratch L;
+  size_t off = sizeof(ScratchHeader);
+  L.slots = off;
+  off += gprtcu_align256((size_t)meshes * 6 * 4);
+  L.arrivals = off;
+  off += gprtcu_align256((size_t)(n > meshes ? n - meshes : 1) * 4);
+  L.keys = off;
+  if (meshes > 1) off += gprtcu_align256((size_t)n * 8);
+  L.sort = off;
+  off += meshes > 1 ? gprtcuSortScratchSize(n, 8, 4) : gprtcuSortScratchSize(n, 4, 4);
+  L.total = off;
+  return L;
+}
+
+int ceil_log2(uint32_t v) {
+  int b = 0;
+  while ((1ull << b) < v) ++b;
+  return b;
+}
+
+template <int KIND, bool BATCHED>
+void launch_build(const float *pos, const uint32_t *tri, MeshMap mm, int codeKind, gprtcuLbvh *out, uint32_t *slots,
+                  uint64_t *keys, uint32_t *arrivals, cudaStream_t stream, int stage) {
+  const int g = grid_for(mm.n, 256, 8);
+  int4 *nodes = (int4 *)out->nodes;
+  if (stage == 0) {
+    k_bounds<KIND, BATCHED><<<g, 256, 0, stream>>>(pos, tri, mm, slots);
+    k_codes<KIND, BATCHED><<<g, 256, 0, stream>>>(pos, tri, mm, slots, codeKind, out->codes, keys, out->ids,
+                                                  out->sceneBounds);
+  } else {
+    if (mm.n > mm.meshes)
+      k_karras<BATCHED><<<grid_for(mm.n - mm.meshes, 256, 8), 256, 0, stream>>>(out->codes, keys, mm, nodes,
+                                                                                  (Bvh2Node *)out->bvh2);
+    k_refit<KIND, BATCHED><<<g, 256, 0, stream>>>(pos, tri, out->ids, keys, mm, nodes, out->aabbs,
+                                                  (Bvh2Node *)out->bvh2, (float4 *)out->leafTris, out->codes,
+                                                  arrivals, out->rootBox);
+  }
+}
+
+gprtcuStatus lbvh_build(int kind, const float *pos, const uint32_t *tri, const uint32_t *prim_off, uint32_t meshes,
+                        uint32_t n, int codeKind, gprtcuLbvh *out, void *scratch, size_t scratchBytes,
+                        cudaStream_t stream) {
   if (!out || !pos || (kind == 0 && !tri)) return GPRTCU_ERR_INVALID_ARG;
-  if (n == 0) return GPRTCU_ERR_INVALID_ARG;
+  if (n == 0 || meshes == 0 || meshes > n) return GPRTCU_ERR_INVALID_ARG;
+  if (meshes > 1 && !prim_off) return GPRTCU_ERR_INVALID_ARG;
   if (n > (1u << 30) - 1) return GPRTCU_ERR_TOO_LARGE;
   if (!out->codes || !out->ids || !out->nodes) return GPRTCU_ERR_INVALID_ARG;
-  if (n > 1 && !out->aabbs && !out->bvh2) return GPRTCU_ERR_INVALID_ARG;  // the refit needs one box store
+  if (n > meshes && !out->aabbs && !out->bvh2) return GPRTCU_ERR_INVALID_ARG;  // the refit needs one box store
   if (out->bvh2 && ((uintptr_t)out->bvh2 & 15)) return GPRTCU_ERR_INVALID_ARG;
   if (out->leafTris && ((uintptr_t)out->leafTris & 15)) return GPRTCU_ERR_INVALID_ARG;
   if (codeKind != 0 && codeKind != 1) return GPRTCU_ERR_INVALID_ARG;
   if (!scratch || ((uintptr_t)scratch & 255)) return GPRTCU_ERR_INVALID_ARG;
-  LbvhScratch L = lbvh_scratch_layout(n);
+  const LbvhScratch L = lbvh_scratch_layout(n, meshes);
   if (scratchBytes < L.total) return GPRTCU_ERR_SCRATCH_TOO_SMALL;
   char *s = (char *)scratch;
   out->numPrims = n;
-  GPRTCU_TRY(cudaMemsetAsync(s, 0, L.sort, stream));  // header, bound slots, arrival counters
+  GPRTCU_TRY(cudaMemsetAsync(s, 0, L.keys, stream));  // header, bound slots, arrival counters
   uint32_t *slots = (uint32_t *)(s + L.slots);
   uint32_t *arrivals = (uint32_t *)(s + L.arrivals);
-  int4 *nodes = (int4 *)out->nodes;
-  Bvh2Node *bvh = (Bvh2Node *)out->bvh2;
-  float4 *leafTris = (float4 *)out->leafTris;
-  const int g = grid_for(n, 256, 8);
-  if (kind == 0) {
-    k_bounds<0><<<g, 256, 0, stream>>>(pos, tri, n, slots);
-    k_codes<0><<<g, 256, 0, stream>>>(pos, tri, n, slots, codeKind, out->codes, out->ids, out->sceneBounds);
-  } else {
-    k_bounds<1><<<g, 256, 0, stream>>>(pos, tri, n, slots);
-    k_codes<1><<<g, 256, 0, stream>>>(pos, tri, n, slots, codeKind, out->codes, out->ids, out->sceneBounds);
-  }
-  GPRTCU_TRY(cudaGetLastError());
-  gprtcuStatus st = gprtcuSortPairsU32(out->codes, out->ids, n, 0, 30, s + L.sort, scratchBytes - L.sort,
-                                       (gprtcuStream)stream);
-  if (st != GPRTCU_OK) return st;
-  if (n > 1) {
-    k_karras<<<grid_for(n - 1, 256, 8), 256, 0, stream>>>(out->codes, n, nodes, bvh);
+  uint64_t *keys = meshes > 1 ? (uint64_t *)(s + L.keys) : nullptr;
+  const MeshMap mm{meshes > 1 ? prim_off : nullptr, meshes, n};
+  const bool batched = meshes > 1;
+  for (int stage = 0; stage < 2; ++stage) {
+    if (stage == 1) {
+      gprtcuStatus st = batched ? gprtcuSortPairsU64(keys, out->ids, n, 0, 32 + (ceil_log2(meshes) > 0 ? ceil_log2(meshes) : 1),
+                                                     s + L.sort, scratchBytes - L.sort, (gprtcuStream)stream)
+                                : gprtcuSortPairsU32(out->codes, out->ids, n, 0, 30, s + L.sort, scratchBytes - L.sort,
+                                                     (gprtcuStream)stream);
+      if (st != GPRTCU_OK) return st;
+    }
+    if (kind == 0 && batched) launch_build<0, true>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
+    else if (kind == 0) launch_build<0, false>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
+    else if (batched) launch_build<1, true>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
+    else launch_build<1, false>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
     GPRTCU_TRY(cudaGetLastError());
   }
-  if (kind == 0)
-    k_refit<0><<<g, 256, 0, stream>>>(pos, tri, out->ids, n, nodes, out->aabbs, bvh, leafTris, arrivals,
-                                      out->rootBox);
-  else
-    k_refit<1><<<g, 256, 0, stream>>>(pos, tri, out->ids, n, nodes, out->aabbs, bvh, leafTris, arrivals,
-                                      out->rootBox);
-  GPRTCU_TRY(cudaGetLastError());
   return GPRTCU_OK;
 }
 
 }  // namespace
 
-extern "C" GPRTCU_API size_t gprtcuLbvhScratchSize(uint32_t n) { return lbvh_scratch_layout(n).total; }
+extern "C" GPRTCU_API size_t gprtcuLbvhScratchSize(uint32_t n) { return lbvh_scratch_layout(n, 1).total; }
 
 extern "C" GPRTCU_API gprtcuStatus gprtcuLbvhBuildTriangles(const float *positions, const uint32_t *triangles,
                                                             uint32_t numTriangles, int codeKind, gprtcuLbvh *bvh,
                                                             void *scratch, size_t scratchBytes, gprtcuStream stream) {
-  return lbvh_build(0, positions, triangles, numTriangles, codeKind, bvh, scratch, scratchBytes, (cudaStream_t)stream);
+  return lbvh_build(0, positions, triangles, nullptr, 1, numTriangles, codeKind, bvh, scratch, scratchBytes,
+                    (cudaStream_t)stream);
 }
 
 extern "C" GPRTCU_API gprtcuStatus gprtcuLbvhBuildPoints(const float *positions, uint32_t numPoints, int codeKind,
                                                          gprtcuLbvh *bvh, void *scratch, size_t scratchBytes,
                                                          gprtcuStream stream) {
-  return lbvh_build(1, positions, nullptr, numPoints, codeKind, bvh, scratch, scratchBytes, (cudaStream_t)stream);
+  return lbvh_build(1, positions, nullptr, nullptr, 1, numPoints, codeKind, bvh, scratch, scratchBytes,
+                    (cudaStream_t)stream);
+}
+
+extern "C" GPRTCU_API size_t gprtcuBatchScratchSize(uint32_t numMeshes, uint32_t totalTriangles) {
+  return lbvh_scratch_layout(totalTriangles, numMeshes).total;
+}
+
+extern "C" GPRTCU_API gprtcuStatus gprtcuBatchBuildTriangles(const float *positions, const uint32_t *triangles,
+                                                             const uint32_t *triOffsets, uint32_t numMeshes,
+                                                             uint32_t totalTriangles, int codeKind, gprtcuLbvh *bvh,
+                                                             void *scratch, size_t scratchBytes, gprtcuStream stream) {
+  return lbvh_build(0, positions, triangles, triOffsets, numMeshes, totalTriangles, codeKind, bvh, scratch,
+                    scratchBytes, (cudaStream_t)stream);
 }

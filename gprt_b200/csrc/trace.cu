@@ -37,10 +37,31 @@ __device__ __forceinline__ void leaf_test(const float4 *leaf, uint32_t slot, con
 // that has finished idles until the warp's last ray is done), so the lanes
 // re-converge at every visit.  A loop with per-lane exits lets the lanes drift
 // apart and run one at a time.
-template <bool ANY>
-__global__ void __launch_bounds__(kTraceThreads) k_trace_bin(const Bvh2Node *bvh, const float4 *leaf, uint32_t n,
-                                                            const float4 *rays, uint64_t nrays, Hit *hits,
-                                                            unsigned long long *counter, uint32_t *err) {
+// Batched form: rays [ray_off[m], ray_off[m+1]) go to mesh m, whose
+// primitives are [tri_off[m], tri_off[m+1]); its traversal nodes start at
+// tri_off[m] - m and its leaves at tri_off[m] (mesh-local references are
+// offset on the fly).  Hits report mesh-local primitive ids.
+struct TraceMeshes {
+  const uint32_t *tri_off;
+  const uint32_t *ray_off;
+  uint32_t meshes;
+};
+
+__device__ __forceinline__ uint32_t mesh_of_ray(const TraceMeshes &tm, uint64_t r) {
+  uint32_t lo = 0, hi = tm.meshes;  // ray_off[lo] <= r < ray_off[hi]
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(tm.ray_off + mid) <= r) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+template <bool ANY, bool BATCHED>
+__global__ void __launch_bounds__(kTraceThreads) k_trace_bin(const Bvh2Node *bvh_all, const float4 *leaf_all,
+                                                            uint32_t n_all, TraceMeshes tm, const float4 *rays,
+                                                            uint64_t nrays, Hit *hits, unsigned long long *counter,
+                                                            uint32_t *err) {
   const int lane = threadIdx.x & 31;
   while (true) {
     unsigned long long base = 0;
@@ -52,13 +73,23 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace_bin(const Bvh2Node *bvh
     Ray R;
     ray_setup(active ? __ldg(rays + 2 * r) : make_float4(0.f, 0.f, 0.f, 1.f),
               active ? __ldg(rays + 2 * r + 1) : make_float4(1.f, 0.f, 0.f, 0.f), R);
+    const Bvh2Node *bvh = bvh_all;
+    const float4 *leaf = leaf_all;
+    uint32_t n = n_all;
+    if (BATCHED && active) {
+      const uint32_t m = mesh_of_ray(tm, r);
+      const uint32_t b = __ldg(tm.tri_off + m);
+      n = __ldg(tm.tri_off + m + 1) - b;
+      bvh = bvh_all + (b - m);
+      leaf = leaf_all + 3 * (size_t)b;
+    }
     uint32_t best = kMiss, best_slot = 0;
     float bt = R.tmax;
     bool done = !active;
     int st_node[kStack];  // inner nodes still to visit (4 B each: the hot top stays in L1)
     int sp = 0;
     int node = 0;
-    if (n == 1) {
+    if (n == 1 || !active) {
       if (active) {
         const float4 a = __ldg(leaf), b = __ldg(leaf + 1), c = __ldg(leaf + 2);
         float tn;
@@ -129,11 +160,13 @@ using namespace gprtcu;
 
 namespace {
 
-gprtcuStatus trace_launch(const gprtcuLbvh *bvh, const float *rays, uint64_t nrays, gprtcuHit *hits, bool any,
-                          void *scratch, size_t scratch_bytes, cudaStream_t stream) {
+gprtcuStatus trace_launch(const gprtcuLbvh *bvh, const uint32_t *tri_off, const uint32_t *ray_off, uint32_t meshes,
+                          const float *rays, uint64_t nrays, gprtcuHit *hits, bool any, void *scratch,
+                          size_t scratch_bytes, cudaStream_t stream) {
   if (!bvh || (!rays && nrays) || (!hits && nrays)) return GPRTCU_ERR_INVALID_ARG;
+  if (meshes == 0 || (meshes > 1 && (!tri_off || !ray_off))) return GPRTCU_ERR_INVALID_ARG;
   if (nrays == 0) return GPRTCU_OK;
-  if (bvh->numPrims == 0 || !bvh->leafTris || (bvh->numPrims > 1 && !bvh->bvh2)) return GPRTCU_ERR_INVALID_ARG;
+  if (bvh->numPrims == 0 || !bvh->leafTris || (bvh->numPrims > meshes && !bvh->bvh2)) return GPRTCU_ERR_INVALID_ARG;
   if (((uintptr_t)rays & 15) || ((uintptr_t)bvh->leafTris & 15) || ((uintptr_t)bvh->bvh2 & 15))
     return GPRTCU_ERR_INVALID_ARG;
   if (!scratch || ((uintptr_t)scratch & 255)) return GPRTCU_ERR_INVALID_ARG;
@@ -144,15 +177,20 @@ gprtcuStatus trace_launch(const gprtcuLbvh *bvh, const float *rays, uint64_t nra
   const int blocks = gprtcu_num_sms() * 10;  // 48 registers: 10 CTAs of 128 threads per SM
   const uint64_t need = (nrays + kTraceThreads - 1) / kTraceThreads;
   const int grid = (int)(need < (uint64_t)blocks ? need : blocks);
-  if (any)
-    k_trace_bin<true><<<grid, kTraceThreads, 0, stream>>>((const Bvh2Node *)bvh->bvh2, (const float4 *)bvh->leafTris,
-                                                          bvh->numPrims, (const float4 *)rays, nrays, (Hit *)hits,
-                                                          counter, &hdr->status);
-  else
-    k_trace_bin<false><<<grid, kTraceThreads, 0, stream>>>((const Bvh2Node *)bvh->bvh2,
-                                                           (const float4 *)bvh->leafTris, bvh->numPrims,
-                                                           (const float4 *)rays, nrays, (Hit *)hits, counter,
-                                                           &hdr->status);
+  const TraceMeshes tm{tri_off, ray_off, meshes};
+  const Bvh2Node *nodes = (const Bvh2Node *)bvh->bvh2;
+  const float4 *leaf = (const float4 *)bvh->leafTris;
+#define GPRTCU_TRACE(A, B)                                                                                         \
+  k_trace_bin<A, B><<<grid, kTraceThreads, 0, stream>>>(nodes, leaf, bvh->numPrims, tm, (const float4 *)rays, nrays, \
+                                                        (Hit *)hits, counter, &hdr->status)
+  if (meshes > 1) {
+    if (any) GPRTCU_TRACE(true, true);
+    else GPRTCU_TRACE(false, true);
+  } else {
+    if (any) GPRTCU_TRACE(true, false);
+    else GPRTCU_TRACE(false, false);
+  }
+#undef GPRTCU_TRACE
   GPRTCU_TRY(cudaGetLastError());
   return GPRTCU_OK;
 }
@@ -164,11 +202,19 @@ extern "C" GPRTCU_API size_t gprtcuTraceScratchSize(void) { return sizeof(Scratc
 extern "C" GPRTCU_API gprtcuStatus gprtcuTraceClosest(const gprtcuLbvh *bvh, const float *rays, uint64_t numRays,
                                                       gprtcuHit *hits, void *scratch, size_t scratchBytes,
                                                       gprtcuStream stream) {
-  return trace_launch(bvh, rays, numRays, hits, false, scratch, scratchBytes, (cudaStream_t)stream);
+  return trace_launch(bvh, nullptr, nullptr, 1, rays, numRays, hits, false, scratch, scratchBytes, (cudaStream_t)stream);
 }
 
 extern "C" GPRTCU_API gprtcuStatus gprtcuTraceAny(const gprtcuLbvh *bvh, const float *rays, uint64_t numRays,
                                                   gprtcuHit *hits, void *scratch, size_t scratchBytes,
                                                   gprtcuStream stream) {
-  return trace_launch(bvh, rays, numRays, hits, true, scratch, scratchBytes, (cudaStream_t)stream);
+  return trace_launch(bvh, nullptr, nullptr, 1, rays, numRays, hits, true, scratch, scratchBytes, (cudaStream_t)stream);
+}
+
+extern "C" GPRTCU_API gprtcuStatus gprtcuBatchTrace(const gprtcuLbvh *bvh, const uint32_t *triOffsets,
+                                                    const uint32_t *rayOffsets, uint32_t numMeshes, const float *rays,
+                                                    uint64_t numRays, int anyHit, gprtcuHit *hits, void *scratch,
+                                                    size_t scratchBytes, gprtcuStream stream) {
+  return trace_launch(bvh, triOffsets, rayOffsets, numMeshes, rays, numRays, hits, anyHit != 0, scratch, scratchBytes,
+                      (cudaStream_t)stream);
 }

@@ -56,3 +56,28 @@ def rays(m, seed=1, lo=(0.0, 0.0, 0.0), size=1.0, radius=2.0):
 def mesh_sizes(count, lo=64, hi=65536, seed=2):
     rng = np.random.default_rng(seed)
     return np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi), size=count))).astype(np.int64)
+
+
+def batch(sizes, seed=0, sigma=0.002, rays_per_tri=0, spacing=2.0):
+    """Meshes of the given triangle counts, mesh m a soup inside its own unit
+    cube at a grid offset (m mod 16, m // 16 mod 16, m // 256) * spacing.
+    Returns pos [V,3], tri [N,3] (global vertex indices), tri_off [M+1] and,
+    when rays_per_tri > 0, rays [R,8] with ray_off [M+1] (rays of mesh m aimed
+    at its cube from the radius-2 sphere around it)."""
+    sizes = np.asarray(sizes, np.int64)
+    off = np.zeros(sizes.size + 1, np.int64)
+    off[1:] = np.cumsum(sizes)
+    pos = np.empty((3 * int(off[-1]), 3), np.float32)
+    rays_l, ray_off = [], np.zeros(sizes.size + 1, np.int64)
+    for m, n in enumerate(sizes):
+        o = np.array([m % 16, (m // 16) % 16, m // 256], np.float32) * spacing
+        p, _ = soup(int(n), seed=seed * 1000003 + m, sigma=sigma, offset=o)
+        pos[3 * off[m]:3 * off[m + 1]] = p
+        if rays_per_tri:
+            r = rays(int(n) * rays_per_tri, seed=seed * 7919 + m + 17, lo=o)
+            rays_l.append(r)
+            ray_off[m + 1] = ray_off[m] + r.shape[0]
+    tri = np.arange(3 * int(off[-1]), dtype=np.uint32).reshape(-1, 3)
+    if rays_per_tri:
+        return pos, tri, off, np.concatenate(rays_l), ray_off
+    return pos, tri, off

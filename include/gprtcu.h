@@ -187,6 +187,33 @@ GPRTCU_API gprtcuStatus gprtcuTraceAny(const gprtcuLbvh *bvh, const float *rays,
                                        void *scratch, size_t scratchBytes, gprtcuStream stream);
 
 /* ------------------------------------------------------------------------
+ * Batched build and trace: many meshes in one set of launches.  No
+ * counterpart in the reference beyond repeated gprtLBVHBuild calls
+ * (gprt/development/gprt_lbvh.h:170-195), one per mesh.
+ * Meshes are consecutive triangle ranges: triOffsets (device, uint32
+ * [numMeshes+1], exclusive prefix of the triangle counts, every mesh >= 1
+ * triangle); `triangles` hold global vertex indices into `positions`.
+ * Output arrays are the per-mesh LBVHs concatenated, each mesh's block
+ * bit-identical to gprtcuLbvhBuildTriangles on that mesh alone:
+ *   codes, ids (mesh-local ids), leafTris    at b = triOffsets[m]
+ *   nodes, aabbs (2 n_m - 1 nodes each)       at 2b - m
+ *   bvh2 (n_m - 1 nodes each)                 at b - m
+ *   sceneBounds, rootBox                      float[numMeshes][6]
+ * The segmented sort runs on 64-bit keys (meshID << 32 | code).
+ * Trace: rays [rayOffsets[m], rayOffsets[m+1]) are traced against mesh m
+ * (rayOffsets device uint32[numMeshes+1]); hits carry mesh-local ids.
+ * ------------------------------------------------------------------------ */
+GPRTCU_API size_t gprtcuBatchScratchSize(uint32_t numMeshes, uint32_t totalTriangles);
+GPRTCU_API gprtcuStatus gprtcuBatchBuildTriangles(const float *positions, const uint32_t *triangles,
+                                                  const uint32_t *triOffsets, uint32_t numMeshes,
+                                                  uint32_t totalTriangles, int codeKind, gprtcuLbvh *bvh,
+                                                  void *scratch, size_t scratchBytes, gprtcuStream stream);
+GPRTCU_API gprtcuStatus gprtcuBatchTrace(const gprtcuLbvh *bvh, const uint32_t *triOffsets,
+                                         const uint32_t *rayOffsets, uint32_t numMeshes, const float *rays,
+                                         uint64_t numRays, int anyHit, gprtcuHit *hits, void *scratch,
+                                         size_t scratchBytes, gprtcuStream stream);
+
+/* ------------------------------------------------------------------------
  * Test hooks (fault injection without a GPU fault).  Process-wide settings
  * read at launch time by the look-back kernels.
  * gprtcuDebugSetSpinBudget: polls a look-back wait makes before it records
