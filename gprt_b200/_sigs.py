@@ -34,6 +34,9 @@ SIGNATURES = {
     "gprtcuBatchScratchSize": ([u32, u32], sz),
     "gprtcuBatchBuildTriangles": ([vp, vp, vp, u32, u32, i32, vp, vp, sz, vp], st),
     "gprtcuBatchTrace": ([vp, vp, vp, u32, vp, u64, i32, vp, vp, sz, vp], st),
+    "gprtcuWideScratchSize": ([u32, u32], sz),
+    "gprtcuWideBuild": ([vp, vp, u32, vp, vp, sz, vp], st),
+    "gprtcuWideTrace": ([vp, vp, u32, vp, u64, i32, vp, vp, sz, vp], st),
     "gprtcuDebugSetSpinBudget": ([u32], None),
     "gprtcuDebugScanSkipTile": ([i64], None),
     "gprtcuDebugScanImpl": ([i32], None),

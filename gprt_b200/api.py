@@ -275,3 +275,66 @@ def batch_trace(batch, rays, ray_off, hits=None, anyhit=False, scr=None):
                                 nr, 1 if anyhit else 0, _ptr(hits), _ptr(scr), scr.numel(), _stream())
     _check(st, "gprtcuBatchTrace")
     return hits
+
+
+# ---------------------------------------------------------------- wide (8-wide quantised) BVH
+class WideDesc(ctypes.Structure):
+    """gprtcuWideBvh (include/gprtcu.h)."""
+    _fields_ = [("nodes", ctypes.c_void_p), ("leafTris", ctypes.c_void_p), ("roots", ctypes.c_void_p),
+                ("numNodes", ctypes.c_void_p), ("capacity", ctypes.c_uint32)]
+
+
+class WideBvh:
+    def __init__(self, n, meshes=1, device="cuda"):
+        dev = torch.device(device)
+        self.n, self.meshes = int(n), int(meshes)
+        self.nodes = torch.zeros((self.n, 20), dtype=torch.int32, device=dev)  # 80 B per node
+        self.leaf = torch.empty((self.n, 12), dtype=torch.float32, device=dev)
+        self.roots = torch.empty(self.meshes, dtype=torch.int32, device=dev)
+        self.count = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.scratch = scratch(lib().gprtcuWideScratchSize(self.meshes, self.n), dev)
+        self.desc = WideDesc(_p(self.nodes), _p(self.leaf), _p(self.roots), _p(self.count), self.n)
+
+
+def wide_build(binary, tri_off=None, wide=None):
+    """Collapse a binary Lbvh / BatchLbvh into the 8-wide quantised form."""
+    meshes = getattr(binary, "meshes", 1)
+    n = binary.n
+    if wide is None:
+        wide = WideBvh(n, meshes, binary.codes.device)
+    toff = tri_off if tri_off is not None else getattr(binary, "tri_off", None)
+    st = lib().gprtcuWideBuild(ctypes.byref(binary.desc), _ptr(toff) if meshes > 1 else None, meshes,
+                               ctypes.byref(wide.desc), _ptr(wide.scratch), wide.scratch.numel(), _stream())
+    _check(st, "gprtcuWideBuild")
+    return wide
+
+
+def wide_trace(wide, rays, ray_off=None, hits=None, anyhit=False, scr=None):
+    _need_cuda(rays)
+    nr = rays.shape[0]
+    if hits is None:
+        hits = torch.empty((nr, 2), dtype=torch.int32, device=rays.device)
+    if scr is None:
+        scr = scratch(lib().gprtcuTraceScratchSize(), rays.device)
+    st = lib().gprtcuWideTrace(ctypes.byref(wide.desc), _ptr(ray_off) if wide.meshes > 1 else None, wide.meshes,
+                               _ptr(rays), nr, 1 if anyhit else 0, _ptr(hits), _ptr(scr), scr.numel(), _stream())
+    _check(st, "gprtcuWideTrace")
+    return hits
+
+
+def wide_decode(wide):
+    """Host copy of the wide nodes as numpy structured fields (tests)."""
+    import numpy as np
+    torch.cuda.synchronize()
+    cnt = int(wide.count.item())
+    raw = wide.nodes[:cnt].cpu().numpy().view(np.uint8).reshape(cnt, 80)
+    f = raw[:, 0:12].copy().view(np.float32).reshape(cnt, 3)
+    e = raw[:, 12:15].copy().view(np.int8).astype(np.int32)
+    imask = raw[:, 15].astype(np.uint32)
+    cb = raw[:, 16:20].copy().view(np.uint32).ravel()
+    lb = raw[:, 20:24].copy().view(np.uint32).ravel()
+    meta = raw[:, 24:32]
+    qlo = raw[:, 32:56].reshape(cnt, 3, 8)
+    qhi = raw[:, 56:80].reshape(cnt, 3, 8)
+    return dict(count=cnt, p=f, e=e, imask=imask, child_base=cb, leaf_base=lb, meta=meta, qlo=qlo, qhi=qhi,
+                roots=wide.roots.cpu().numpy(), leaf=wide.leaf.cpu().numpy())

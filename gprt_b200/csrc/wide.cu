@@ -1,0 +1,480 @@
+// wide.cu -- 8-wide BVH with 8-bit quantised child boxes, collapsed from the
+// binary LBVH, and its closest-hit / any-hit traversal.  No counterpart in
+// the reference (its traversal is Vulkan ray-tracing hardware); the node
+// format follows the compressed-wide-BVH idea of Ylitie, Karras, Laine 2017
+// ("Efficient Incoherent Ray Traversal on GPUs Through Compressed Wide
+// BVHs"), written here for this build.
+//
+// Node (80 bytes, five 16-byte loads):
+//   p.xyz      fp32 origin = min corner of the children's union box
+//   e.xyz      int8 scale exponents, scale s = 2^e per axis, chosen (in FP64)
+//              as the smallest power of two with 255 * s >= extent
+//   imask      bit c: child slot c is an inner node
+//   child_base first inner child's node index (inner children contiguous)
+//   leaf_base  first leaf child's index in the wide leaf array (contiguous)
+//   meta[c]    0xFF empty; else the child's rank among the inner (imask) or
+//              leaf children
+//   qlo/qhi    per axis, per child: floor((lo - p) / s), ceil((hi - p) / s)
+// Decoding uses round-down (lo) and round-up (hi) FMAs, so every decoded box
+// contains its exact fp32 child box; a ray therefore never misses a child the
+// binary traversal would enter, and intersection is the same FP32 watertight
+// test, giving the same hits.  A node is 80 bytes for up to eight children
+// against 64 bytes for two in the binary layout.
+#include "common.cuh"
+#include "lbvh.cuh"
+#include "rtmath.cuh"
+
+namespace gprtcu {
+
+struct __align__(16) WideNode {
+  float px, py, pz;
+  int8_t ex, ey, ez;
+  uint8_t imask;
+  uint32_t child_base;
+  uint32_t leaf_base;
+  uint8_t meta[8];
+  uint8_t qlo[3][8];
+  uint8_t qhi[3][8];
+};
+static_assert(sizeof(WideNode) == 80, "80-byte wide node");
+
+struct WorkItem {
+  uint32_t mesh;
+  int32_t bref;  // binary inner node (mesh-local) or ~slot for a one-leaf mesh
+  uint32_t wide;
+  uint32_t pad;
+};
+
+enum { Q_HEAD = 0, Q_TAIL = 1, Q_DONE = 2, Q_WIDE = 3, Q_LEAF = 4 };
+
+__device__ __forceinline__ float box_area(const float *b) {
+  const float dx = b[3] - b[0], dy = b[4] - b[1], dz = b[5] - b[2];
+  return dx * dy + dy * dz + dz * dx;
+}
+
+// Smallest e with 255 * 2^e >= ext (FP64), clamped to the normal fp32 range.
+__device__ __forceinline__ int frame_exponent(double ext) {
+  if (!(ext > 0.0)) return -126;
+  int k;
+  frexp(ext / 255.0, &k);
+  int e = k - 1;
+  while (ldexp(255.0, e) < ext) ++e;
+  while (e > -126 && ldexp(255.0, e - 1) >= ext) --e;
+  return e < -126 ? -126 : (e > 127 ? 127 : e);
+}
+
+__global__ void k_wide_init(const uint32_t *tri_off, uint32_t meshes, uint32_t n, WorkItem *queue, uint32_t *ready,
+                            uint32_t *roots, uint32_t *counters) {
+  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < meshes; m += gridDim.x * blockDim.x) {
+    const uint32_t cnt = tri_off ? tri_off[m + 1] - tri_off[m] : n;
+    queue[m] = WorkItem{m, cnt == 1 ? ~0 : 0, m, 0};
+    ready[m] = 1;
+    roots[m] = m;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    counters[Q_TAIL] = meshes;
+    counters[Q_WIDE] = meshes;
+  }
+}
+
+// Persistent top-down collapse.  Every thread is a worker: it takes the next
+// queue slot, waits (bounded) until that item is published or all work is
+// done, expands the binary node greedily -- the inner child of largest
+// surface area is replaced by its two children until there are eight -- then
+// writes the quantised wide node, copies its leaf triangles and publishes its
+// inner children as new items.  All work is done when the number of finished
+// items equals the number of items ever published (read in that order).
+__global__ void __launch_bounds__(128) k_wide_collapse(const Bvh2Node *bvh2, const float4 *leaf_tris,
+                                                       const uint32_t *tri_off, uint32_t n, WideNode *wnodes,
+                                                       float4 *wleaf, WorkItem *queue, uint32_t *ready,
+                                                       uint32_t *counters, uint32_t budget, ScratchHeader *hdr) {
+  while (true) {
+    const uint32_t idx = atomicAdd(&counters[Q_HEAD], 1u);
+    // At most n items ever exist (one per wide node: a root per mesh plus one
+    // per binary inner node), and queue/ready hold exactly n entries.
+    if (idx >= n) return;
+    uint32_t spins = 0;
+    bool have = false;
+    while (true) {
+      if (ld_acquire_u32(&ready[idx])) {
+        have = true;
+        break;
+      }
+      const uint32_t done = ld_acquire_u32(&counters[Q_DONE]);
+      const uint32_t tail = ld_relaxed_u32(&counters[Q_TAIL]);
+      if (done == tail && idx >= tail) break;
+      if (++spins > budget) {
+        record_error(hdr, GPRTCU_ERR_TIMEOUT);
+        break;
+      }
+      __nanosleep(64);
+    }
+    if (!have) return;
+    // Published by another SM: read through L2, not a possibly stale L1 line.
+    const uint4 raw = __ldcg(reinterpret_cast<const uint4 *>(queue + idx));
+    const WorkItem it{raw.x, (int32_t)raw.y, raw.z, 0u};
+    const uint32_t m = it.mesh;
+    const uint32_t b = tri_off ? tri_off[m] : 0u;
+    const Bvh2Node *mb = bvh2 + (b - m);
+    // children: ref (>= 0 inner local, < 0 ~leaf slot) and exact boxes
+    int ref[8];
+    float box[8][6];
+    int cnt = 0;
+    if (it.bref < 0) {
+      const uint32_t slot = (uint32_t)~it.bref;
+      const float4 a = leaf_tris[3 * (size_t)(b + slot)], c = leaf_tris[3 * (size_t)(b + slot) + 1],
+                   d = leaf_tris[3 * (size_t)(b + slot) + 2];
+      ref[0] = it.bref;
+      box[0][0] = fminf(a.x, fminf(c.x, d.x));
+      box[0][1] = fminf(a.y, fminf(c.y, d.y));
+      box[0][2] = fminf(a.z, fminf(c.z, d.z));
+      box[0][3] = fmaxf(a.x, fmaxf(c.x, d.x));
+      box[0][4] = fmaxf(a.y, fmaxf(c.y, d.y));
+      box[0][5] = fmaxf(a.z, fmaxf(c.z, d.z));
+      cnt = 1;
+    } else {
+      const Bvh2Node nd = mb[it.bref];
+      for (int c = 0; c < 2; ++c) {
+        ref[c] = nd.ref[c];
+        for (int k = 0; k < 6; ++k) box[c][k] = nd.box[6 * c + k];
+      }
+      cnt = 2;
+      while (cnt < 8) {
+        int best = -1;
+        float ba = -1.0f;
+        for (int c = 0; c < cnt; ++c)
+          if (ref[c] >= 0) {
+            const float a = box_area(box[c]);
+            if (a > ba) {
+              ba = a;
+              best = c;
+            }
+          }
+        if (best < 0) break;
+        const Bvh2Node ch = mb[ref[best]];
+        ref[best] = ch.ref[0];
+        for (int k = 0; k < 6; ++k) box[best][k] = ch.box[k];
+        ref[cnt] = ch.ref[1];
+        for (int k = 0; k < 6; ++k) box[cnt][k] = ch.box[6 + k];
+        ++cnt;
+      }
+    }
+    int n_inner = 0, n_leaf = 0;
+    for (int c = 0; c < cnt; ++c) (ref[c] >= 0 ? n_inner : n_leaf)++;
+    const uint32_t child_base = n_inner ? atomicAdd(&counters[Q_WIDE], (uint32_t)n_inner) : 0u;
+    const uint32_t leaf_base = n_leaf ? atomicAdd(&counters[Q_LEAF], (uint32_t)n_leaf) : 0u;
+    WideNode w;
+    float lo[3] = {box[0][0], box[0][1], box[0][2]}, hi[3] = {box[0][3], box[0][4], box[0][5]};
+    for (int c = 1; c < cnt; ++c)
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = fminf(lo[k], box[c][k]);
+        hi[k] = fmaxf(hi[k], box[c][3 + k]);
+      }
+    w.px = lo[0];
+    w.py = lo[1];
+    w.pz = lo[2];
+    int e[3];
+    double s[3];
+    for (int k = 0; k < 3; ++k) {
+      e[k] = frame_exponent((double)hi[k] - (double)lo[k]);
+      s[k] = ldexp(1.0, e[k]);
+    }
+    w.ex = (int8_t)e[0];
+    w.ey = (int8_t)e[1];
+    w.ez = (int8_t)e[2];
+    w.imask = 0;
+    w.child_base = child_base;
+    w.leaf_base = leaf_base;
+    int ri = 0, rl = 0;
+    for (int c = 0; c < 8; ++c) {
+      if (c >= cnt) {
+        w.meta[c] = 0xFF;
+        for (int k = 0; k < 3; ++k) {
+          w.qlo[k][c] = 0;
+          w.qhi[k][c] = 0;
+        }
+        continue;
+      }
+      for (int k = 0; k < 3; ++k) {
+        double ql = floor(((double)box[c][k] - (double)lo[k]) / s[k]);
+        double qh = ceil(((double)box[c][3 + k] - (double)lo[k]) / s[k]);
+        w.qlo[k][c] = (uint8_t)(ql < 0.0 ? 0.0 : (ql > 255.0 ? 255.0 : ql));
+        w.qhi[k][c] = (uint8_t)(qh < 0.0 ? 0.0 : (qh > 255.0 ? 255.0 : qh));
+      }
+      if (ref[c] >= 0) {
+        w.imask |= (uint8_t)(1u << c);
+        w.meta[c] = (uint8_t)ri;
+        ++ri;
+      } else {
+        const uint32_t slot = (uint32_t)~ref[c];
+        const size_t src = 3 * (size_t)(b + slot), dst = 3 * (size_t)(leaf_base + rl);
+        wleaf[dst] = leaf_tris[src];
+        wleaf[dst + 1] = leaf_tris[src + 1];
+        wleaf[dst + 2] = leaf_tris[src + 2];
+        w.meta[c] = (uint8_t)rl;
+        ++rl;
+      }
+    }
+    const uint4 *wp = reinterpret_cast<const uint4 *>(&w);
+    uint4 *op = reinterpret_cast<uint4 *>(wnodes + it.wide);
+    for (int k = 0; k < 5; ++k) op[k] = wp[k];
+    // publish inner children as new work items, in rank order
+    ri = 0;
+    for (int c = 0; c < cnt; ++c)
+      if (ref[c] >= 0) {
+        const uint32_t q = atomicAdd(&counters[Q_TAIL], 1u);
+        queue[q] = WorkItem{m, ref[c], child_base + (uint32_t)ri, 0};
+        __threadfence();
+        st_relaxed_u32(&ready[q], 1u);
+        ++ri;
+      }
+    __threadfence();
+    atomicAdd(&counters[Q_DONE], 1u);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// traversal
+// ---------------------------------------------------------------------------
+constexpr int kWideThreads = 128;
+constexpr int kWideStack = 64;
+
+__device__ __forceinline__ float scale_of(int8_t e) { return __int_as_float(((int)e + 127) << 23); }
+
+__device__ __forceinline__ void wide_leaf_test(const float4 *leaf, uint32_t i, const Ray &R, uint32_t &best,
+                                               uint32_t &best_leaf, float &bt) {
+  const float4 a = __ldg(leaf + 3 * (size_t)i), b = __ldg(leaf + 3 * (size_t)i + 1), c = __ldg(leaf + 3 * (size_t)i + 2);
+  const float v0[3] = {a.x, a.y, a.z}, v1[3] = {b.x, b.y, b.z}, v2[3] = {c.x, c.y, c.z};
+  const uint32_t id = __float_as_uint(a.w);
+  float t;
+  if (isect_tri(R, v0, v1, v2, t) && (best == kMiss || t < bt || (t == bt && id < best))) {
+    best = id;
+    best_leaf = i;
+    bt = t;
+  }
+}
+
+template <bool ANY, bool BATCHED>
+__global__ void __launch_bounds__(kWideThreads) k_trace_wide(const WideNode *nodes, const float4 *leaf,
+                                                            const uint32_t *roots, const uint32_t *ray_off,
+                                                            uint32_t meshes, const float4 *rays, uint64_t nrays,
+                                                            Hit *hits, unsigned long long *counter, uint32_t *err) {
+  const int lane = threadIdx.x & 31;
+  while (true) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32ull);
+    base = __shfl_sync(FULL_MASK, base, 0);
+    if (base >= nrays) break;
+    const uint64_t r = base + lane;
+    const bool active = r < nrays;
+    Ray R;
+    ray_setup(active ? __ldg(rays + 2 * r) : make_float4(0.f, 0.f, 0.f, 1.f),
+              active ? __ldg(rays + 2 * r + 1) : make_float4(1.f, 0.f, 0.f, 0.f), R);
+    uint32_t node = 0;
+    if (active) {
+      uint32_t m = 0;
+      if (BATCHED) {
+        uint32_t lo = 0, hi = meshes;
+        while (hi - lo > 1) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (__ldg(ray_off + mid) <= r) lo = mid;
+          else hi = mid;
+        }
+        m = lo;
+      }
+      node = __ldg(roots + m);
+    }
+    uint32_t best = kMiss, best_leaf = 0;
+    float bt = R.tmax;
+    bool done = !active;
+    uint2 stack[kWideStack];  // {child_base, mask of inner children still to visit}
+    int sp = 0;
+    while (__any_sync(FULL_MASK, !done)) {
+      if (!done) {
+        const uint4 *np = reinterpret_cast<const uint4 *>(nodes + node);
+        const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+        const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
+        const float sx = scale_of((int8_t)(w0.w & 0xFF)), sy = scale_of((int8_t)((w0.w >> 8) & 0xFF)),
+                    sz = scale_of((int8_t)((w0.w >> 16) & 0xFF));
+        const uint32_t imask = w0.w >> 24;
+        const uint32_t child_base = w1.x, leaf_base = w1.y;
+        const uint32_t meta_lo = w1.z, meta_hi = w1.w;
+        const uint32_t qlx[2] = {w2.x, w2.y}, qly[2] = {w2.z, w2.w}, qlz[2] = {w3.x, w3.y};
+        const uint32_t qhx[2] = {w3.z, w3.w}, qhy[2] = {w4.x, w4.y}, qhz[2] = {w4.z, w4.w};
+        float ctn[8];
+        uint32_t hitmask = 0;  // bit = inner-child rank
+        uint32_t rank_of[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          const uint32_t meta = ((c < 4 ? meta_lo : meta_hi) >> (8 * (c & 3))) & 0xFF;
+          rank_of[c] = meta;
+          ctn[c] = 0.0f;
+          if (meta == 0xFF) continue;
+          const int h = c >> 2, sh = 8 * (c & 3);
+          const float lx = __fmaf_rd((float)((qlx[h] >> sh) & 0xFF), sx, px);
+          const float ly = __fmaf_rd((float)((qly[h] >> sh) & 0xFF), sy, py);
+          const float lz = __fmaf_rd((float)((qlz[h] >> sh) & 0xFF), sz, pz);
+          const float ux = __fmaf_ru((float)((qhx[h] >> sh) & 0xFF), sx, px);
+          const float uy = __fmaf_ru((float)((qhy[h] >> sh) & 0xFF), sy, py);
+          const float uz = __fmaf_ru((float)((qhz[h] >> sh) & 0xFF), sz, pz);
+          float tn;
+          if (ray_box(R, lx, ly, lz, ux, uy, uz, bt, tn) && tn <= bt) {
+            if ((imask >> c) & 1u) {
+              hitmask |= 1u << meta;
+              ctn[c] = tn;
+            } else {
+              wide_leaf_test(leaf, leaf_base + meta, R, best, best_leaf, bt);
+            }
+          }
+        }
+        if (ANY && best != kMiss) {
+          done = true;
+        } else {
+          // drop inner children now behind the best hit; descend into the nearest
+          int nearest = -1;
+          float nt = 0.0f;
+#pragma unroll
+          for (int c = 0; c < 8; ++c) {
+            if (!((imask >> c) & 1u) || !((hitmask >> rank_of[c]) & 1u)) continue;
+            if (ctn[c] > bt) {
+              hitmask &= ~(1u << rank_of[c]);
+            } else if (nearest < 0 || ctn[c] < nt) {
+              nearest = (int)rank_of[c];
+              nt = ctn[c];
+            }
+          }
+          if (nearest >= 0) {
+            hitmask &= ~(1u << nearest);
+            if (hitmask) {
+              if (sp < kWideStack) {
+                stack[sp++] = make_uint2(child_base, hitmask);
+              } else {
+                atomicCAS(err, 0u, 5u);  // traversal stack overflow
+                done = true;
+              }
+            }
+            node = child_base + (uint32_t)nearest;
+          } else if (sp > 0) {
+            uint2 &top = stack[sp - 1];
+            const uint32_t rr = __ffs(top.y) - 1;
+            top.y &= top.y - 1;
+            node = top.x + rr;
+            if (top.y == 0) --sp;
+          } else {
+            done = true;
+          }
+        }
+      }
+    }
+    if (active) {
+      Hit h;
+      h.prim = best;
+      h.t = __int_as_float(0x7f800000);
+      if (best != kMiss) {
+        const float4 a = __ldg(leaf + 3 * (size_t)best_leaf), b = __ldg(leaf + 3 * (size_t)best_leaf + 1),
+                     c = __ldg(leaf + 3 * (size_t)best_leaf + 2);
+        const float v0[3] = {a.x, a.y, a.z}, v1[3] = {b.x, b.y, b.z}, v2[3] = {c.x, c.y, c.z};
+        h.t = refine_t(R, v0, v1, v2);
+      }
+      hits[r] = h;
+    }
+  }
+}
+
+}  // namespace gprtcu
+
+using namespace gprtcu;
+
+uint32_t gprtcu_spin_budget(void);
+
+namespace {
+
+struct WideScratch {
+  size_t counters, queue, ready, total;
+};
+
+WideScratch wide_layout(uint32_t meshes, uint32_t n) {
+  WideScratch L;
+  size_t off = sizeof(ScratchHeader);
+  L.counters = off;
+  off += 256;
+  L.ready = off;
+  off += gprtcu_align256((size_t)n * 4);
+  L.queue = off;
+  off += gprtcu_align256((size_t)n * sizeof(WorkItem));
+  L.total = off;
+  (void)meshes;
+  return L;
+}
+
+}  // namespace
+
+extern "C" GPRTCU_API size_t gprtcuWideScratchSize(uint32_t numMeshes, uint32_t totalTriangles) {
+  return wide_layout(numMeshes, totalTriangles).total;
+}
+
+extern "C" GPRTCU_API gprtcuStatus gprtcuWideBuild(const gprtcuLbvh *binary, const uint32_t *triOffsets,
+                                                   uint32_t numMeshes, gprtcuWideBvh *out, void *scratch,
+                                                   size_t scratchBytes, gprtcuStream stream_) {
+  cudaStream_t stream = (cudaStream_t)stream_;
+  if (!binary || !out || numMeshes == 0) return GPRTCU_ERR_INVALID_ARG;
+  const uint32_t n = binary->numPrims;
+  if (n == 0 || numMeshes > n || (numMeshes > 1 && !triOffsets)) return GPRTCU_ERR_INVALID_ARG;
+  if (!binary->leafTris || (n > numMeshes && !binary->bvh2)) return GPRTCU_ERR_INVALID_ARG;
+  if (!out->nodes || !out->leafTris || !out->roots || out->capacity < n) return GPRTCU_ERR_INVALID_ARG;
+  if (((uintptr_t)out->nodes & 15) || ((uintptr_t)out->leafTris & 15)) return GPRTCU_ERR_INVALID_ARG;
+  if (!scratch || ((uintptr_t)scratch & 255)) return GPRTCU_ERR_INVALID_ARG;
+  const WideScratch L = wide_layout(numMeshes, n);
+  if (scratchBytes < L.total) return GPRTCU_ERR_SCRATCH_TOO_SMALL;
+  char *s = (char *)scratch;
+  GPRTCU_TRY(cudaMemsetAsync(s, 0, L.queue, stream));  // header, counters, ready flags
+  uint32_t *counters = (uint32_t *)(s + L.counters);
+  uint32_t *ready = (uint32_t *)(s + L.ready);
+  WorkItem *queue = (WorkItem *)(s + L.queue);
+  const uint32_t *toff = numMeshes > 1 ? triOffsets : nullptr;
+  k_wide_init<<<(numMeshes + 255) / 256, 256, 0, stream>>>(toff, numMeshes, n, queue, ready, out->roots, counters);
+  GPRTCU_TRY(cudaGetLastError());
+  k_wide_collapse<<<gprtcu_num_sms() * 8, 128, 0, stream>>>((const Bvh2Node *)binary->bvh2,
+                                                            (const float4 *)binary->leafTris, toff, n,
+                                                            (WideNode *)out->nodes, (float4 *)out->leafTris, queue,
+                                                            ready, counters, gprtcu_spin_budget(),
+                                                            (ScratchHeader *)s);
+  GPRTCU_TRY(cudaGetLastError());
+  if (out->numNodes) GPRTCU_TRY(cudaMemcpyAsync(out->numNodes, counters + Q_WIDE, 4, cudaMemcpyDeviceToDevice, stream));
+  return GPRTCU_OK;
+}
+
+extern "C" GPRTCU_API gprtcuStatus gprtcuWideTrace(const gprtcuWideBvh *bvh, const uint32_t *rayOffsets,
+                                                   uint32_t numMeshes, const float *rays, uint64_t numRays, int anyHit,
+                                                   gprtcuHit *hits, void *scratch, size_t scratchBytes,
+                                                   gprtcuStream stream_) {
+  cudaStream_t stream = (cudaStream_t)stream_;
+  if (!bvh || numMeshes == 0 || (numMeshes > 1 && !rayOffsets)) return GPRTCU_ERR_INVALID_ARG;
+  if ((!rays || !hits) && numRays) return GPRTCU_ERR_INVALID_ARG;
+  if (numRays == 0) return GPRTCU_OK;
+  if (!bvh->nodes || !bvh->leafTris || !bvh->roots) return GPRTCU_ERR_INVALID_ARG;
+  if (((uintptr_t)rays & 15) || ((uintptr_t)bvh->nodes & 15) || ((uintptr_t)bvh->leafTris & 15))
+    return GPRTCU_ERR_INVALID_ARG;
+  if (!scratch || ((uintptr_t)scratch & 255)) return GPRTCU_ERR_INVALID_ARG;
+  if (scratchBytes < sizeof(ScratchHeader)) return GPRTCU_ERR_SCRATCH_TOO_SMALL;
+  ScratchHeader *hdr = (ScratchHeader *)scratch;
+  unsigned long long *counter = reinterpret_cast<unsigned long long *>(&hdr->ticket[0]);
+  GPRTCU_TRY(cudaMemsetAsync(scratch, 0, sizeof(ScratchHeader), stream));
+  const int blocks = gprtcu_num_sms() * 8;
+  const uint64_t need = (numRays + kWideThreads - 1) / kWideThreads;
+  const int grid = (int)(need < (uint64_t)blocks ? need : blocks);
+#define GPRTCU_WTRACE(A, B)                                                                                       \
+  k_trace_wide<A, B><<<grid, kWideThreads, 0, stream>>>((const WideNode *)bvh->nodes, (const float4 *)bvh->leafTris, \
+                                                        bvh->roots, rayOffsets, numMeshes, (const float4 *)rays,     \
+                                                        numRays, (Hit *)hits, counter, &hdr->status)
+  if (numMeshes > 1) {
+    if (anyHit) GPRTCU_WTRACE(true, true);
+    else GPRTCU_WTRACE(false, true);
+  } else {
+    if (anyHit) GPRTCU_WTRACE(true, false);
+    else GPRTCU_WTRACE(false, false);
+  }
+#undef GPRTCU_WTRACE
+  GPRTCU_TRY(cudaGetLastError());
+  return GPRTCU_OK;
+}

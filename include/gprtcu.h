@@ -214,6 +214,35 @@ GPRTCU_API gprtcuStatus gprtcuBatchTrace(const gprtcuLbvh *bvh, const uint32_t *
                                          size_t scratchBytes, gprtcuStream stream);
 
 /* ------------------------------------------------------------------------
+ * 8-wide quantised BVH.  No counterpart in the reference.  Collapsed from a
+ * binary LBVH (plain or batched, which needs bvh2 and leafTris): every node
+ * has up to 8 children whose boxes are stored as uint8 per axis against an
+ * fp32 origin and a power-of-two scale per axis (computed in FP64, floor /
+ * ceil rounding), so the decoded boxes always contain the exact ones; leaf
+ * triangles are copied into leaf order of the wide tree.  Traversal returns
+ * the same hits as gprtcuTraceClosest / gprtcuBatchTrace.
+ *   nodes     80 B x capacity (capacity >= total triangles)
+ *   leafTris  float[total][12]
+ *   roots     uint32[numMeshes]: root node of each mesh
+ *   numNodes  optional device uint32: node count written by the build
+ * triOffsets / rayOffsets: NULL (one mesh) or device uint32[numMeshes+1].
+ * ------------------------------------------------------------------------ */
+typedef struct {
+  void *nodes;
+  float *leafTris;
+  uint32_t *roots;
+  uint32_t *numNodes;
+  uint32_t capacity;
+} gprtcuWideBvh;
+
+GPRTCU_API size_t gprtcuWideScratchSize(uint32_t numMeshes, uint32_t totalTriangles);
+GPRTCU_API gprtcuStatus gprtcuWideBuild(const gprtcuLbvh *binary, const uint32_t *triOffsets, uint32_t numMeshes,
+                                        gprtcuWideBvh *out, void *scratch, size_t scratchBytes, gprtcuStream stream);
+GPRTCU_API gprtcuStatus gprtcuWideTrace(const gprtcuWideBvh *bvh, const uint32_t *rayOffsets, uint32_t numMeshes,
+                                        const float *rays, uint64_t numRays, int anyHit, gprtcuHit *hits,
+                                        void *scratch, size_t scratchBytes, gprtcuStream stream);
+
+/* ------------------------------------------------------------------------
  * Test hooks (fault injection without a GPU fault).  Process-wide settings
  * read at launch time by the look-back kernels.
  * gprtcuDebugSetSpinBudget: polls a look-back wait makes before it records
