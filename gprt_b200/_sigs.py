@@ -37,6 +37,9 @@ SIGNATURES = {
     "gprtcuWideScratchSize": ([u32, u32], sz),
     "gprtcuWideBuild": ([vp, vp, u32, vp, vp, sz, vp], st),
     "gprtcuWideTrace": ([vp, vp, u32, vp, u64, i32, vp, vp, sz, vp], st),
+    "gprtcuGenSoup": ([u64, u64, ctypes.c_float, vp, u32, ctypes.c_float, vp, vp, vp], st),
+    "gprtcuGenMixture": ([u64, u32, u64, ctypes.c_float, vp, vp, vp], st),
+    "gprtcuGenRays": ([u64, u64, vp, u32, vp, vp, vp], st),
     "gprtcuDebugSetSpinBudget": ([u32], None),
     "gprtcuDebugScanSkipTile": ([i64], None),
     "gprtcuDebugScanImpl": ([i32], None),

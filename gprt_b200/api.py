@@ -338,3 +338,26 @@ def wide_decode(wide):
     qhi = raw[:, 56:80].reshape(cnt, 3, 8)
     return dict(count=cnt, p=f, e=e, imask=imask, child_base=cb, leaf_base=lb, meta=meta, qlo=qlo, qhi=qhi,
                 roots=wide.roots.cpu().numpy(), leaf=wide.leaf.cpu().numpy())
+
+
+# ---------------------------------------------------------------- device scene generators
+def gen_soup(n, seed=0, sigma=0.002, tri_off=None, meshes=1, spacing=2.0, device="cuda"):
+    pos = torch.empty((3 * n, 3), dtype=torch.float32, device=device)
+    tri = torch.empty((n, 3), dtype=torch.int32, device=device)
+    _check(lib().gprtcuGenSoup(n, seed, sigma, _ptr(tri_off), meshes, spacing, _ptr(pos), _ptr(tri), _stream()),
+           "gprtcuGenSoup")
+    return pos, tri
+
+
+def gen_mixture(n, clusters=64, seed=0, edge_sigma=0.001, device="cuda"):
+    pos = torch.empty((3 * n, 3), dtype=torch.float32, device=device)
+    tri = torch.empty((n, 3), dtype=torch.int32, device=device)
+    _check(lib().gprtcuGenMixture(n, clusters, seed, edge_sigma, _ptr(pos), _ptr(tri), _stream()), "gprtcuGenMixture")
+    return pos, tri
+
+
+def gen_rays(nrays, seed=1, ray_off=None, meshes=1, boxes=None, device="cuda"):
+    rays = torch.empty((nrays, 8), dtype=torch.float32, device=device)
+    _check(lib().gprtcuGenRays(nrays, seed, _ptr(ray_off), meshes, _ptr(boxes), _ptr(rays), _stream()),
+           "gprtcuGenRays")
+    return rays

@@ -243,6 +243,29 @@ GPRTCU_API gprtcuStatus gprtcuWideTrace(const gprtcuWideBvh *bvh, const uint32_t
                                         void *scratch, size_t scratchBytes, gprtcuStream stream);
 
 /* ------------------------------------------------------------------------
+ * Seeded synthetic scenes on the device (benchmark and test inputs; no
+ * counterpart in the reference, which has no benchmark inputs).
+ * gprtcuGenSoup: n triangles; mesh m (triOffsets NULL = one mesh) inside the
+ *   unit cube at offset (m mod 16, m/16 mod 16, m/256) * spacing; centroid
+ *   uniform, vertices centroid + N(0, sigma^2); indices (3i, 3i+1, 3i+2).
+ * gprtcuGenMixture: n triangles of a `clusters`-component Gaussian mixture
+ *   (centres uniform in [0,1]^3, sigma uniform in [0.005, 0.05], equal
+ *   weights, consecutive triangles in the same cluster), vertices centroid
+ *   + N(0, edgeSigma^2).
+ * gprtcuGenRays: rays per mesh box (meshBoxes float[numMeshes][6], NULL =
+ *   the unit cube): origin uniform on the sphere of radius 2 * largest extent
+ *   about the box centre, unit direction towards a uniform point in the box,
+ *   tmin 0, tmax +inf.
+ * ------------------------------------------------------------------------ */
+GPRTCU_API gprtcuStatus gprtcuGenSoup(uint64_t n, uint64_t seed, float sigma, const uint32_t *triOffsets,
+                                      uint32_t numMeshes, float spacing, float *positions, uint32_t *triangles,
+                                      gprtcuStream stream);
+GPRTCU_API gprtcuStatus gprtcuGenMixture(uint64_t n, uint32_t clusters, uint64_t seed, float edgeSigma,
+                                         float *positions, uint32_t *triangles, gprtcuStream stream);
+GPRTCU_API gprtcuStatus gprtcuGenRays(uint64_t numRays, uint64_t seed, const uint32_t *rayOffsets, uint32_t numMeshes,
+                                      const float *meshBoxes, float *rays, gprtcuStream stream);
+
+/* ------------------------------------------------------------------------
  * Test hooks (fault injection without a GPU fault).  Process-wide settings
  * read at launch time by the look-back kernels.
  * gprtcuDebugSetSpinBudget: polls a look-back wait makes before it records
