@@ -43,6 +43,7 @@ SIGNATURES = {
     "gprtcuDebugSetSpinBudget": ([u32], None),
     "gprtcuDebugScanSkipTile": ([i64], None),
     "gprtcuDebugScanImpl": ([i32], None),
+    "gprtcuDebugWideOccupancy": ([i32], None),
 }
 
 

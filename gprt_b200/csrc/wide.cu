@@ -254,8 +254,10 @@ __device__ __forceinline__ void wide_leaf_test(const float4 *leaf, uint32_t i, c
   }
 }
 
-template <bool ANY, bool BATCHED>
-__global__ void __launch_bounds__(kWideThreads) k_trace_wide(const WideNode *nodes, const float4 *leaf,
+// MINB: minimum resident CTAs per SM requested from the register allocator
+// (1: no cap, 8: at most 64 registers).
+template <bool ANY, bool BATCHED, int MINB>
+__global__ void __launch_bounds__(kWideThreads, MINB) k_trace_wide(const WideNode *nodes, const float4 *leaf,
                                                             const uint32_t *roots, const uint32_t *ray_off,
                                                             uint32_t meshes, const float4 *rays, uint64_t nrays,
                                                             Hit *hits, unsigned long long *counter, uint32_t *err) {
@@ -301,6 +303,32 @@ __global__ void __launch_bounds__(kWideThreads) k_trace_wide(const WideNode *nod
         const uint32_t meta_lo = w1.z, meta_hi = w1.w;
         const uint32_t qlx[2] = {w2.x, w2.y}, qly[2] = {w2.z, w2.w}, qlz[2] = {w3.x, w3.y};
         const uint32_t qhx[2] = {w3.z, w3.w}, qhy[2] = {w4.x, w4.y}, qhz[2] = {w4.z, w4.w};
+        // The ray in this node's quantised frame, per axis: the distance to
+        // the plane p + q*s is A + q*B with A = (p - o)/d and B = s/d (exact,
+        // s a power of two).  The near plane (qlo when 1/d >= 0, else qhi)
+        // takes a lower bound of A and rounds down, the far plane an upper
+        // bound and rounds up, so each child's entry/exit interval contains
+        // the one of its decoded box, which contains its exact box.
+        float An[3], Af[3], Bq[3];
+        uint32_t qn[3][2], qf[3][2];
+        {
+          const float pa[3] = {px, py, pz}, oa[3] = {R.ox, R.oy, R.oz}, ia[3] = {R.ix, R.iy, R.iz};
+          const float sa[3] = {sx, sy, sz};
+          const uint32_t ql[3][2] = {{qlx[0], qlx[1]}, {qly[0], qly[1]}, {qlz[0], qlz[1]}};
+          const uint32_t qh[3][2] = {{qhx[0], qhx[1]}, {qhy[0], qhy[1]}, {qhz[0], qhz[1]}};
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const float dlo = __fsub_rd(pa[a], oa[a]), dhi = __fsub_ru(pa[a], oa[a]);
+            const bool pos = !(ia[a] < 0.0f);
+            An[a] = __fmul_rd(pos ? dlo : dhi, ia[a]);
+            Af[a] = __fmul_ru(pos ? dhi : dlo, ia[a]);
+            Bq[a] = __fmul_rn(sa[a], ia[a]);
+            qn[a][0] = pos ? ql[a][0] : qh[a][0];
+            qn[a][1] = pos ? ql[a][1] : qh[a][1];
+            qf[a][0] = pos ? qh[a][0] : ql[a][0];
+            qf[a][1] = pos ? qh[a][1] : ql[a][1];
+          }
+        }
         float ctn[8];
         uint32_t hitmask = 0;  // bit = inner-child rank
         uint32_t rank_of[8];
@@ -310,15 +338,20 @@ __global__ void __launch_bounds__(kWideThreads) k_trace_wide(const WideNode *nod
           rank_of[c] = meta;
           ctn[c] = 0.0f;
           if (meta == 0xFF) continue;
-          const int h = c >> 2, sh = 8 * (c & 3);
-          const float lx = __fmaf_rd((float)((qlx[h] >> sh) & 0xFF), sx, px);
-          const float ly = __fmaf_rd((float)((qly[h] >> sh) & 0xFF), sy, py);
-          const float lz = __fmaf_rd((float)((qlz[h] >> sh) & 0xFF), sz, pz);
-          const float ux = __fmaf_ru((float)((qhx[h] >> sh) & 0xFF), sx, px);
-          const float uy = __fmaf_ru((float)((qhy[h] >> sh) & 0xFF), sy, py);
-          const float uz = __fmaf_ru((float)((qhz[h] >> sh) & 0xFF), sz, pz);
-          float tn;
-          if (ray_box(R, lx, ly, lz, ux, uy, uz, bt, tn) && tn <= bt) {
+          const int h = c >> 2;
+          // byte c&3 of the packed word as an exact float: 2^23 + q, minus 2^23
+          const uint32_t sel = 0x7540u | (uint32_t)(c & 3);
+          float tn = R.tmin, tf = bt;
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const float fn = __fsub_rn(__uint_as_float(__byte_perm(qn[a][h], 0x4B000000u, sel)), 8388608.0f);
+            const float ff = __fsub_rn(__uint_as_float(__byte_perm(qf[a][h], 0x4B000000u, sel)), 8388608.0f);
+            tn = fmaxf(tn, __fmaf_rd(fn, Bq[a], An[a]));
+            tf = fminf(tf, __fmaf_ru(ff, Bq[a], Af[a]));
+          }
+          tn = __fmul_rn(tn, kBoxLo);
+          tf = __fmul_rn(tf, kBoxHi);
+          if (tn <= tf && tn <= bt) {
             if ((imask >> c) & 1u) {
               hitmask |= 1u << meta;
               ctn[c] = tn;
@@ -386,6 +419,11 @@ __global__ void __launch_bounds__(kWideThreads) k_trace_wide(const WideNode *nod
 using namespace gprtcu;
 
 uint32_t gprtcu_spin_budget(void);
+
+// Wide traversal register cap: 8 = at most 64 registers (8 CTAs/SM; the
+// default, measured faster), else none.
+static int g_wide_occupancy = 8;
+extern "C" GPRTCU_API void gprtcuDebugWideOccupancy(int ctasPerSm) { g_wide_occupancy = ctasPerSm; }
 
 namespace {
 
@@ -463,16 +501,27 @@ extern "C" GPRTCU_API gprtcuStatus gprtcuWideTrace(const gprtcuWideBvh *bvh, con
   const int blocks = gprtcu_num_sms() * 8;
   const uint64_t need = (numRays + kWideThreads - 1) / kWideThreads;
   const int grid = (int)(need < (uint64_t)blocks ? need : blocks);
-#define GPRTCU_WTRACE(A, B)                                                                                       \
-  k_trace_wide<A, B><<<grid, kWideThreads, 0, stream>>>((const WideNode *)bvh->nodes, (const float4 *)bvh->leafTris, \
-                                                        bvh->roots, rayOffsets, numMeshes, (const float4 *)rays,     \
-                                                        numRays, (Hit *)hits, counter, &hdr->status)
-  if (numMeshes > 1) {
-    if (anyHit) GPRTCU_WTRACE(true, true);
-    else GPRTCU_WTRACE(false, true);
+#define GPRTCU_WTRACE(A, B, M)                                                                              \
+  k_trace_wide<A, B, M><<<grid, kWideThreads, 0, stream>>>((const WideNode *)bvh->nodes,                      \
+                                                           (const float4 *)bvh->leafTris, bvh->roots, rayOffsets, \
+                                                           numMeshes, (const float4 *)rays, numRays, (Hit *)hits, \
+                                                           counter, &hdr->status)
+  if (g_wide_occupancy == 8) {
+    if (numMeshes > 1) {
+      if (anyHit) GPRTCU_WTRACE(true, true, 8);
+      else GPRTCU_WTRACE(false, true, 8);
+    } else {
+      if (anyHit) GPRTCU_WTRACE(true, false, 8);
+      else GPRTCU_WTRACE(false, false, 8);
+    }
   } else {
-    if (anyHit) GPRTCU_WTRACE(true, false);
-    else GPRTCU_WTRACE(false, false);
+    if (numMeshes > 1) {
+      if (anyHit) GPRTCU_WTRACE(true, true, 1);
+      else GPRTCU_WTRACE(false, true, 1);
+    } else {
+      if (anyHit) GPRTCU_WTRACE(true, false, 1);
+      else GPRTCU_WTRACE(false, false, 1);
+    }
   }
 #undef GPRTCU_WTRACE
   GPRTCU_TRY(cudaGetLastError());
