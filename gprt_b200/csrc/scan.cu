@@ -234,7 +234,6 @@ __global__ void __launch_bounds__(THREADS) k_scan_u32(const uint32_t *__restrict
 // per CTA let seven CTAs share an SM, so many tiles' loads are in flight while
 // other tiles wait on their look-back.
 constexpr int TS_THREADS = 128;
-constexpr int TS_WARPS = TS_THREADS / 32;
 constexpr int TS_ROWS = 16;  // rows of 128 elements per warp
 constexpr size_t TS_SMEM = (size_t)SCAN_TILE * 4;
 
