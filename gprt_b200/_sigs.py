@@ -25,6 +25,12 @@ SIGNATURES = {
     "gprtcuSortKeysU64": ([vp, u64, i32, i32, vp, sz, vp], st),
     "gprtcuSortPairsU64": ([vp, vp, u64, i32, i32, vp, sz, vp], st),
     "gprtcuSortPairsU64U64": ([vp, vp, u64, i32, i32, vp, sz, vp], st),
+    "gprtcuSortConfigCount": ([], i32),
+    "gprtcuSortConfigAt": ([i32, vp], st),
+    "gprtcuSortGetConfig": ([i32, i32, vp], st),
+    "gprtcuSortSetConfig": ([i32, i32, vp], st),
+    "gprtcuSortWithConfig": ([vp, vp, u64, i32, i32, i32, i32, vp, vp, sz, vp], st),
+    "gprtcuSortAutotune": ([i32, i32, u64, i32, vp, i32, vp, vp, vp], st),
     "gprtcuLbvhScratchSize": ([u32], sz),
     "gprtcuLbvhBuildTriangles": ([vp, vp, u32, i32, vp, vp, sz, vp], st),
     "gprtcuLbvhBuildPoints": ([vp, u32, i32, vp, vp, sz, vp], st),

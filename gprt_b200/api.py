@@ -126,6 +126,66 @@ def sort(keys, values=None, begin_bit=0, end_bit=None, scr=None):
     return keys, values
 
 
+class SortConfig(ctypes.Structure):
+    """gprtcuSortConfig (include/gprtcu.h): digit bits, keys per tile, warps per block."""
+    _fields_ = [("digitBits", ctypes.c_int32), ("tile", ctypes.c_int32), ("warps", ctypes.c_int32)]
+
+    def tuple(self):
+        return (self.digitBits, self.tile, self.warps)
+
+
+def sort_configs():
+    """Every shape of the sort's tuning grid as (digit bits, tile, warps)."""
+    out = []
+    for i in range(lib().gprtcuSortConfigCount()):
+        c = SortConfig()
+        _check(lib().gprtcuSortConfigAt(i, ctypes.byref(c)), "gprtcuSortConfigAt")
+        out.append(c.tuple())
+    return out
+
+
+def sort_get_config(key_bytes, value_bytes):
+    c = SortConfig()
+    _check(lib().gprtcuSortGetConfig(key_bytes, value_bytes, ctypes.byref(c)), "gprtcuSortGetConfig")
+    return c.tuple()
+
+
+def sort_set_config(key_bytes, value_bytes, cfg):
+    """Install shape `cfg` (a tuple) for the type pair; None restores the default."""
+    arg = None if cfg is None else ctypes.byref(SortConfig(*cfg))
+    _check(lib().gprtcuSortSetConfig(key_bytes, value_bytes, arg), "gprtcuSortSetConfig")
+
+
+def sort_with_config(keys, values, cfg, begin_bit=0, end_bit=None, scr=None):
+    """One sort with an explicit shape (keys/values as in sort())."""
+    _need_cuda(keys, values)
+    kw = keys.element_size()
+    vw = 0 if values is None else values.element_size()
+    n = keys.numel()
+    if end_bit is None:
+        end_bit = 8 * kw
+    if scr is None:
+        scr = scratch(sort_scratch_size(n, kw, vw), keys.device)
+    _check(lib().gprtcuSortWithConfig(_ptr(keys), _ptr(values), n, kw, vw, begin_bit, end_bit,
+                                      ctypes.byref(SortConfig(*cfg)), _ptr(scr), scr.numel(), _stream()),
+           "gprtcuSortWithConfig")
+    return keys, values
+
+
+def sort_autotune(key_bytes, value_bytes, n, end_bit=None, sample=None, repeats=3):
+    """Time every shape on this device, install the fastest for the type pair.
+    Returns (best shape, {shape: median ms or None if it failed})."""
+    if end_bit is None:
+        end_bit = 8 * key_bytes
+    count = lib().gprtcuSortConfigCount()
+    ms = (ctypes.c_float * count)()
+    best = SortConfig()
+    _check(lib().gprtcuSortAutotune(key_bytes, value_bytes, int(n), end_bit, _ptr(sample), repeats, ms,
+                                    ctypes.byref(best), _stream()), "gprtcuSortAutotune")
+    times = {cfg: (None if ms[i] < 0 else float(ms[i])) for i, cfg in enumerate(sort_configs())}
+    return best.tuple(), times
+
+
 # ---------------------------------------------------------------- LBVH + trace
 class LbvhDesc(ctypes.Structure):
     """gprtcuLbvh (include/gprtcu.h)."""

@@ -1,0 +1,482 @@
+// sort_kernels.cuh -- the radix-sort kernels, templated over the shape the
+// autotuner chooses: digit width RB (4, 6 or 8 bits), warps per block and
+// keys per tile.  Each sort_*.cu file instantiates the whole tuning grid for
+// one key/payload type pair; sort.cu holds the host driver and the tuner.
+//
+// Replaces gprtBufferSort / gprtBufferSortPayload (gprt/gprt_host.h:2384,2416;
+// host driver gprt/gprt.cpp:8821-9073; kernels gprt/gprt_sort.slang:109-637).
+// Same contract: stable ascending sort, result in place in the caller's
+// buffers.  The reference runs FidelityFX's reduce-then-scan with 4-bit
+// digits: five dispatches per digit, 16 passes over 64-bit words.  This is a
+// onesweep design instead (Adinets & Merrill 2022):
+//   1. one histogram kernel reads every key once and builds the digit
+//      histograms of all passes; its last CTA scans them into global digit
+//      offsets and marks passes whose digit is constant (skipped);
+//   2. one digit-binning kernel per pass: a tile of keys and one of payloads
+//      arrive in shared memory by bulk async copies (TMA); warps rank their
+//      keys with a ballot multisplit against per-warp shared histograms,
+//      each digit's tile count is published to a per-(tile, digit) status
+//      word and a decoupled
+//      look-back over earlier tiles gives the digit's global position; keys,
+//      then payloads, are reordered in shared memory so the scatter leaves
+//      the tile as coalesced per-digit runs.
+// Traffic per pass: read + write of keys and payloads; plus one read of the
+// keys for the histograms.
+#pragma once
+#include <array>
+#include <utility>
+
+#include "common.cuh"
+
+namespace gprtcu {
+
+constexpr uint32_t LB_AGG = 1u << 30;
+constexpr uint32_t LB_INC = 2u << 30;
+constexpr uint32_t LB_POISON = 3u << 30;
+constexpr uint32_t LB_VALUE = (1u << 30) - 1;
+constexpr int SORT_MAX_PASSES = 16;
+// Per-pass flag written by the histogram kernel: every key has the same
+// digit, the pass is skipped.
+constexpr uint32_t SORT_FLAG_TRIVIAL = 1u;
+
+// The sort's scratch header: the common 256-byte header (error status first)
+// followed by per-pass tile tickets and ping-pong selectors.  ticket[0] is the
+// histogram kernel's done-counter, ticket[1+p] pass p's tile ticket; sel[p]
+// says which buffer holds pass p's input (sel[passes]: the final result).
+struct SortHeader {
+  ScratchHeader h;
+  uint32_t ticket[SORT_MAX_PASSES + 1];
+  uint32_t sel[SORT_MAX_PASSES + 1];
+  uint32_t pad[64 - 2 * (SORT_MAX_PASSES + 1)];
+};
+static_assert(sizeof(SortHeader) == 512, "sort header is 512 bytes");
+
+// One point of the tuning grid.
+struct SortShape {
+  int rb;     // digit bits
+  int tile;   // keys per tile (one CTA per tile)
+  int warps;  // warps per CTA
+};
+
+// The tuning grid: digit bits {4, 6, 8} x tile {1024 .. 8192} x warps {4, 8,
+// 16}, keeping shapes with 1..32 keys per thread and at least one thread per
+// digit (so 8-bit digits need 8 or 16 warps).
+inline constexpr SortShape kSortGrid[] = {
+    {8, 1024, 8}, {8, 2048, 8}, {8, 4096, 8}, {8, 8192, 8},                   //
+    {8, 1024, 16}, {8, 2048, 16}, {8, 4096, 16}, {8, 8192, 16},               //
+    {6, 1024, 4}, {6, 2048, 4}, {6, 4096, 4},                                 //
+    {6, 1024, 8}, {6, 2048, 8}, {6, 4096, 8}, {6, 8192, 8},                   //
+    {6, 1024, 16}, {6, 2048, 16}, {6, 4096, 16}, {6, 8192, 16},               //
+    {4, 1024, 4}, {4, 2048, 4}, {4, 4096, 4},                                 //
+    {4, 1024, 8}, {4, 2048, 8}, {4, 4096, 8}, {4, 8192, 8},                   //
+    {4, 1024, 16}, {4, 2048, 16}, {4, 4096, 16}, {4, 8192, 16},               //
+};
+inline constexpr int kSortGridSize = (int)(sizeof(kSortGrid) / sizeof(kSortGrid[0]));
+inline constexpr int kSortMinTile = 1024;
+
+// Everything one sort call's kernels need (device pointers into the caller's
+// buffers and the scratch).
+struct SortArgs {
+  void *keys, *keys_alt, *vals, *vals_alt;
+  uint64_t n, tiles;
+  int begin_bit, end_bit, passes;
+  uint32_t *hist;     // [passes][RADIX] digit counts, then global offsets
+  uint32_t *trivial;  // [passes] SORT_FLAG_* bits
+  SortHeader *hdr;
+  uint32_t *status;   // two regions of [tiles][RADIX] look-back words
+  uint32_t budget;
+  int use_bulk;
+  int sms;
+};
+
+using SortRunFn = gprtcuStatus (*)(const SortArgs &, cudaStream_t);
+
+template <typename K> __device__ __forceinline__ uint32_t digit_of(K key, int shift, uint32_t mask) {
+  return (uint32_t)(key >> shift) & mask;
+}
+
+// Lanes of the warp holding the same BITS-bit digit as this lane, among the
+// lanes with valid == true (warp-level multisplit by ballots, one per digit
+// bit).  Replaces __match_any_sync, whose pipe throughput made the ranking
+// issue-bound on sm_100a.
+template <int BITS> __device__ __forceinline__ unsigned warp_peers(uint32_t d, bool valid) {
+  unsigned m = __ballot_sync(FULL_MASK, valid);
+#pragma unroll
+  for (int b = 0; b < BITS; ++b) {
+    const bool bit = (d >> b) & 1u;
+    const unsigned bb = __ballot_sync(FULL_MASK, bit);
+    m &= bit ? bb : ~bb;
+  }
+  return valid ? m : 0u;
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// ---------------------------------------------------------------------------
+// 1. histogram of every pass's digit, one read of the keys
+// ---------------------------------------------------------------------------
+template <typename K, int RB>
+__global__ void __launch_bounds__(512) k_sort_hist(const K *__restrict__ keys, uint64_t n, int begin_bit, int end_bit,
+                                                   int passes, uint32_t *ghist, uint32_t *trivial, SortHeader *hdr) {
+  constexpr int RADIX = 1 << RB;
+  static_assert(SORT_MAX_PASSES * RADIX <= 4096, "histogram fits 16 KB of shared memory");
+  __shared__ uint32_t sh[SORT_MAX_PASSES * RADIX];
+  __shared__ bool s_last;
+  __shared__ uint32_t s_triv[SORT_MAX_PASSES];
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int i = tid; i < passes * RADIX; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  // Grid-stride over all keys; warp-aggregated shared atomics (skewed inputs
+  // put a whole warp on one bin).
+  const uint64_t total = (n + 31) & ~31ull;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + tid; i < total; i += stride) {
+    const bool valid = i < n;
+    K key = valid ? keys[i] : (K)0;
+    for (int p = 0; p < passes; ++p) {
+      const int shift = begin_bit + p * RB;
+      const int bits = min(RB, end_bit - shift);
+      const uint32_t d = valid ? digit_of(key, shift, (1u << bits) - 1u) : 0u;
+      const unsigned peers = warp_peers<RB>(d, valid);
+      if (valid && lane == 31 - __clz(peers)) atomicAdd(&sh[p * RADIX + d], (uint32_t)__popc(peers));
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < passes * RADIX; i += blockDim.x)
+    if (sh[i]) atomicAdd(&ghist[i], sh[i]);
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) s_last = atomicAdd(&hdr->ticket[0], 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  // Last CTA: exclusive scan of each pass's histogram in place, trivial-pass
+  // detection, and the ping-pong selector of every pass.
+  for (int p = tid >> 5; p < passes; p += blockDim.x >> 5) {
+    uint32_t carry = 0, triv = 0;
+    for (int base = 0; base < RADIX; base += 32) {
+      uint32_t c = base + lane < RADIX ? ld_relaxed_u32(&ghist[p * RADIX + base + lane]) : 0u;
+      if ((uint64_t)c == n) triv = 1;
+      uint32_t inc = warp_incl_scan(c, lane);
+      if (base + lane < RADIX) ghist[p * RADIX + base + lane] = carry + inc - c;
+      carry += __shfl_sync(FULL_MASK, inc, 31);
+    }
+    triv = __any_sync(FULL_MASK, triv);
+    if (lane == 0) s_triv[p] = triv ? SORT_FLAG_TRIVIAL : 0u;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t sel = 0;
+    for (int p = 0; p < passes; ++p) {
+      hdr->sel[p] = sel;
+      trivial[p] = s_triv[p];
+      if (!(s_triv[p] & SORT_FLAG_TRIVIAL)) sel ^= 1u;
+    }
+    hdr->sel[passes] = sel;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2. one digit-binning pass
+// ---------------------------------------------------------------------------
+template <typename K, typename V, int RB, int WARPS, int ITEMS> struct PassCfg {
+  static constexpr int RADIX = 1 << RB;
+  static constexpr int THREADS = WARPS * 32;
+  static constexpr int TILE = THREADS * ITEMS;
+  static constexpr int WARP_KEYS = 32 * ITEMS;
+  static constexpr bool HAS_V = sizeof(V) > 1;
+  static constexpr size_t KEY_BYTES = (size_t)TILE * sizeof(K);
+  static constexpr size_t VAL_BYTES = HAS_V ? (size_t)TILE * sizeof(V) : 0;
+  static constexpr size_t HIST_BYTES = (size_t)WARPS * RADIX * 4;
+  static constexpr size_t SMEM = KEY_BYTES + VAL_BYTES + HIST_BYTES + RADIX * 4 /*goff*/ + RADIX * 4 /*tile start*/ +
+                                 16 /*barriers*/;
+  // CTAs per SM the kernel is compiled for: as many as shared memory allows,
+  // up to 2048 threads, and no fewer registers than 64 per thread.
+  static constexpr int SMEM_CTAS = (int)((228 * 1024) / (SMEM + 1024));
+  static constexpr int THREAD_CTAS = 2048 / THREADS;
+  static constexpr int REG_CTAS = 65536 / (THREADS * 64);
+  static constexpr int MIN_CTAS_A = SMEM_CTAS < THREAD_CTAS ? SMEM_CTAS : THREAD_CTAS;
+  static constexpr int MIN_CTAS_B = MIN_CTAS_A < REG_CTAS ? MIN_CTAS_A : REG_CTAS;
+  static constexpr int MIN_CTAS = MIN_CTAS_B < 1 ? 1 : MIN_CTAS_B;
+  static_assert(THREADS >= RADIX, "one thread per digit");
+  static_assert(ITEMS >= 1 && ITEMS <= 32, "1..32 keys per thread");
+};
+
+// Exclusive scan of v over threads [0, RADIX) (RADIX <= THREADS); every
+// thread of the block must call it.
+template <int RADIX>
+__device__ __forceinline__ uint32_t block_excl_scan_digits(uint32_t v, uint32_t *s_tmp) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int DW = RADIX >= 32 ? RADIX / 32 : 1;
+  uint32_t inc = warp_incl_scan(tid < RADIX ? v : 0u, lane);
+  if (tid < RADIX && lane == 31 && DW > 1) s_tmp[warp] = inc;
+  __syncthreads();
+  uint32_t add = 0;
+  if (DW > 1 && tid < RADIX)
+    for (int w = 0; w < warp; ++w) add += s_tmp[w];
+  __syncthreads();
+  return add + inc - v;
+}
+
+template <typename K, typename V, int RB, int WARPS, int ITEMS>
+__global__ void __launch_bounds__(WARPS * 32, (PassCfg<K, V, RB, WARPS, ITEMS>::MIN_CTAS))
+    k_sort_pass(const SortArgs a, int pass, int shift, int bits) {
+  using C = PassCfg<K, V, RB, WARPS, ITEMS>;
+  constexpr int RADIX = C::RADIX, THREADS = C::THREADS, TILE = C::TILE, WK = C::WARP_KEYS;
+  const uint32_t flags = ld_relaxed_u32(&a.trivial[pass]);
+  if (flags & SORT_FLAG_TRIVIAL) return;  // every key has the same digit: nothing moves
+
+  extern __shared__ __align__(128) unsigned char smem[];
+  K *s_keys = reinterpret_cast<K *>(smem);
+  V *s_vals = reinterpret_cast<V *>(smem + C::KEY_BYTES);
+  uint32_t *s_hist = reinterpret_cast<uint32_t *>(smem + C::KEY_BYTES + C::VAL_BYTES);  // [WARPS][RADIX]
+  uint32_t *s_goff = s_hist + WARPS * RADIX;
+  uint32_t *s_tstart = s_goff + RADIX;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(s_tstart + RADIX);
+  __shared__ uint32_t s_tile, s_abort;
+  __shared__ uint32_t s_tmp[32];
+
+  SortHeader *hdr = a.hdr;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t sel = hdr->sel[pass];
+  const K *src_k = static_cast<const K *>(sel ? a.keys_alt : a.keys);
+  K *dst_k = static_cast<K *>(sel ? a.keys : a.keys_alt);
+  const V *src_v = static_cast<const V *>(sel ? a.vals_alt : a.vals);
+  V *dst_v = static_cast<V *>(sel ? a.vals : a.vals_alt);
+  const uint32_t mask = (1u << bits) - 1u;
+  // Look-back words: executed passes alternate between two regions (sel
+  // flips with every executed pass); this pass clears its tile's words of the
+  // other region for the next executed pass.
+  uint32_t *status = a.status + (sel ? a.tiles * RADIX : 0);
+  uint32_t *status_next = a.status + (sel ? 0 : a.tiles * RADIX);
+
+  if (tid == 0) {
+    s_tile = atomicAdd(&hdr->ticket[1 + pass], 1u);
+    s_abort = 0;
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint64_t tile_start = (uint64_t)tile * TILE;
+  const uint32_t tile_n = (uint32_t)min((uint64_t)TILE, a.n - tile_start);
+  const bool bulk = a.use_bulk && tile_n == TILE;
+  if (tid == 0 && bulk) {
+    mbar_arrive_expect_tx(&bars[0], (uint32_t)C::KEY_BYTES);
+    bulk_g2s(s_keys, src_k + tile_start, (uint32_t)C::KEY_BYTES, &bars[0]);
+    if constexpr (C::HAS_V) {
+      mbar_arrive_expect_tx(&bars[1], (uint32_t)C::VAL_BYTES);
+      bulk_g2s(s_vals, src_v + tile_start, (uint32_t)C::VAL_BYTES, &bars[1]);
+    }
+  }
+  for (int i = tid; i < WARPS * RADIX; i += THREADS) s_hist[i] = 0;
+  for (int i = tid; i < RADIX; i += THREADS) status_next[(uint64_t)tile * RADIX + i] = 0;
+  if (!bulk) {
+    for (int i = tid; i < TILE; i += THREADS)
+      if ((uint32_t)i < tile_n) s_keys[i] = src_k[tile_start + i];
+  } else if (!mbar_wait(&bars[0], 0, MBAR_WAIT_BUDGET)) {
+    s_abort = 1;
+  }
+  __syncthreads();
+  if (s_abort) {
+    if (tid == 0) record_error(&hdr->h, GPRTCU_ERR_TIMEOUT);
+    return;
+  }
+
+  // ---- rank: warp w owns tile positions [w*WK, (w+1)*WK), item-major.  A
+  // key's rank within its warp is the warp histogram wh[d] so far plus its
+  // equal-digit lanes below it.
+  K k[ITEMS];
+  uint32_t rank[ITEMS];
+  uint32_t *wh = s_hist + warp * RADIX;
+  const uint32_t lt = lanemask_lt();
+#pragma unroll
+  for (int i = 0; i < ITEMS; ++i) {
+    const uint32_t pos = warp * WK + i * 32 + lane;
+    const bool valid = pos < tile_n;
+    k[i] = valid ? s_keys[pos] : (K)0;
+    const uint32_t d = valid ? digit_of(k[i], shift, mask) : 0u;
+    const unsigned peers = warp_peers<RB>(d, valid);
+    uint32_t base = 0;
+    if (valid) base = wh[d];
+    __syncwarp();
+    if (valid && lane == 31 - __clz(peers)) wh[d] = base + __popc(peers);
+    __syncwarp();
+    rank[i] = base + __popc(peers & lt);
+  }
+  __syncthreads();
+
+  // ---- per digit: warp-exclusive offsets, tile count, publish, look-back.
+  uint32_t tcount = 0;
+  if (tid < RADIX) {
+    uint32_t run = 0;
+#pragma unroll 4
+    for (int w = 0; w < WARPS; ++w) {
+      uint32_t c = s_hist[w * RADIX + tid];
+      s_hist[w * RADIX + tid] = run;
+      run += c;
+    }
+    tcount = run;
+    st_relaxed_u32(status + (uint64_t)tile * RADIX + tid, (tile == 0 ? LB_INC : LB_AGG) | tcount);
+  }
+  const uint32_t tstart = block_excl_scan_digits<RADIX>(tcount, s_tmp);
+  if (tid < RADIX) {
+    uint32_t excl = 0;
+    bool ok = true;
+    if (tile > 0) {
+      // Eight predecessors per probe (loads issued together), nearest first:
+      // the inclusive prefix of a digit can only advance one probe window per
+      // L2 round trip.
+      int64_t j = (int64_t)tile - 1;
+      uint32_t spins = 0;
+      bool done = false;
+      while (!done && ok) {
+        uint32_t s[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          s[c] = j - c >= 0 ? ld_relaxed_u32(status + (uint64_t)(j - c) * RADIX + tid) : LB_INC;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          if (done || !ok) break;
+          uint32_t x = s[c];
+          while ((x & ~LB_VALUE) == 0) {
+            if (++spins > a.budget) {
+              ok = false;
+              break;
+            }
+            x = ld_relaxed_u32(status + (uint64_t)(j - c) * RADIX + tid);
+          }
+          if (!ok) break;
+          const uint32_t f = x & ~LB_VALUE;
+          if (f == LB_POISON) {
+            ok = false;
+            break;
+          }
+          excl += x & LB_VALUE;
+          if (f == LB_INC) done = true;
+        }
+        j -= 8;
+      }
+      st_relaxed_u32(status + (uint64_t)tile * RADIX + tid, ok ? (LB_INC | (excl + tcount)) : LB_POISON);
+      if (!ok) s_abort = 1;
+    }
+    s_tstart[tid] = tstart;
+    // global position of tile-sorted slot p of this digit = s_goff[d] + p
+    // (mod 2^32; the true value is below 2^30)
+    s_goff[tid] = a.hist[pass * RADIX + tid] + excl - tstart;
+  }
+  __syncthreads();
+  if (s_abort) {
+    if (tid == 0) record_error(&hdr->h, GPRTCU_ERR_TIMEOUT);
+    return;
+  }
+
+  // ---- reorder keys in shared memory by (digit, rank), then scatter runs.
+  uint32_t q[ITEMS];
+#pragma unroll
+  for (int i = 0; i < ITEMS; ++i) {
+    const uint32_t pos = warp * WK + i * 32 + lane;
+    if (pos < tile_n) {
+      const uint32_t d = digit_of(k[i], shift, mask);
+      q[i] = s_tstart[d] + s_hist[warp * RADIX + d] + rank[i];
+      s_keys[q[i]] = k[i];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < ITEMS; ++j) {
+    const uint32_t p = j * THREADS + tid;
+    if (p < tile_n) {
+      const K key = s_keys[p];
+      dst_k[s_goff[digit_of(key, shift, mask)] + p] = key;
+    }
+  }
+  if constexpr (C::HAS_V) {
+    V v[ITEMS];
+    if (bulk) {
+      if (!mbar_wait(&bars[1], 0, MBAR_WAIT_BUDGET)) s_abort = 1;
+    } else {
+      for (int i = tid; i < TILE; i += THREADS)
+        if ((uint32_t)i < tile_n) s_vals[i] = src_v[tile_start + i];
+    }
+    __syncthreads();
+    if (s_abort) {
+      if (tid == 0) record_error(&hdr->h, GPRTCU_ERR_TIMEOUT);
+      return;
+    }
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      const uint32_t pos = warp * WK + i * 32 + lane;
+      if (pos < tile_n) v[i] = s_vals[pos];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      const uint32_t pos = warp * WK + i * 32 + lane;
+      if (pos < tile_n) s_vals[q[i]] = v[i];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+      const uint32_t p = j * THREADS + tid;
+      if (p < tile_n) dst_v[s_goff[digit_of(s_keys[p], shift, mask)] + p] = s_vals[p];
+    }
+  }
+}
+
+// Copies the sorted result back into the caller's buffers when the number of
+// executed passes was odd (the data then ended in the alternate buffers).
+template <typename K, typename V>
+__global__ void k_sort_final_copy(K *keys, const K *keys_alt, V *vals, const V *vals_alt, uint64_t n, int passes,
+                                  const SortHeader *hdr) {
+  if (hdr->sel[passes] == 0) return;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    keys[i] = keys_alt[i];
+    if constexpr (sizeof(V) > 1) vals[i] = vals_alt[i];
+  }
+}
+
+// Shared memory a pass kernel of this shape needs.
+template <typename K, typename V, int RB, int WARPS, int ITEMS>
+gprtcuStatus sort_run(const SortArgs &a, cudaStream_t stream) {
+  using C = PassCfg<K, V, RB, WARPS, ITEMS>;
+  static_assert(C::SMEM <= 227 * 1024, "shared memory per CTA");
+  K *keys = static_cast<K *>(a.keys);
+  k_sort_hist<K, RB><<<a.sms * 2, 512, 0, stream>>>(keys, a.n, a.begin_bit, a.end_bit, a.passes, a.hist, a.trivial,
+                                                    a.hdr);
+  GPRTCU_TRY(cudaGetLastError());
+  GPRTCU_TRY(cudaFuncSetAttribute(k_sort_pass<K, V, RB, WARPS, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)C::SMEM));
+  for (int p = 0; p < a.passes; ++p) {
+    const int shift = a.begin_bit + p * RB;
+    const int bits = a.end_bit - shift < RB ? a.end_bit - shift : RB;
+    k_sort_pass<K, V, RB, WARPS, ITEMS><<<(unsigned)a.tiles, C::THREADS, C::SMEM, stream>>>(a, p, shift, bits);
+    GPRTCU_TRY(cudaGetLastError());
+  }
+  k_sort_final_copy<K, V><<<a.sms * 4, 256, 0, stream>>>(keys, static_cast<const K *>(a.keys_alt),
+                                                         static_cast<V *>(a.vals),
+                                                         static_cast<const V *>(a.vals_alt), a.n, a.passes, a.hdr);
+  GPRTCU_TRY(cudaGetLastError());
+  return GPRTCU_OK;
+}
+
+template <typename K, typename V, size_t... I>
+constexpr std::array<SortRunFn, sizeof...(I)> make_sort_table(std::index_sequence<I...>) {
+  return {{&sort_run<K, V, kSortGrid[I].rb, kSortGrid[I].warps, kSortGrid[I].tile / (32 * kSortGrid[I].warps)>...}};
+}
+
+// One table per key/payload type pair (char = no payload), defined in the
+// sort_*.cu files.
+extern const std::array<SortRunFn, kSortGridSize> kSortTableK32;
+extern const std::array<SortRunFn, kSortGridSize> kSortTableK32V32;
+extern const std::array<SortRunFn, kSortGridSize> kSortTableK64;
+extern const std::array<SortRunFn, kSortGridSize> kSortTableK64V32;
+extern const std::array<SortRunFn, kSortGridSize> kSortTableK64V64;
+
+}  // namespace gprtcu

@@ -117,6 +117,42 @@ GPRTCU_API gprtcuStatus gprtcuSortPairsU64(uint64_t *keys, uint32_t *values, uin
 GPRTCU_API gprtcuStatus gprtcuSortPairsU64U64(uint64_t *keys, uint64_t *values, uint64_t n, int beginBit, int endBit,
                                               void *scratch, size_t scratchBytes, gprtcuStream stream);
 
+/* Sort shapes and the autotuner (no counterpart in the reference, whose
+ * FidelityFX sort is fixed at 4-bit digits and 256-thread groups).  A shape is
+ * the digit width (4, 6 or 8 bits), the keys per tile (1024 .. 8192, one
+ * thread block per tile) and the warps per block (4, 8 or 16); the grid holds
+ * the combinations with 1..32 keys per thread and at least one thread per
+ * digit.  Each key/payload type pair has an active shape, used by the entry
+ * points above (and by the LBVH builds, which sort u32/u32 or u64/u32 pairs):
+ * the one installed by gprtcuSortSetConfig or gprtcuSortAutotune, else a
+ * built-in default that depends on n (gprtcuSortGetConfig reports the default
+ * for large n).  gprtcuSortScratchSize covers every shape, so a scratch
+ * buffer stays valid when the active shape changes. */
+typedef struct {
+  int32_t digitBits;
+  int32_t tile;
+  int32_t warps;
+} gprtcuSortConfig;
+GPRTCU_API int gprtcuSortConfigCount(void);
+GPRTCU_API gprtcuStatus gprtcuSortConfigAt(int index, gprtcuSortConfig *cfg);
+GPRTCU_API gprtcuStatus gprtcuSortGetConfig(int keyBytes, int valueBytes, gprtcuSortConfig *cfg);
+/* cfg = NULL restores the built-in default shape. */
+GPRTCU_API gprtcuStatus gprtcuSortSetConfig(int keyBytes, int valueBytes, const gprtcuSortConfig *cfg);
+/* One sort with an explicit shape (keys/values as in the typed entries). */
+GPRTCU_API gprtcuStatus gprtcuSortWithConfig(void *keys, void *values, uint64_t n, int keyBytes, int valueBytes,
+                                             int beginBit, int endBit, const gprtcuSortConfig *cfg, void *scratch,
+                                             size_t scratchBytes, gprtcuStream stream);
+/* Times every shape on n keys of [0, 2^endBit) -- a copy of sampleKeys (device
+ * pointer, n keys) when given, else uniform keys from a fixed seed -- with one
+ * untimed and `repeats` timed runs each (CUDA events on `stream`), installs
+ * the fastest by median as the active shape for the type pair and returns it
+ * in *best.  msPerConfig (optional, gprtcuSortConfigCount() floats) receives
+ * each shape's median, -1 for a shape that failed.  Setup-time call: it
+ * allocates and frees its own device buffers and synchronizes. */
+GPRTCU_API gprtcuStatus gprtcuSortAutotune(int keyBytes, int valueBytes, uint64_t n, int endBit,
+                                           const void *sampleKeys, int repeats, float *msPerConfig,
+                                           gprtcuSortConfig *best, gprtcuStream stream);
+
 /* ------------------------------------------------------------------------
  * LBVH build.  Replaces gprtTriangleLBVHCreate / gprtPointsLBVHCreate +
  * gprtLBVHBuild (gprt/development/gprt_lbvh.h:91-195; kernels

@@ -45,3 +45,31 @@ def test_host_side_argument_checks_without_gpu():
     assert L.gprtcuScanScratchSize(0) == 256
     assert L.gprtcuScanScratchSize(8192) == 256 + 256
     assert L.gprtcuStatusString(4) == b"device-side wait exceeded its budget"
+
+
+def test_sort_tuning_grid_host_side():
+    # host-only calls: the grid, get/set of the active shape, argument checks
+    import ctypes
+    from gprt_b200 import api
+    grid = api.sort_configs()
+    assert len(grid) == len(set(grid))
+    assert {g[0] for g in grid} == {4, 6, 8}
+    assert {g[1] for g in grid} == {1024, 2048, 4096, 8192}
+    assert {g[2] for g in grid} == {4, 8, 16}
+    for rb, tile, warps in grid:
+        items = tile // (32 * warps)
+        assert tile % (32 * warps) == 0 and 1 <= items <= 32 and 32 * warps >= (1 << rb)
+    default = api.sort_get_config(4, 4)
+    assert default in grid
+    api.sort_set_config(4, 4, grid[0])
+    assert api.sort_get_config(4, 4) == grid[0]
+    api.sort_set_config(4, 4, None)
+    assert api.sort_get_config(4, 4) == default
+    L = api.lib()
+    bad = api.SortConfig(5, 1024, 4)
+    assert L.gprtcuSortSetConfig(4, 4, ctypes.byref(bad)) == 1
+    assert L.gprtcuSortSetConfig(4, 8, ctypes.byref(api.SortConfig(*grid[0]))) == 1  # no u32-key/u64-payload
+    assert L.gprtcuSortConfigAt(len(grid), ctypes.byref(bad)) == 1
+    # scratch covers the largest shape: two look-back regions at 1024-key tiles, 8-bit digits
+    n = 1 << 20
+    assert api.sort_scratch_size(n, 4, 4) >= 8 * n + 2 * (n // 1024) * 256 * 4

@@ -148,3 +148,61 @@ def test_sort_host_errors(cuda):
     big = api.scratch(api.sort_scratch_size(100, 4, 0))
     assert L.gprtcuSortKeysU32(api._ptr(k), 100, 0, 33, api._ptr(big), big.numel(), api._stream()) == 1
     assert L.gprtcuSortKeysU32(api._ptr(k), 100, 5, 5, api._ptr(big), big.numel(), api._stream()) == 1
+
+
+_TYPES = [(4, 0), (4, 4), (8, 0), (8, 4), (8, 8)]
+
+
+@pytest.mark.parametrize("kw,vw", _TYPES)
+def test_sort_every_tuning_shape(cuda, kw, vw):
+    # every shape of the tuner's grid is a correct stable sort on ragged sizes
+    import torch
+    from gprt_b200 import api
+    rng = np.random.default_rng(kw * 10 + vw)
+    kdt = np.uint32 if kw == 4 else np.uint64
+    for cfg in api.sort_configs():
+        for n in (cfg[1] - 1, 3 * cfg[1] + 17):
+            if kw == 4:
+                k = rng.integers(0, 2 ** 32, size=n, dtype=np.uint64).astype(np.uint32)
+            else:
+                k = rng.integers(0, 2 ** 63, size=n, dtype=np.uint64) | (rng.integers(0, 2, size=n, dtype=np.uint64) << 63)
+            k[::7] = k[0]  # repeated keys make stability visible
+            v = None
+            if vw:
+                v = np.arange(n, dtype=np.uint32 if vw == 4 else np.uint64)
+            kt = torch.from_numpy(k.view(np.int32 if kw == 4 else np.int64).copy()).cuda()
+            vt = None if v is None else torch.from_numpy(v.view(np.int32 if vw == 4 else np.int64).copy()).cuda()
+            api.sort_with_config(kt, vt, cfg)
+            got = kt.cpu().numpy().view(kdt)
+            if v is None:
+                assert np.array_equal(got, np.sort(k, kind="stable")), (cfg, n)
+            else:
+                ek, ev = oracle.sort(k, v)
+                assert np.array_equal(got, ek), (cfg, n)
+                assert np.array_equal(vt.cpu().numpy().view(v.dtype), ev), (cfg, n)
+
+
+def test_sort_autotune_installs_a_shape(cuda):
+    import torch
+    from gprt_b200 import api
+    try:
+        best, times = api.sort_autotune(4, 4, 1 << 20, repeats=1)
+        assert best in times and times[best] is not None
+        assert all(t is None or t > 0 for t in times.values())
+        assert times[best] == min(t for t in times.values() if t is not None)
+        assert api.sort_get_config(4, 4) == best
+        # a sort through the plain entry point now runs the tuned shape
+        rng = np.random.default_rng(3)
+        k = rng.integers(0, 2 ** 32, size=300001, dtype=np.uint64).astype(np.uint32)
+        v = np.arange(k.size, dtype=np.uint32)
+        gk, gv = _sort_gpu(torch, k, v)
+        ek, ev = oracle.sort(k, v)
+        assert np.array_equal(gk, ek) and np.array_equal(gv, ev)
+        # tuning on caller keys (a device copy is sorted, the sample is untouched)
+        sample = torch.from_numpy(_zipf_u32(rng, 1 << 18).view(np.int32)).cuda()
+        before = sample.clone()
+        best2, _ = api.sort_autotune(4, 0, sample.numel(), sample=sample, repeats=1)
+        assert torch.equal(sample, before) and api.sort_get_config(4, 0) == best2
+    finally:
+        api.sort_set_config(4, 4, None)
+        api.sort_set_config(4, 0, None)
