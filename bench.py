@@ -2,24 +2,36 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-One step = one LBVH build over 262,144 fp32 triangles (bounds, Morton30
-codes, stable code/id radix sort, Karras topology, refit) followed by one
-closest-hit trace of 1,048,576 rays -- the plain LBVH build + trace workload
-(soup of triangles with centroids uniform in the unit cube and vertices
-N(0, 0.002^2) about them; ray origins uniform on the radius-2 sphere, aimed
-at uniform points in the cube).  Synthetic, seeded data; inputs resident in
-HBM when a step starts; L2 (126 MB) flushed by a 256 MB write between steps,
-outside the timed events.
+One step = the large combined workload's batched + quantised pass, replayed
+from one CUDA graph: a batched LBVH build over 67,108,864 fp32 triangles in
+16,384 meshes (bounds, Morton30 codes, segmented 64-bit (mesh, code) radix
+sort, Karras topology, refit), the collapse into 8-wide BVHs with uint8
+outward-rounded child boxes, and the closest-hit trace of 134,217,728 rays
+(2 per triangle, each mesh's rays aimed at its own box).  Triangles: a
+256-cluster Gaussian mixture (centres uniform in [0,1]^3, sigma uniform in
+[0.005, 0.05], edges N(0, 0.001^2)); mesh sizes log-uniform in [64, 65536]
+scaled to the total.  Synthetic, seeded data generated on the device; inputs
+resident in HBM when a step starts; L2 (126 MB) flushed by a 256 MB write
+between steps, outside the timed events.
 
-The JSON line's value is whole-job Mrays/s over build + trace.  It also
-carries:
-  roofline      the trace kernel (the largest share of the step) against the
-                measured HBM copy bandwidth, at 40 algorithmic bytes per ray
-  cpu_baseline  the CPU oracle on this host's cores, bounded ray sample
-  e2e           the same step through the C ABI from pinned host buffers
-                (host->device copies of triangles and rays, device->host
-                copy of the hits inside the timed region)
-  build, trace  the two halves separately (Mprims/s, Mrays/s)
+The JSON line's value is whole-job Mrays/s of that step.  It also carries:
+  roofline      the wide trace kernel (the largest share of the step) against
+                the measured HBM copy bandwidth, at 40 algorithmic bytes per ray
+  plain         the same scene through the single-mesh entry points, one build
+                and one trace per mesh, and the batched binary path; hits of
+                all three compared on every ray
+  t_check       hit distances of a seeded 1% subsample of the hits against an
+                FP64 plane-equation distance
+  cpu_baseline  the CPU oracle on this host's cores, on the first meshes of
+                the same workload (regenerated on the host)
+  e2e           the same step from pinned host buffers: triangles, indices,
+                offsets and rays copied in and the hits copied out inside the
+                timed region
+  gpu_launches  this library's kernels in the timed region, counted from the
+                captured graph's kernel nodes
+  small_lbvh    plain LBVH build + trace, 262,144 triangles, 1,048,576 rays
+  wide_bvh      binary against quantised wide BVH, 16,777,216 triangles and
+                rays, closest and any hit
   sort, scan    268,435,456 Zipf(1.1) uint32 key/payload pairs and a
                 1,073,741,824-element uint32 exclusive sum, GB/s of
                 algorithmic traffic against the measured HBM bandwidth
@@ -41,13 +53,15 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "LBVH build Mprims/s + closest-hit Mrays/s, batched+quantised vs plain; sort GB/s"
-N_TRI = 262_144
-N_RAYS = 1_048_576
 TRACE_BYTES_PER_RAY = 40
 BUILD_BYTES_PER_PRIM = 300
 SORT_N = 268_435_456
 SCAN_N = 1_073_741_824
-WORKLOAD = "plain LBVH build + closest-hit trace: 262,144 fp32 triangles, 1,048,576 rays"
+WORKLOAD = ("large combined, batched + quantised: {tris:,} fp32 triangles in {meshes:,} meshes, {rays:,} "
+            "closest-hit rays; batched LBVH build + 8-wide uint8-quantised collapse + wide trace in one CUDA graph")
+# DRAM bytes of one k_trace_wide launch on this workload, from the ncu capture
+# summarised in profiles/k_trace_wide_large.md (None until captured).
+TRACE_WIDE_DRAM_BYTES = None
 
 
 def measured_peaks():
@@ -118,27 +132,6 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def cpu_baseline(pos, tri, rays, sample_rays):
-    """The CPU oracle (test infrastructure) timed on this host: full build,
-    bounded ray sample, scaled to the whole step."""
-    import oracle
-    oracle.lib()
-    rs = rays[:sample_rays]
-    oracle.lbvh_build_tri(pos, tri)  # warm-up
-    t0 = time.perf_counter()
-    e = oracle.lbvh_build_tri(pos, tri)
-    t1 = time.perf_counter()
-    oracle.trace_lbvh(pos, tri, e, rs)
-    t2 = time.perf_counter()
-    build_s = t1 - t0
-    trace_s = (t2 - t1) * (rays.shape[0] / rs.shape[0])
-    return {"value": rays.shape[0] / (build_s + trace_s) / 1e6, "unit": "Mrays/s", "cores": oracle.num_threads(),
-            "kind": "port",
-            "sample": "full %d-triangle build + closest-hit trace of the first %d of %d rays, trace time scaled "
-                      "to all rays" % (pos.shape[0] // 3 if tri is None else tri.shape[0], rs.shape[0], rays.shape[0]),
-            "build_mprims_s": tri.shape[0] / build_s / 1e6, "trace_mrays_s": rays.shape[0] / trace_s / 1e6}
-
-
 def zipf_keys(n, seed, s=1.1):
     import torch
     g = torch.Generator(device="cuda")
@@ -146,173 +139,6 @@ def zipf_keys(n, seed, s=1.1):
     u = torch.rand(n, generator=g, device="cuda", dtype=torch.float64)
     r = torch.floor((1.0 - u) ** (-1.0 / (s - 1.0))).clamp_(1, 2 ** 32 - 1)
     return (r - 1).to(torch.int64).to(torch.int32)  # wraps to the uint32 bit pattern
-
-
-def run_reference(args, world, rank):
-    if rank != 0:
-        return
-    from gprt_b200 import scenes
-    pos, tri = scenes.soup(N_TRI, seed=0)
-    rays = scenes.rays(N_RAYS, seed=1)
-    sample = 65536
-    vals = []
-    for _ in range(args.warmup):
-        cpu_baseline(pos, tri, rays, sample)
-    for _ in range(args.steps):
-        vals.append(cpu_baseline(pos, tri, rays, sample))
-    v = float(np.median([x["value"] for x in vals]))
-    cb = dict(vals[0])
-    cb["value"] = v
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mrays/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": N_RAYS / v / 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "triangles": N_TRI, "rays": N_RAYS},
-            "cpu_baseline": cb,
-            "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "the reference's GPU path needs Vulkan + slangc (unavailable on this box); this arm is the "
-                    "CPU restatement of its LBVH build with the watertight traversal, all host threads"}
-    print(json.dumps(line), flush=True)
-
-
-def run_b200(args, world, rank, local):
-    import torch
-    import torch.distributed as dist
-
-    import gprt_b200
-    from gprt_b200 import api, scenes
-
-    torch.cuda.set_device(local)
-    gprt_b200.lib()
-    if world > 1:
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
-    dev = torch.device("cuda", local)
-    peak, peak_kind = measured_peaks()
-
-    pos_h, tri_h = scenes.soup(N_TRI, seed=rank)
-    rays_h = scenes.rays(N_RAYS, seed=1000 + rank)
-    pos = torch.from_numpy(pos_h).to(dev)
-    tri = torch.from_numpy(tri_h.view(np.int32)).to(dev)
-    rays = torch.from_numpy(rays_h).to(dev)
-    bvh = api.Lbvh(N_TRI, dev)
-    hits = torch.empty((N_RAYS, 2), dtype=torch.int32, device=dev)
-    tscr = api.scratch(gprt_b200.lib().gprtcuTraceScratchSize(), dev)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    stream = torch.cuda.current_stream()
-
-    def step():
-        api.lbvh_build_triangles(pos, tri, bvh)
-        api.trace(bvh, rays, hits, scr=tscr)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    for _ in range(args.warmup):
-        flush.zero_()
-        step()
-    barrier()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    with Clocks(local) as clk:
-        barrier()
-        for e0, e1, e2 in ev:
-            flush.zero_()
-            e0.record(stream)
-            api.lbvh_build_triangles(pos, tri, bvh)
-            e1.record(stream)
-            api.trace(bvh, rays, hits, scr=tscr)
-            e2.record(stream)
-        barrier()
-    clocks = clk.summary()
-    build_ms = [a.elapsed_time(b) for a, b, _ in ev]
-    trace_ms = [b.elapsed_time(c) for _, b, c in ev]
-    step_ms = sum(build_ms) / len(ev) + sum(trace_ms) / len(ev)
-    total = torch.tensor([step_ms * args.steps], device=dev)
-    if world > 1:
-        dist.all_reduce(total, op=dist.ReduceOp.MAX)
-    step_ms = float(total.item()) / args.steps
-    value = world * N_RAYS / (step_ms * 1e-3) / 1e6
-    trace_avg = sum(trace_ms) / len(trace_ms)
-    build_avg = sum(build_ms) / len(build_ms)
-    launches_per_step = 11  # bounds, codes, sort (hist + 4 passes + final copy), karras, refit, trace
-
-    # ---- end to end through the C ABI from pinned host memory
-    pos_p = torch.from_numpy(pos_h).pin_memory()
-    tri_p = torch.from_numpy(tri_h.view(np.int32)).pin_memory()
-    rays_p = torch.from_numpy(rays_h).pin_memory()
-    hits_p = torch.empty((N_RAYS, 2), dtype=torch.int32).pin_memory()
-    h2d = pos_p.numel() * 4 + tri_p.numel() * 4 + rays_p.numel() * 4
-    d2h = hits_p.numel() * 4
-
-    def e2e_step():
-        pos.copy_(pos_p, non_blocking=True)
-        tri.copy_(tri_p, non_blocking=True)
-        rays.copy_(rays_p, non_blocking=True)
-        step()
-        hits_p.copy_(hits, non_blocking=True)
-
-    for _ in range(max(1, args.warmup)):
-        e2e_step()
-    barrier()
-    e2e_ms = []
-    for _ in range(args.steps):
-        flush.zero_()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        e2e_step()
-        b.record(stream)
-        b.synchronize()
-        e2e_ms.append(a.elapsed_time(b))
-    e2e_t = torch.tensor([sum(e2e_ms)], device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_v = world * N_RAYS / (float(e2e_t.item()) / args.steps * 1e-3) / 1e6
-
-    # ---- parity spot check of this run's output against the oracle (sample)
-    got = api.hits_numpy(hits)
-
-    # ---- sort and scan at the large sizes (rank-local)
-    extra = {}
-    if not args.skip_sortscan:
-        del flush
-        torch.cuda.empty_cache()
-        extra = sortscan(args, dev, peak, rank)
-        flush = None
-
-    if world > 1:
-        dist.barrier()
-    if rank == 0:
-        cb = None
-        if world == 1 and not args.skip_cpu:
-            cb = cpu_baseline(pos_h, tri_h, rays_h, args.cpu_rays)
-        achieved = TRACE_BYTES_PER_RAY * N_RAYS / (trace_avg * 1e-3) / 1e9
-        line = {
-            "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "triangles_per_gpu": N_TRI, "rays_per_gpu": N_RAYS,
-                       "l2": "flushed (256 MB write) between timed steps", "code": "morton30",
-                       "parallelism": "independent scene per GPU" if world > 1 else "single GPU"},
-            "roofline": {"kernel": "k_trace_bin (closest hit)", "bound": "hbm", "achieved": achieved,
-                         "peak": peak, "peak_kind": peak_kind + " hbm_gbs", "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "algorithmic_bytes": "40 B/ray (32 B ray in + 8 B hit out) x 1,048,576 rays per launch",
-                         "launch_ms": trace_avg},
-            "build": {"value": N_TRI / (build_avg * 1e-3) / 1e6, "unit": "Mprims/s", "ms": build_avg,
-                      "algorithmic_gbs": BUILD_BYTES_PER_PRIM * N_TRI / (build_avg * 1e-3) / 1e9},
-            "trace": {"value": N_RAYS / (trace_avg * 1e-3) / 1e6, "unit": "Mrays/s", "ms": trace_avg,
-                      "hit_fraction": float((got["prim"] != 0xFFFFFFFF).mean())},
-            "e2e": {"value": e2e_v, "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-            "gpu_launches": launches_per_step * args.steps,
-            "clocks": clocks,
-            "cpu_baseline": cb,
-        }
-        line.update(extra)
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
 
 
 def sortscan(args, dev, peak, rank):
@@ -371,14 +197,263 @@ def sortscan(args, dev, peak, rank):
     return out
 
 
+
+
+def cpu_sample_run(sample):
+    """The CPU oracle (test infrastructure) over a list of (pos, tri, rays)
+    meshes: a full build and a closest-hit trace of every mesh.  Returns
+    (seconds building, seconds tracing, triangles, rays)."""
+    import oracle
+    tb = tt = 0.0
+    ntri = nray = 0
+    for pos, tri, rays in sample:
+        t0 = time.perf_counter()
+        e = oracle.lbvh_build_tri(pos, tri)
+        t1 = time.perf_counter()
+        oracle.trace_lbvh(pos, tri, e, rays)
+        t2 = time.perf_counter()
+        tb += t1 - t0
+        tt += t2 - t1
+        ntri += tri.shape[0]
+        nray += rays.shape[0]
+    return tb, tt, ntri, nray
+
+
+def cpu_baseline(min_tris, meshes, triangles):
+    import oracle
+    from gprt_b200 import workloads
+    oracle.lib()
+    sample = workloads.large_cpu_sample(min_tris, meshes=meshes, n=triangles)
+    cpu_sample_run(sample[:1])  # warm-up
+    tb, tt, ntri, nray = cpu_sample_run(sample)
+    return {"value": nray / (tb + tt) / 1e6, "unit": "Mrays/s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": "first %d of %d meshes of the same workload (%d triangles, %d rays), regenerated on the "
+                      "host; per mesh a full LBVH build and a closest-hit trace of its rays"
+                      % (len(sample), meshes, ntri, nray),
+            "build_mprims_s": ntri / tb / 1e6, "trace_mrays_s": nray / tt / 1e6}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    import oracle
+    from gprt_b200 import workloads
+    oracle.lib()
+    sample = workloads.large_cpu_sample(args.ref_tris, meshes=args.meshes, n=args.triangles)
+    for _ in range(args.warmup):
+        cpu_sample_run(sample)
+    vals, ms = [], []
+    for _ in range(args.steps):
+        tb, tt, ntri, nray = cpu_sample_run(sample)
+        vals.append(nray / (tb + tt) / 1e6)
+        ms.append((tb + tt) * 1e3)
+    v = float(np.median(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mrays/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.median(ms)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD.format(tris=args.triangles, meshes=args.meshes, rays=2 * args.triangles),
+                       "triangles_per_gpu": args.triangles, "meshes_per_gpu": args.meshes,
+                       "rays_per_gpu": 2 * args.triangles},
+            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": oracle.num_threads(), "kind": "port",
+                             "sample": "first %d of %d meshes (%d triangles, %d rays) per step, regenerated on "
+                                       "the host; per mesh a full LBVH build and a closest-hit trace"
+                                       % (len(sample), args.meshes, ntri, nray)},
+            "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference's GPU path needs Vulkan + slangc (unavailable on this box); this arm is the CPU "
+                    "restatement of its LBVH build with the watertight traversal, on all host threads"}
+    print(json.dumps(line), flush=True)
+
+
+def t_check(sc, frac=0.01, seed=0):
+    """FP64 plane-equation distance against the reported t on a seeded
+    subsample of the hits (prim ids of a batch are mesh-local)."""
+    import torch
+    h = sc.h_q.cpu().numpy()
+    hit = np.nonzero(h[:, 0] != -1)[0]
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(hit, size=max(1, int(frac * hit.size)), replace=False))
+    mesh = np.searchsorted(sc.roff, idx, side="right") - 1
+    prim = sc.off[mesh] + h[idx, 0].astype(np.int64)
+    rays = sc.rays[torch.from_numpy(idx).to(sc.rays.device)].double().cpu().numpy()
+    tri_ix = torch.from_numpy(prim).to(sc.pos.device)
+    v = sc.pos.view(-1, 3, 3)[tri_ix].double().cpu().numpy()
+    o, d = rays[:, 0:3], rays[:, 4:7]
+    n = np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0])
+    t64 = np.einsum("ij,ij->i", v[:, 0] - o, n) / np.einsum("ij,ij->i", d, n)
+    t32 = h[idx, 1].view(np.float32).astype(np.float64)
+    rel = np.abs(t32 - t64) / np.abs(t64)
+    return {"rays_checked": int(idx.size), "max_rel_err": float(rel.max()), "tolerance": 1e-6,
+            "within_tolerance": bool(rel.max() <= 1e-6)}
+
+
+def run_b200(args, world, rank, local):
+    import torch
+    import torch.distributed as dist
+
+    import gprt_b200
+    from gprt_b200 import launches, workloads
+
+    torch.cuda.set_device(local)
+    gprt_b200.lib()
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    peak, peak_kind = measured_peaks()
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    sc = workloads.LargeScene(meshes=args.meshes, n=args.triangles, seed_offset=rank, device=dev)
+    g = sc.capture()
+    names = launches.graph_kernels(g)
+    launches_per_step = sum(c for n, c in names.items() if launches.PREFIX in n)
+    other_kernels = sum(c for n, c in names.items() if launches.PREFIX not in n)
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        g.replay()
+    barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with Clocks(local) as clk:
+        barrier()
+        for e0, e1 in ev:
+            flush.zero_()
+            e0.record(stream)
+            g.replay()
+            e1.record(stream)
+        barrier()
+    clocks = clk.summary()
+    step_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev)) / args.steps
+    value = world * sc.nrays / (step_ms * 1e-3) / 1e6
+
+    # the step's parts, eager, for the roofline and the build rate
+    trace_ms = float(np.mean(workloads.time_steps(sc.trace_quantised, args.steps, 1, flush)))
+    build_ms = float(np.mean(workloads.time_steps(sc.build_quantised, args.steps, 1, flush)))
+    # the plain and batched binary paths on the same scene
+    bat_ms = float(np.mean(workloads.time_steps(sc.batched, args.steps, 1, flush)))
+    plain_steps = max(1, min(args.steps, args.plain_steps))
+    plain_ms = max_over_ranks(np.mean(workloads.time_steps(sc.plain, plain_steps, 1, flush)))
+    g.replay()
+    torch.cuda.synchronize()
+    same_bat = bool(torch.equal(sc.h_plain, sc.h_bat))
+    same_q = bool(torch.equal(sc.h_plain, sc.h_q))
+    hit_fraction = float((sc.h_q[:, 0] != -1).float().mean().item())
+    tchk = t_check(sc)
+    plain_launches, _ = launches.count_kernels(lambda: sc.plain_mesh(0, torch.cuda.current_stream().cuda_stream))
+
+    # ---- end to end from pinned host buffers through the same graph
+    host = {}
+    for name, t in (("pos", sc.pos), ("tri", sc.tri), ("rays", sc.rays), ("ray_off", sc.ray_off),
+                    ("tri_off", sc.batch.tri_off)):
+        h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        h.copy_(t)
+        host[name] = (h, t)
+    hits_p = torch.empty(sc.h_q.shape, dtype=sc.h_q.dtype).pin_memory()
+    h2d = sum(h.numel() * h.element_size() for h, _ in host.values())
+    d2h = hits_p.numel() * hits_p.element_size()
+
+    def e2e_step():
+        for h, d in host.values():
+            d.copy_(h, non_blocking=True)
+        g.replay()
+        hits_p.copy_(sc.h_q, non_blocking=True)
+
+    e2e_ms = max_over_ranks(np.sum(workloads.time_steps(e2e_step, args.steps, max(1, args.warmup), flush))) / args.steps
+    e2e_v = world * sc.nrays / (e2e_ms * 1e-3) / 1e6
+    e2e_ok = bool(torch.equal(hits_p, sc.h_q.cpu()))
+    nrays, ntri, meshes = sc.nrays, sc.n, sc.meshes
+    del host, hits_p, g
+    sc.release()
+    del sc
+    torch.cuda.empty_cache()
+
+    extra = {}
+    if not args.skip_extra:
+        ps = workloads.PlainScene(seed=rank, device=dev)
+        pb = workloads.time_steps(ps.build, args.steps, args.warmup, flush)
+        pt = workloads.time_steps(ps.trace, args.steps, args.warmup, flush)
+        extra["small_lbvh"] = {
+            "triangles": ps.n, "rays": ps.nrays, "build_ms": float(np.mean(pb)), "trace_ms": float(np.mean(pt)),
+            "build_mprims_s": ps.n / np.mean(pb) / 1e3, "trace_mrays_s": ps.nrays / np.mean(pt) / 1e3,
+            "step_mrays_s": ps.nrays / (np.mean(pb) + np.mean(pt)) / 1e3}
+        del ps
+        ws = workloads.WideScene(device=dev)
+        extra["wide_bvh"] = ws.run(steps=2, warmup=1, flush=flush)
+        del ws
+        torch.cuda.empty_cache()
+        del flush
+        torch.cuda.empty_cache()
+        extra.update(sortscan(args, dev, peak, rank))
+    barrier()
+
+    if rank == 0:
+        cb = None
+        if world == 1 and not args.skip_cpu:
+            cb = cpu_baseline(args.cpu_tris, args.meshes, args.triangles)
+        achieved = TRACE_BYTES_PER_RAY * nrays / (trace_ms * 1e-3) / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD.format(tris=ntri, meshes=meshes, rays=nrays),
+                       "triangles_per_gpu": ntri, "meshes_per_gpu": meshes,
+                       "rays_per_gpu": nrays, "l2": "flushed (256 MB write) between timed steps",
+                       "parallelism": "independent scene per GPU" if world > 1 else "single GPU"},
+            "roofline": {"kernel": "k_trace_wide (closest hit, batched)", "bound": "hbm", "achieved": achieved,
+                         "peak": peak, "peak_kind": peak_kind + " hbm_gbs (copy)", "unit": "GB/s",
+                         "frac": achieved / peak,
+                         "traffic": TRACE_WIDE_DRAM_BYTES,
+                         "algorithmic_bytes": "40 B/ray (32 B ray in + 8 B hit out) x %d rays per launch" % nrays,
+                         "launch_ms": trace_ms},
+            "build": {"value": ntri / (build_ms * 1e-3) / 1e6, "unit": "Mprims/s", "ms": build_ms,
+                      "includes": "batched build + wide collapse",
+                      "algorithmic_gbs": BUILD_BYTES_PER_PRIM * ntri / (build_ms * 1e-3) / 1e9},
+            "plain": {"plain_ms": plain_ms, "plain_mrays_s": world * nrays / (plain_ms * 1e-3) / 1e6,
+                      "plain_steps": plain_steps, "plain_launches_per_mesh": plain_launches,
+                      "batched_binary_ms": bat_ms, "batched_binary_mrays_s": nrays / (bat_ms * 1e-3) / 1e6,
+                      "speedup_batched_quantised_vs_plain": plain_ms / step_ms,
+                      "speedup_batched_quantised_vs_batched_binary": bat_ms / step_ms,
+                      "hits_identical_plain_batched": same_bat, "hits_identical_plain_quantised": same_q,
+                      "hit_fraction": hit_fraction},
+            "t_check": tchk,
+            "e2e": {"value": e2e_v, "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "ms_per_step": e2e_ms, "hits_match_device": e2e_ok},
+            "gpu_launches": launches_per_step * args.steps,
+            "gpu_launches_detail": {"per_step": launches_per_step, "other_kernels_in_graph": other_kernels,
+                                    "source": "kernel nodes of the replayed CUDA graph"},
+            "clocks": clocks,
+            "cpu_baseline": cb,
+        }
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--cpu-rays", type=int, default=131072)
-    ap.add_argument("--skip-sortscan", action="store_true")
+    ap.add_argument("--meshes", type=int, default=16_384, help="meshes of the large workload")
+    ap.add_argument("--triangles", type=int, default=67_108_864, help="triangles of the large workload")
+    ap.add_argument("--plain-steps", type=int, default=2, help="timed steps of the per-mesh plain path")
+    ap.add_argument("--cpu-tris", type=int, default=1 << 23, help="triangles in the CPU baseline sample")
+    ap.add_argument("--ref-tris", type=int, default=1 << 20, help="triangles per step of the reference arm")
+    ap.add_argument("--skip-extra", action="store_true", help="only the headline workload")
     ap.add_argument("--skip-cpu", action="store_true")
     args = ap.parse_args()
     world, rank, local = dist_env()

@@ -81,3 +81,77 @@ def batch(sizes, seed=0, sigma=0.002, rays_per_tri=0, spacing=2.0):
     if rays_per_tri:
         return pos, tri, off, np.concatenate(rays_l), ray_off
     return pos, tri, off
+
+
+# ---------------------------------------------------------------------------
+# Host restatement of the device generators (gprt_b200/csrc/gen.cu): the same
+# counter-based SplitMix64 streams and formulas evaluated with numpy, so a CPU
+# process can rebuild any index range of a device-generated scene (the values
+# agree up to the rounding of the device's log/sin/cos/rsqrt).
+# ---------------------------------------------------------------------------
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+_STREAM = np.uint64(0x632BE59BD9B4E019)
+
+
+def _splitmix64(x):
+    x = (x + _GOLDEN).astype(np.uint64)
+    x = (x ^ (x >> np.uint64(30))) * _M1
+    x = (x ^ (x >> np.uint64(27))) * _M2
+    return x ^ (x >> np.uint64(31))
+
+
+def _u01(seed, stream, i):
+    with np.errstate(over="ignore"):
+        h = _splitmix64(np.uint64(seed) ^ _splitmix64(np.uint64(stream) * _STREAM + np.asarray(i, np.uint64)))
+    return (h >> np.uint64(40)).astype(np.float64) * (1.0 / 16777216.0)
+
+
+def _normal2(seed, stream, i):
+    i = np.asarray(i, np.uint64)
+    u = np.maximum(_u01(seed, stream, 2 * i), 1e-7)
+    v = _u01(seed, stream, 2 * i + 1)
+    r = np.sqrt(-2.0 * np.log(u))
+    return r * np.cos(2.0 * np.pi * v), r * np.sin(2.0 * np.pi * v)
+
+
+def device_mixture_range(n, clusters, seed, lo, hi, edge_sigma=0.001):
+    """Triangles [lo, hi) of gprtcuGenMixture(n, clusters, seed, edge_sigma):
+    positions [3*(hi-lo), 3] and local indices."""
+    i = np.arange(lo, hi, dtype=np.uint64)
+    k = (i * np.uint64(clusters)) // np.uint64(n)
+    centre = np.stack([_u01(seed, 10, 3 * k + a) for a in range(3)], axis=1)
+    sg = 0.005 + 0.045 * _u01(seed, 11, k)
+    g = np.empty((i.size, 12))
+    for j in range(6):
+        a, b = _normal2(seed, 12, 6 * i + j)
+        g[:, 2 * j], g[:, 2 * j + 1] = a, b
+    c = centre + sg[:, None] * g[:, 0:3]
+    pos = np.empty((i.size, 3, 3), np.float64)
+    for v in range(3):
+        pos[:, v, :] = c + edge_sigma * g[:, 3 + 3 * v:6 + 3 * v]
+    pos = pos.reshape(-1, 3).astype(np.float32)
+    tri = np.arange(3 * i.size, dtype=np.uint32).reshape(-1, 3)
+    return pos, tri
+
+
+def device_rays_range(seed, lo, hi, box_lo, box_hi):
+    """Rays [lo, hi) of gprtcuGenRays aimed at one box: [hi-lo, 8] float32."""
+    r = np.arange(lo, hi, dtype=np.uint64)
+    box_lo = np.asarray(box_lo, np.float64)
+    box_hi = np.asarray(box_hi, np.float64)
+    ext = float(np.max(box_hi - box_lo))
+    ux, uy = _normal2(seed, 20, 2 * r)
+    uz, _ = _normal2(seed, 20, 2 * r + 1)
+    inv = 1.0 / np.sqrt(np.maximum(ux * ux + uy * uy + uz * uz, 1e-20))
+    centre = 0.5 * (box_lo + box_hi)
+    o = centre + 2.0 * ext * np.stack([ux, uy, uz], axis=1) * inv[:, None]
+    t = box_lo + (box_hi - box_lo) * np.stack([_u01(seed, 21, 3 * r + a) for a in range(3)], axis=1)
+    d = t - o
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    out = np.zeros((r.size, 8), np.float32)
+    out[:, 0:3] = o
+    out[:, 4:7] = d
+    out[:, 7] = np.inf
+    return out

@@ -1,17 +1,21 @@
-"""Timed workloads beyond the headline step (used by bench.py).
+"""The benchmark workloads as device-resident scenes with their timed steps.
 
-  c3  quantised wide BVH: 16,777,216 triangles of a 64-cluster Gaussian
-      mixture, 16,777,216 rays; plain (binary build + binary trace) against
-      quantised (binary build + collapse + wide trace), closest and any hit.
-  c4  large combined: 67,108,864 mixture triangles (256 clusters) split into
-      16,384 meshes of log-uniform size, 134,217,728 rays (2 per triangle,
-      each mesh's rays aimed at that mesh's box):
-        plain     the plain entry points once per mesh (build, then trace):
-                  what a caller of the single-mesh API issues;
-        batched   one batched build + one batched binary trace;
-        batched+q one batched build + collapse + wide trace, captured once in
-                  a CUDA graph and replayed.
-      Hits of all three are compared on every ray (must be identical).
+  PlainScene  plain LBVH build + closest-hit trace: 262,144 soup triangles
+              (centroids uniform in the unit cube, vertices N(0, 0.002^2)
+              about them), 1,048,576 rays from the radius-2 sphere aimed at
+              uniform points in the cube.
+  WideScene   quantised wide BVH: 16,777,216 triangles of a 64-cluster
+              Gaussian mixture, 16,777,216 rays; plain (binary build + binary
+              trace) against quantised (binary build + collapse + wide
+              trace), closest and any hit.
+  LargeScene  large combined: 67,108,864 mixture triangles (256 clusters)
+              split into 16,384 meshes of log-uniform size, 134,217,728 rays
+              (2 per triangle, each mesh's rays aimed at that mesh's box):
+                plain     the single-mesh entry points once per mesh (build,
+                          then trace): what a caller of the plain API issues;
+                batched   one batched build + one batched binary trace;
+                batched+q one batched build + collapse + wide trace, captured
+                          once in a CUDA graph and replayed.
 Every time is device time from CUDA events on the launching stream.
 """
 import ctypes
@@ -19,15 +23,19 @@ import ctypes
 import numpy as np
 import torch
 
-from . import api, lib
+from . import api, lib, scenes
 
 
 def _ev():
     return torch.cuda.Event(enable_timing=True)
 
 
-def _time(fn, steps, warmup, flush=None):
+def time_steps(fn, steps, warmup, flush=None):
+    """Per-step device times (ms) of fn() after `warmup` untimed calls; the L2
+    is flushed (a write larger than it) before every call when flush is given."""
     for _ in range(warmup):
+        if flush is not None:
+            flush.zero_()
         fn()
     ts = []
     for _ in range(steps):
@@ -39,45 +47,75 @@ def _time(fn, steps, warmup, flush=None):
         b.record()
         b.synchronize()
         ts.append(a.elapsed_time(b))
-    return float(np.mean(ts)), ts
+    return ts
 
 
-def c3(steps=2, warmup=1, n=16_777_216, nrays=16_777_216, flush=None):
-    dev = torch.device("cuda")
-    pos, tri = api.gen_mixture(n, clusters=64, seed=3)
-    rays = api.gen_rays(nrays, seed=4)
-    bvh = api.Lbvh(n, dev, with_aabbs=False)
-    wide = api.WideBvh(n, 1, dev)
-    hb = torch.empty((nrays, 2), dtype=torch.int32, device=dev)
-    hw = torch.empty_like(hb)
-    tscr = api.scratch(lib().gprtcuTraceScratchSize(), dev)
-    out = {"triangles": n, "rays": nrays, "clusters": 64}
-    t_build, _ = _time(lambda: api.lbvh_build_triangles(pos, tri, bvh), steps, warmup, flush)
-    t_collapse, _ = _time(lambda: api.wide_build(bvh, wide=wide), steps, warmup, flush)
-    for anyhit in (False, True):
-        key = "any" if anyhit else "closest"
-        t_bin, _ = _time(lambda: api.trace(bvh, rays, hb, anyhit=anyhit, scr=tscr), steps, warmup, flush)
-        t_wide, _ = _time(lambda: api.wide_trace(wide, rays, hits=hw, anyhit=anyhit, scr=tscr), steps, warmup, flush)
-        if anyhit:
-            same = bool(torch.equal(hb[:, 0] == -1, hw[:, 0] == -1))
-        else:
-            same = bool(torch.equal(hb, hw))
-        out[key] = {"plain_trace_ms": t_bin, "quantised_trace_ms": t_wide,
-                    "plain_mrays_s": nrays / (t_build + t_bin) / 1e3,
-                    "quantised_mrays_s": nrays / (t_build + t_collapse + t_wide) / 1e3,
-                    "trace_only_speedup": t_bin / t_wide, "hits_identical": same,
-                    "hit_fraction": float((hw[:, 0] != -1).float().mean().item())}
-    out["build_ms"] = t_build
-    out["collapse_ms"] = t_collapse
-    out["build_mprims_s"] = n / t_build / 1e3
-    torch.cuda.synchronize()
-    out["wide_nodes"] = int(wide.count.item())
-    del pos, tri, rays, bvh, wide, hb, hw
-    torch.cuda.empty_cache()
-    return out
+class PlainScene:
+    def __init__(self, n=262_144, nrays=1_048_576, seed=0, device="cuda"):
+        dev = torch.device(device)
+        self.n, self.nrays = n, nrays
+        self.pos_h, self.tri_h = scenes.soup(n, seed=seed)
+        self.rays_h = scenes.rays(nrays, seed=1000 + seed)
+        self.pos = torch.from_numpy(self.pos_h).to(dev)
+        self.tri = torch.from_numpy(self.tri_h.view(np.int32)).to(dev)
+        self.rays = torch.from_numpy(self.rays_h).to(dev)
+        self.bvh = api.Lbvh(n, dev)
+        self.hits = torch.empty((nrays, 2), dtype=torch.int32, device=dev)
+        self.tscr = api.scratch(lib().gprtcuTraceScratchSize(), dev)
+
+    def build(self):
+        api.lbvh_build_triangles(self.pos, self.tri, self.bvh)
+
+    def trace(self):
+        api.trace(self.bvh, self.rays, self.hits, scr=self.tscr)
+
+    def step(self):
+        self.build()
+        self.trace()
 
 
-def c4_sizes(meshes=16_384, total=67_108_864, seed=2):
+class WideScene:
+    def __init__(self, n=16_777_216, nrays=16_777_216, clusters=64, device="cuda"):
+        dev = torch.device(device)
+        self.n, self.nrays, self.clusters = n, nrays, clusters
+        self.pos, self.tri = api.gen_mixture(n, clusters=clusters, seed=3, device=dev)
+        self.rays = api.gen_rays(nrays, seed=4, device=dev)
+        self.bvh = api.Lbvh(n, dev, with_aabbs=False)
+        self.wide = api.WideBvh(n, 1, dev)
+        self.hb = torch.empty((nrays, 2), dtype=torch.int32, device=dev)
+        self.hw = torch.empty_like(self.hb)
+        self.tscr = api.scratch(lib().gprtcuTraceScratchSize(), dev)
+
+    def run(self, steps=2, warmup=1, flush=None):
+        mean = lambda ts: float(np.mean(ts))
+        out = {"triangles": self.n, "rays": self.nrays, "clusters": self.clusters}
+        t_build = mean(time_steps(lambda: api.lbvh_build_triangles(self.pos, self.tri, self.bvh), steps, warmup, flush))
+        t_collapse = mean(time_steps(lambda: api.wide_build(self.bvh, wide=self.wide), steps, warmup, flush))
+        for anyhit in (False, True):
+            t_bin = mean(time_steps(lambda: api.trace(self.bvh, self.rays, self.hb, anyhit=anyhit, scr=self.tscr),
+                                    steps, warmup, flush))
+            t_wide = mean(time_steps(lambda: api.wide_trace(self.wide, self.rays, hits=self.hw, anyhit=anyhit,
+                                                            scr=self.tscr), steps, warmup, flush))
+            if anyhit:
+                same = bool(torch.equal(self.hb[:, 0] == -1, self.hw[:, 0] == -1))
+            else:
+                same = bool(torch.equal(self.hb, self.hw))
+            out["any" if anyhit else "closest"] = {
+                "plain_trace_ms": t_bin, "quantised_trace_ms": t_wide,
+                "plain_mrays_s": self.nrays / (t_build + t_bin) / 1e3,
+                "quantised_mrays_s": self.nrays / (t_build + t_collapse + t_wide) / 1e3,
+                "trace_only_speedup": t_bin / t_wide, "hits_identical": same,
+                "hit_fraction": float((self.hw[:, 0] != -1).float().mean().item())}
+        out["build_ms"] = t_build
+        out["collapse_ms"] = t_collapse
+        out["build_mprims_s"] = self.n / t_build / 1e3
+        torch.cuda.synchronize()
+        out["wide_nodes"] = int(self.wide.count.item())
+        return out
+
+
+def large_sizes(meshes=16_384, total=67_108_864, seed=2):
+    """Log-uniform mesh sizes in [64, 65536], scaled to sum to `total`."""
     rng = np.random.default_rng(seed)
     s = np.exp(rng.uniform(np.log(64), np.log(65536), size=meshes))
     s = np.maximum(np.floor(s * (total / s.sum())), 2).astype(np.int64)
@@ -85,90 +123,121 @@ def c4_sizes(meshes=16_384, total=67_108_864, seed=2):
     return s
 
 
-def c4(steps=2, warmup=1, meshes=16_384, n=67_108_864, rays_per_tri=2, flush=None):
-    dev = torch.device("cuda")
-    sizes = c4_sizes(meshes, n)
-    off = np.zeros(meshes + 1, np.int64)
-    off[1:] = np.cumsum(sizes)
-    roff = off * rays_per_tri
-    nrays = int(roff[-1])
-    pos, tri = api.gen_mixture(n, clusters=256, seed=5)
-    batch = api.BatchLbvh(off, dev, with_aabbs=False)
-    ray_off = torch.from_numpy(roff.astype(np.uint32).view(np.int32)).to(dev)
-    # per-mesh boxes for aiming the rays: from one batched build
-    api.batch_build_triangles(pos, tri, batch)
-    rays = api.gen_rays(nrays, seed=6, ray_off=ray_off, meshes=meshes, boxes=batch.scene)
-    wide = api.WideBvh(n, meshes, dev)
-    tscr = api.scratch(lib().gprtcuTraceScratchSize(), dev)
-    h_plain = torch.empty((nrays, 2), dtype=torch.int32, device=dev)
-    h_bat = torch.empty_like(h_plain)
-    h_q = torch.empty_like(h_plain)
-    out = {"triangles": n, "meshes": meshes, "rays": nrays, "mesh_sizes": "log-uniform in [64, 65536] scaled to the total",
-           "clusters": 256}
+class LargeScene:
+    TRI_SEED, RAY_SEED, CLUSTERS = 5, 6, 256
+
+    def __init__(self, meshes=16_384, n=67_108_864, rays_per_tri=2, device="cuda", seed_offset=0):
+        dev = torch.device(device)
+        self.dev = dev
+        self.meshes, self.n = meshes, n
+        self.tri_seed = self.TRI_SEED + 1000 * seed_offset
+        self.ray_seed = self.RAY_SEED + 1000 * seed_offset
+        self.sizes = large_sizes(meshes, n)
+        self.off = np.zeros(meshes + 1, np.int64)
+        self.off[1:] = np.cumsum(self.sizes)
+        self.roff = self.off * rays_per_tri
+        self.nrays = int(self.roff[-1])
+        self.pos, self.tri = api.gen_mixture(n, clusters=self.CLUSTERS, seed=self.tri_seed, device=dev)
+        self.batch = api.BatchLbvh(self.off, dev, with_aabbs=False)
+        self.ray_off = torch.from_numpy(self.roff.astype(np.uint32).view(np.int32)).to(dev)
+        api.batch_build_triangles(self.pos, self.tri, self.batch)  # per-mesh boxes to aim the rays at
+        self.rays = api.gen_rays(self.nrays, seed=self.ray_seed, ray_off=self.ray_off, meshes=meshes,
+                                 boxes=self.batch.scene, device=dev)
+        self.wide = api.WideBvh(n, meshes, dev)
+        self.tscr = api.scratch(lib().gprtcuTraceScratchSize(), dev)
+        self.h_plain = torch.empty((self.nrays, 2), dtype=torch.int32, device=dev)
+        self.h_bat = torch.empty_like(self.h_plain)
+        self.h_q = torch.empty_like(self.h_plain)
+        self._plain_ready = False
+        self.graph = None
 
     # ---- plain: one build + one trace per mesh through the single-mesh API
-    L = lib()
-    maxn = int(sizes.max())
-    local_tri = torch.arange(3 * maxn, dtype=torch.int32, device=dev)
-    pscr = api.scratch(L.gprtcuLbvhScratchSize(maxn), dev)
-    descs = []
-    for m in range(meshes):
-        b = int(off[m])
-        d = api.LbvhDesc(0, batch.codes.data_ptr() + 4 * b, batch.ids.data_ptr() + 4 * b,
-                         batch.nodes.data_ptr() + 16 * (2 * b - m), None, None, None,
-                         batch.bvh2.data_ptr() + 64 * (b - m), batch.leaf.data_ptr() + 48 * b)
-        descs.append(d)
-    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-    pos_p, hits_p, rays_p = pos.data_ptr(), h_plain.data_ptr(), rays.data_ptr()
-    build, trace = L.gprtcuLbvhBuildTriangles, L.gprtcuTraceClosest
-    lt, sp, sn, tp, tn = local_tri.data_ptr(), pscr.data_ptr(), pscr.numel(), tscr.data_ptr(), tscr.numel()
+    def _plain_setup(self):
+        L = lib()
+        maxn = int(self.sizes.max())
+        self.local_tri = torch.arange(3 * maxn, dtype=torch.int32, device=self.dev)
+        self.pscr = api.scratch(L.gprtcuLbvhScratchSize(maxn), self.dev)
+        b = self.batch
+        self.descs = []
+        for m in range(self.meshes):
+            o = int(self.off[m])
+            self.descs.append(api.LbvhDesc(0, b.codes.data_ptr() + 4 * o, b.ids.data_ptr() + 4 * o,
+                                           b.nodes.data_ptr() + 16 * (2 * o - m), None, None, None,
+                                           b.bvh2.data_ptr() + 64 * (o - m), b.leaf.data_ptr() + 48 * o))
+        self._plain_ready = True
 
-    def plain():
-        for m in range(meshes):
-            b, cnt = int(off[m]), int(sizes[m])
-            st = build(pos_p + 36 * b, lt, cnt, 0, ctypes.byref(descs[m]), sp, sn, stream)
-            if st:
-                raise RuntimeError("plain build failed: %d" % st)
-            r0, rc = int(roff[m]), int(roff[m + 1] - roff[m])
-            st = trace(ctypes.byref(descs[m]), rays_p + 32 * r0, rc, hits_p + 8 * r0, tp, tn, stream)
-            if st:
-                raise RuntimeError("plain trace failed: %d" % st)
+    def plain_mesh(self, m, stream):
+        L = lib()
+        o, cnt = int(self.off[m]), int(self.sizes[m])
+        st = L.gprtcuLbvhBuildTriangles(self.pos.data_ptr() + 36 * o, self.local_tri.data_ptr(), cnt, 0,
+                                        ctypes.byref(self.descs[m]), self.pscr.data_ptr(), self.pscr.numel(), stream)
+        if st:
+            raise RuntimeError("plain build failed: %d" % st)
+        r0, rc = int(self.roff[m]), int(self.roff[m + 1] - self.roff[m])
+        st = L.gprtcuTraceClosest(ctypes.byref(self.descs[m]), self.rays.data_ptr() + 32 * r0, rc,
+                                  self.h_plain.data_ptr() + 8 * r0, self.tscr.data_ptr(), self.tscr.numel(), stream)
+        if st:
+            raise RuntimeError("plain trace failed: %d" % st)
 
-    t_plain, _ = _time(plain, steps, warmup, flush)
+    def plain(self):
+        if not self._plain_ready:
+            self._plain_setup()
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        for m in range(self.meshes):
+            self.plain_mesh(m, stream)
 
     # ---- batched binary
-    def batched():
-        api.batch_build_triangles(pos, tri, batch)
-        api.batch_trace(batch, rays, ray_off, hits=h_bat, scr=tscr)
+    def batched(self):
+        api.batch_build_triangles(self.pos, self.tri, self.batch)
+        api.batch_trace(self.batch, self.rays, self.ray_off, hits=self.h_bat, scr=self.tscr)
 
-    t_bat, _ = _time(batched, steps, warmup, flush)
+    # ---- batched + quantised
+    def build_quantised(self):
+        api.batch_build_triangles(self.pos, self.tri, self.batch)
+        api.wide_build(self.batch, wide=self.wide)
 
-    # ---- batched + quantised, captured in a CUDA graph
-    def bq():
-        api.batch_build_triangles(pos, tri, batch)
-        api.wide_build(batch, wide=wide)
-        api.wide_trace(wide, rays, ray_off, hits=h_q, scr=tscr)
+    def trace_quantised(self):
+        api.wide_trace(self.wide, self.rays, self.ray_off, hits=self.h_q, scr=self.tscr)
 
-    bq()
-    torch.cuda.synchronize()
-    g = torch.cuda.CUDAGraph()
-    with torch.cuda.graph(g):
-        bq()
-    t_q, _ = _time(g.replay, steps, warmup, flush)
-    torch.cuda.synchronize()
-    same_bat = bool(torch.equal(h_plain, h_bat))
-    same_q = bool(torch.equal(h_plain, h_q))
-    out.update({
-        "plain_ms": t_plain, "batched_ms": t_bat, "batched_quantised_graph_ms": t_q,
-        "plain_mrays_s": nrays / t_plain / 1e3, "batched_mrays_s": nrays / t_bat / 1e3,
-        "batched_quantised_mrays_s": nrays / t_q / 1e3,
-        "speedup_batched_quantised_vs_plain": t_plain / t_q,
-        "speedup_batched_quantised_vs_batched": t_bat / t_q,
-        "hits_identical_plain_batched": same_bat, "hits_identical_plain_quantised": same_q,
-        "hit_fraction": float((h_q[:, 0] != -1).float().mean().item()),
-        "plain_launches_per_step": meshes * 11,
-    })
-    del g
-    del pos, tri, batch, rays, wide, h_plain, h_bat, h_q, pscr, local_tri
-    torch.cuda.empty_cache()
+    def quantised(self):
+        self.build_quantised()
+        self.trace_quantised()
+
+    def capture(self):
+        """Capture the batched + quantised step once into a CUDA graph."""
+        self.quantised()
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph(keep_graph=True)
+        with torch.cuda.graph(self.graph):
+            self.quantised()
+        self.graph.replay()
+        torch.cuda.synchronize()
+        return self.graph
+
+    def release(self):
+        self.graph = None
+        for k in ("pos", "tri", "batch", "rays", "wide", "h_plain", "h_bat", "h_q", "pscr", "local_tri", "descs",
+                  "tscr", "ray_off"):
+            if hasattr(self, k):
+                delattr(self, k)
+        torch.cuda.empty_cache()
+
+
+def large_cpu_sample(min_tris=1 << 21, meshes=16_384, n=67_108_864, rays_per_tri=2, seed_offset=0):
+    """The large workload's first meshes up to `min_tris` triangles, generated
+    on the host only (no device): list of (pos, tri, rays) per mesh."""
+    sizes = large_sizes(meshes, n)
+    off = np.zeros(meshes + 1, np.int64)
+    off[1:] = np.cumsum(sizes)
+    m_end = int(np.searchsorted(off, min_tris)) + 1
+    m_end = min(max(m_end, 1), meshes)
+    tri_seed = LargeScene.TRI_SEED + 1000 * seed_offset
+    ray_seed = LargeScene.RAY_SEED + 1000 * seed_offset
+    out = []
+    for m in range(m_end):
+        lo, hi = int(off[m]), int(off[m + 1])
+        pos, tri = scenes.device_mixture_range(n, LargeScene.CLUSTERS, tri_seed, lo, hi)
+        box = pos.min(axis=0), pos.max(axis=0)
+        rays = scenes.device_rays_range(ray_seed, lo * rays_per_tri, hi * rays_per_tri, *box)
+        out.append((pos, tri, rays))
     return out
