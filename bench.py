@@ -342,15 +342,19 @@ def run_b200(args, world, rank, local):
     build_ms = float(np.mean(workloads.time_steps(sc.build_quantised, args.steps, 1, flush)))
     # the plain and batched binary paths on the same scene
     bat_ms = float(np.mean(workloads.time_steps(sc.batched, args.steps, 1, flush)))
-    plain_steps = max(1, min(args.steps, args.plain_steps))
-    plain_ms = max_over_ranks(np.mean(workloads.time_steps(sc.plain, plain_steps, 1, flush)))
+    plain_steps = min(args.steps, args.plain_steps)
+    plain_ms = None
+    if plain_steps > 0:
+        plain_ms = max_over_ranks(np.mean(workloads.time_steps(sc.plain, plain_steps, 1, flush)))
     g.replay()
     torch.cuda.synchronize()
-    same_bat = bool(torch.equal(sc.h_plain, sc.h_bat))
-    same_q = bool(torch.equal(sc.h_plain, sc.h_q))
+    same_bat = bool(torch.equal(sc.h_plain, sc.h_bat)) if plain_ms is not None else None
+    same_q = bool(torch.equal(sc.h_plain, sc.h_q)) if plain_ms is not None else bool(torch.equal(sc.h_bat, sc.h_q))
     hit_fraction = float((sc.h_q[:, 0] != -1).float().mean().item())
     tchk = t_check(sc)
-    plain_launches, _ = launches.count_kernels(lambda: sc.plain_mesh(0, torch.cuda.current_stream().cuda_stream))
+    plain_launches = None
+    if plain_ms is not None:
+        plain_launches, _ = launches.count_kernels(lambda: sc.plain_mesh(0, torch.cuda.current_stream().cuda_stream))
 
     # ---- end to end from pinned host buffers through the same graph
     host = {}
@@ -419,12 +423,14 @@ def run_b200(args, world, rank, local):
             "build": {"value": ntri / (build_ms * 1e-3) / 1e6, "unit": "Mprims/s", "ms": build_ms,
                       "includes": "batched build + wide collapse",
                       "algorithmic_gbs": BUILD_BYTES_PER_PRIM * ntri / (build_ms * 1e-3) / 1e9},
-            "plain": {"plain_ms": plain_ms, "plain_mrays_s": world * nrays / (plain_ms * 1e-3) / 1e6,
+            "plain": {"plain_ms": plain_ms,
+                      "plain_mrays_s": world * nrays / (plain_ms * 1e-3) / 1e6 if plain_ms else None,
                       "plain_steps": plain_steps, "plain_launches_per_mesh": plain_launches,
                       "batched_binary_ms": bat_ms, "batched_binary_mrays_s": nrays / (bat_ms * 1e-3) / 1e6,
-                      "speedup_batched_quantised_vs_plain": plain_ms / step_ms,
+                      "speedup_batched_quantised_vs_plain": plain_ms / step_ms if plain_ms else None,
                       "speedup_batched_quantised_vs_batched_binary": bat_ms / step_ms,
-                      "hits_identical_plain_batched": same_bat, "hits_identical_plain_quantised": same_q,
+                      "hits_identical_plain_batched": same_bat,
+                      "hits_identical_plain_quantised" if plain_ms else "hits_identical_batched_quantised": same_q,
                       "hit_fraction": hit_fraction},
             "t_check": tchk,
             "e2e": {"value": e2e_v, "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
@@ -450,7 +456,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--meshes", type=int, default=16_384, help="meshes of the large workload")
     ap.add_argument("--triangles", type=int, default=67_108_864, help="triangles of the large workload")
-    ap.add_argument("--plain-steps", type=int, default=2, help="timed steps of the per-mesh plain path")
+    ap.add_argument("--plain-steps", type=int, default=2,
+                    help="timed steps of the per-mesh plain comparison (0: no plain comparison)")
     ap.add_argument("--cpu-tris", type=int, default=1 << 23, help="triangles in the CPU baseline sample")
     ap.add_argument("--ref-tris", type=int, default=1 << 20, help="triangles per step of the reference arm")
     ap.add_argument("--skip-extra", action="store_true", help="only the headline workload")
