@@ -51,6 +51,15 @@ __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p) {
   return v;
 }
 
+// Atomic add with acquire-release semantics at GPU scope: the caller's earlier
+// writes are visible to whoever observes this add, and writes made visible by
+// the add it observes are visible to the caller's later reads.
+__device__ __forceinline__ uint32_t atom_add_acq_rel_u32(uint32_t *p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
 // Streaming 128-bit load through the non-coherent path without L1 allocation
 // (input read exactly once).
 __device__ __forceinline__ uint4 ldg_stream(const uint4 *p) {

@@ -316,70 +316,87 @@ __global__ void __launch_bounds__(256) k_karras(const uint32_t *codes, const uin
 
 // Leaf boxes and the bottom-up union (BuildTriangleHierarchy,
 // gprt/development/gprt_lbvh.hlsl:400-428, with MakeNodes' +-1e38 start
-// :279-285).  One thread per leaf; the second arrival at a node forms it.
+// :279-285).  One thread per leaf (no grid-stride loop: a thread's walk up
+// the tree is a chain of dependent L2 round trips, so the threads must not
+// queue behind each other's walks); the second arrival at a node forms it.
 template <int KIND, bool BATCHED>
 __global__ void __launch_bounds__(256) k_refit(const float *pos, const uint32_t *tri, const uint32_t *ids,
                                                const uint64_t *keys, MeshMap mm, int4 *nodes, float *aabbs,
                                                Bvh2Node *bvh, float4 *leaf_tris, uint32_t *codes_out,
                                                uint32_t *arrivals, float *root_box) {
-  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < mm.n; s += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t m = BATCHED ? mm.mesh_of_prim(s) : 0u;
-    const uint64_t b = BATCHED ? mm.begin(m) : 0;
-    const int64_t N = BATCHED ? mm.count(m) : mm.n;
-    const uint64_t inner_base = b - m, node_base = 2 * b - m;
-    const int64_t i = (int64_t)(s - b);
-    const uint32_t id = ids[s];
-    float v[9], bx[6];
-    prim_box<KIND>(pos, tri, b + id, v, bx);
-    if (BATCHED && codes_out) codes_out[s] = (uint32_t)keys[s];
-    if (leaf_tris) {
-      leaf_tris[3 * s + 0] = make_float4(v[0], v[1], v[2], __uint_as_float(id));
-      leaf_tris[3 * s + 1] = make_float4(v[3], v[4], v[5], 0.0f);
-      leaf_tris[3 * s + 2] = make_float4(v[6], v[7], v[8], 0.0f);
+  const uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (s >= mm.n) return;
+  uint32_t m = 0;
+  if (BATCHED) {
+    const uint64_t key = keys[s];  // (mesh << 32 | code), sorted
+    m = (uint32_t)(key >> 32);
+    if (codes_out) codes_out[s] = (uint32_t)key;
+  }
+  const uint64_t b = BATCHED ? mm.begin(m) : 0;
+  const int64_t N = BATCHED ? mm.count(m) : mm.n;
+  const uint64_t inner_base = b - m, node_base = 2 * b - m;
+  const int64_t i = (int64_t)(s - b);
+  const uint32_t id = ids[s];
+  float v[9], bx[6];
+  prim_box<KIND>(pos, tri, b + id, v, bx);
+  if (leaf_tris) {
+    leaf_tris[3 * s + 0] = make_float4(v[0], v[1], v[2], __uint_as_float(id));
+    leaf_tris[3 * s + 1] = make_float4(v[3], v[4], v[5], 0.0f);
+    leaf_tris[3 * s + 2] = make_float4(v[6], v[7], v[8], 0.0f);
+  }
+  const int64_t leaf = (N - 1) + i;
+  int *nl = reinterpret_cast<int *>(&nodes[node_base + leaf]);
+  nl[0] = -1;
+  nl[1] = -1;
+  nl[3] = (int)id;
+  if (N == 1) nl[2] = -1;
+  if (aabbs)
+    for (int k = 0; k < 6; ++k) aabbs[6 * (node_base + leaf) + k] = bx[k];
+  int64_t child = leaf;
+  int64_t p = N == 1 ? -1 : (int64_t)nl[2];
+  while (p >= 0) {
+    const int4 pn = nodes[node_base + p];
+    const int side = pn.x == (int)child ? 0 : 1;
+    // This child's box goes into its slot of the parent's traversal node (or
+    // is already in the reference-layout array); the release half of the
+    // arrival count publishes it.
+    if (bvh) {
+      float2 *cb = reinterpret_cast<float2 *>(bvh[inner_base + p].box + 6 * side);
+      cb[0] = make_float2(bx[0], bx[1]);
+      cb[1] = make_float2(bx[2], bx[3]);
+      cb[2] = make_float2(bx[4], bx[5]);
     }
-    const int64_t leaf = (N - 1) + i;
-    int *nl = reinterpret_cast<int *>(&nodes[node_base + leaf]);
-    nl[0] = -1;
-    nl[1] = -1;
-    nl[3] = (int)id;
-    if (N == 1) nl[2] = -1;
-    if (aabbs)
-      for (int k = 0; k < 6; ++k) aabbs[6 * (node_base + leaf) + k] = bx[k];
-    int64_t child = leaf;
-    int64_t p = N == 1 ? -1 : (int64_t)nl[2];
-    while (p >= 0) {
-      const int side = nodes[node_base + p].x == (int)child ? 0 : 1;
-      // This child's box goes into its slot of the parent's traversal node
-      // (or is already in the reference-layout array); publish it before
-      // counting the arrival.
-      if (bvh) {
-        float *cb = bvh[inner_base + p].box + 6 * side;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) cb[k] = bx[k];
-      }
-      __threadfence();
-      if (atomicAdd(&arrivals[inner_base + p], 1u) == 0) break;  // first arrival: the sibling finishes the node
-      __threadfence();
-      // Second arrival: read the sibling's box (from L2) and form the union,
-      // starting from +-1e38 exactly as MakeNodes initialises inner boxes.
-      const int64_t sib = side == 0 ? nodes[node_base + p].y : nodes[node_base + p].x;
-      const float *ob = bvh ? bvh[inner_base + p].box + 6 * (1 - side) : aabbs + 6 * (node_base + sib);
-      float sb[6];
-#pragma unroll
-      for (int k = 0; k < 6; ++k) sb[k] = __ldcg(ob + k);
+    if (atom_add_acq_rel_u32(&arrivals[inner_base + p], 1u) == 0) break;  // first arrival: the sibling finishes
+    // Second arrival (the acquire half makes the sibling's box visible): read
+    // it from L2 and form the union, starting from +-1e38 exactly as
+    // MakeNodes initialises inner boxes.
+    const int64_t sib = side == 0 ? pn.y : pn.x;
+    const float *ob = bvh ? bvh[inner_base + p].box + 6 * (1 - side) : aabbs + 6 * (node_base + sib);
+    float sb[6];
+    if (bvh) {
+      const float2 *o2 = reinterpret_cast<const float2 *>(ob);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        bx[k] = fminf(1e38f, fminf(bx[k], sb[k]));
-        bx[3 + k] = fmaxf(-1e38f, fmaxf(bx[3 + k], sb[3 + k]));
+        const float2 t = __ldcg(o2 + k);
+        sb[2 * k] = t.x;
+        sb[2 * k + 1] = t.y;
       }
-      if (aabbs)
-        for (int k = 0; k < 6; ++k) aabbs[6 * (node_base + p) + k] = bx[k];
-      child = p;
-      p = nodes[node_base + p].z;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) sb[k] = __ldcg(ob + k);
     }
-    if (p < 0 && child == 0 && root_box)
-      for (int k = 0; k < 6; ++k) root_box[6 * (size_t)m + k] = bx[k];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      bx[k] = fminf(1e38f, fminf(bx[k], sb[k]));
+      bx[3 + k] = fmaxf(-1e38f, fmaxf(bx[3 + k], sb[3 + k]));
+    }
+    if (aabbs)
+      for (int k = 0; k < 6; ++k) aabbs[6 * (node_base + p) + k] = bx[k];
+    child = p;
+    p = pn.z;
   }
+  if (p < 0 && child == 0 && root_box)
+    for (int k = 0; k < 6; ++k) root_box[6 * (size_t)m + k] = bx[k];
 }
 
 }  // namespace gprtcu
@@ -431,11 +448,11 @@ void launch_build(const float *pos, const uint32_t *tri, MeshMap mm, int codeKin
                                                   out->sceneBounds);
   } else {
     if (mm.n > mm.meshes)
-      k_karras<BATCHED><<<grid_for(mm.n - mm.meshes, 256, 8), 256, 0, stream>>>(out->codes, keys, mm, nodes,
-                                                                                  (Bvh2Node *)out->bvh2);
-    k_refit<KIND, BATCHED><<<g, 256, 0, stream>>>(pos, tri, out->ids, keys, mm, nodes, out->aabbs,
-                                                  (Bvh2Node *)out->bvh2, (float4 *)out->leafTris, out->codes,
-                                                  arrivals, out->rootBox);
+      k_karras<BATCHED><<<(unsigned)((mm.n - mm.meshes + 255) / 256), 256, 0, stream>>>(out->codes, keys, mm, nodes,
+                                                                                         (Bvh2Node *)out->bvh2);
+    k_refit<KIND, BATCHED><<<(unsigned)((mm.n + 255) / 256), 256, 0, stream>>>(
+        pos, tri, out->ids, keys, mm, nodes, out->aabbs, (Bvh2Node *)out->bvh2, (float4 *)out->leafTris, out->codes,
+        arrivals, out->rootBox);
   }
 }
 
