@@ -49,7 +49,6 @@ SIGNATURES = {
     "gprtcuDebugSetSpinBudget": ([u32], None),
     "gprtcuDebugScanSkipTile": ([i64], None),
     "gprtcuDebugScanImpl": ([i32], None),
-    "gprtcuDebugWideOccupancy": ([i32], None),
 }
 
 

@@ -238,6 +238,7 @@ __global__ void __launch_bounds__(128) k_wide_collapse(const Bvh2Node *bvh2, con
 // ---------------------------------------------------------------------------
 constexpr int kWideThreads = 128;
 constexpr int kWideStack = 64;
+constexpr int kWideRefill = 8;
 
 __device__ __forceinline__ float scale_of(int8_t e) { return __int_as_float(((int)e + 127) << 23); }
 
@@ -254,162 +255,185 @@ __device__ __forceinline__ void wide_leaf_test(const float4 *leaf, uint32_t i, c
   }
 }
 
-// MINB: minimum resident CTAs per SM requested from the register allocator
-// (1: no cap, 8: at most 64 registers).
-template <bool ANY, bool BATCHED, int MINB>
-__global__ void __launch_bounds__(kWideThreads, MINB) k_trace_wide(const WideNode *nodes, const float4 *leaf,
-                                                            const uint32_t *roots, const uint32_t *ray_off,
-                                                            uint32_t meshes, const float4 *rays, uint64_t nrays,
-                                                            Hit *hits, unsigned long long *counter, uint32_t *err) {
+// One lane per ray.  Per node: the ray is moved into the node's quantised
+// frame once, the eight child boxes are tested, and only then are the hit
+// leaf children's triangles tested (the lanes with leaf hits run those tests
+// together, whatever slots they are in; testing them inside the child loop
+// ran each slot's test separately with few lanes active).  The nearest hit
+// inner child is entered and the others are pushed as one entry {child_base,
+// mask of inner-child ranks}.  Lanes are refilled as their rays finish: when
+// at least kWideRefill lanes of a warp are idle, the warp takes that many
+// new rays from the global counter (waiting for the whole warp to finish left
+// most lanes idle behind the longest ray).  On 16.7M rays of one 16.7M-
+// triangle mesh and on 134M rays over 16,384 meshes, thresholds of 4, 8, 16
+// and 32 (no refill) idle lanes measured 33.6 / 34.7 / 38.5 / 63.7 ms and
+// 71.3 / 69.0 / 74.8 / 155.5 ms; testing leaf triangles inside the child loop
+// instead measured 174.7 ms on the second.
+template <bool ANY, bool BATCHED>
+__global__ void __launch_bounds__(kWideThreads, 8)
+    k_trace_wide(const WideNode *nodes, const float4 *leaf, const uint32_t *roots, const uint32_t *ray_off,
+                    uint32_t meshes, const float4 *rays, uint64_t nrays, Hit *hits, unsigned long long *counter,
+                    uint32_t *err) {
   const int lane = threadIdx.x & 31;
+  const uint32_t lt = (1u << lane) - 1u;
+  bool active = false, drained = false;
+  uint64_t r = 0;
+  Ray R;
+  uint32_t node = 0, best = kMiss, best_leaf = 0;
+  float bt = 0.0f;
+  uint2 stack[kWideStack];  // {child_base, mask of inner-child ranks still to visit}
+  int sp = 0;
   while (true) {
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(counter, 32ull);
-    base = __shfl_sync(FULL_MASK, base, 0);
-    if (base >= nrays) break;
-    const uint64_t r = base + lane;
-    const bool active = r < nrays;
-    Ray R;
-    ray_setup(active ? __ldg(rays + 2 * r) : make_float4(0.f, 0.f, 0.f, 1.f),
-              active ? __ldg(rays + 2 * r + 1) : make_float4(1.f, 0.f, 0.f, 0.f), R);
-    uint32_t node = 0;
-    if (active) {
-      uint32_t m = 0;
-      if (BATCHED) {
-        uint32_t lo = 0, hi = meshes;
-        while (hi - lo > 1) {
-          const uint32_t mid = (lo + hi) >> 1;
-          if (__ldg(ray_off + mid) <= r) lo = mid;
-          else hi = mid;
-        }
-        m = lo;
-      }
-      node = __ldg(roots + m);
-    }
-    uint32_t best = kMiss, best_leaf = 0;
-    float bt = R.tmax;
-    bool done = !active;
-    uint2 stack[kWideStack];  // {child_base, mask of inner children still to visit}
-    int sp = 0;
-    while (__any_sync(FULL_MASK, !done)) {
-      if (!done) {
-        const uint4 *np = reinterpret_cast<const uint4 *>(nodes + node);
-        const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
-        const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
-        const float sx = scale_of((int8_t)(w0.w & 0xFF)), sy = scale_of((int8_t)((w0.w >> 8) & 0xFF)),
-                    sz = scale_of((int8_t)((w0.w >> 16) & 0xFF));
-        const uint32_t imask = w0.w >> 24;
-        const uint32_t child_base = w1.x, leaf_base = w1.y;
-        const uint32_t meta_lo = w1.z, meta_hi = w1.w;
-        const uint32_t qlx[2] = {w2.x, w2.y}, qly[2] = {w2.z, w2.w}, qlz[2] = {w3.x, w3.y};
-        const uint32_t qhx[2] = {w3.z, w3.w}, qhy[2] = {w4.x, w4.y}, qhz[2] = {w4.z, w4.w};
-        // The ray in this node's quantised frame, per axis: the distance to
-        // the plane p + q*s is A + q*B with A = (p - o)/d and B = s/d (exact,
-        // s a power of two).  The near plane (qlo when 1/d >= 0, else qhi)
-        // takes a lower bound of A and rounds down, the far plane an upper
-        // bound and rounds up, so each child's entry/exit interval contains
-        // the one of its decoded box, which contains its exact box.
-        float An[3], Af[3], Bq[3];
-        uint32_t qn[3][2], qf[3][2];
-        {
-          const float pa[3] = {px, py, pz}, oa[3] = {R.ox, R.oy, R.oz}, ia[3] = {R.ix, R.iy, R.iz};
-          const float sa[3] = {sx, sy, sz};
-          const uint32_t ql[3][2] = {{qlx[0], qlx[1]}, {qly[0], qly[1]}, {qlz[0], qlz[1]}};
-          const uint32_t qh[3][2] = {{qhx[0], qhx[1]}, {qhy[0], qhy[1]}, {qhz[0], qhz[1]}};
-#pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            const float dlo = __fsub_rd(pa[a], oa[a]), dhi = __fsub_ru(pa[a], oa[a]);
-            const bool pos = !(ia[a] < 0.0f);
-            An[a] = __fmul_rd(pos ? dlo : dhi, ia[a]);
-            Af[a] = __fmul_ru(pos ? dhi : dlo, ia[a]);
-            Bq[a] = __fmul_rn(sa[a], ia[a]);
-            qn[a][0] = pos ? ql[a][0] : qh[a][0];
-            qn[a][1] = pos ? ql[a][1] : qh[a][1];
-            qf[a][0] = pos ? qh[a][0] : ql[a][0];
-            qf[a][1] = pos ? qh[a][1] : ql[a][1];
-          }
-        }
-        float ctn[8];
-        uint32_t hitmask = 0;  // bit = inner-child rank
-        uint32_t rank_of[8];
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          const uint32_t meta = ((c < 4 ? meta_lo : meta_hi) >> (8 * (c & 3))) & 0xFF;
-          rank_of[c] = meta;
-          ctn[c] = 0.0f;
-          if (meta == 0xFF) continue;
-          const int h = c >> 2;
-          // byte c&3 of the packed word as an exact float: 2^23 + q, minus 2^23
-          const uint32_t sel = 0x7540u | (uint32_t)(c & 3);
-          float tn = R.tmin, tf = bt;
-#pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            const float fn = __fsub_rn(__uint_as_float(__byte_perm(qn[a][h], 0x4B000000u, sel)), 8388608.0f);
-            const float ff = __fsub_rn(__uint_as_float(__byte_perm(qf[a][h], 0x4B000000u, sel)), 8388608.0f);
-            tn = fmaxf(tn, __fmaf_rd(fn, Bq[a], An[a]));
-            tf = fminf(tf, __fmaf_ru(ff, Bq[a], Af[a]));
-          }
-          tn = __fmul_rn(tn, kBoxLo);
-          tf = __fmul_rn(tf, kBoxHi);
-          if (tn <= tf && tn <= bt) {
-            if ((imask >> c) & 1u) {
-              hitmask |= 1u << meta;
-              ctn[c] = tn;
-            } else {
-              wide_leaf_test(leaf, leaf_base + meta, R, best, best_leaf, bt);
+    const unsigned idle = __ballot_sync(FULL_MASK, !active);
+    const int n_idle = __popc(idle);
+    if (!drained && (n_idle >= kWideRefill || n_idle == 32)) {
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(counter, (unsigned long long)n_idle);
+      base = __shfl_sync(FULL_MASK, base, 0);
+      if (base + n_idle >= nrays) drained = true;
+      if (!active) {
+        const uint64_t mine = base + __popc(idle & lt);
+        if (mine < nrays) {
+          r = mine;
+          active = true;
+          ray_setup(__ldg(rays + 2 * r), __ldg(rays + 2 * r + 1), R);
+          uint32_t m = 0;
+          if (BATCHED) {
+            uint32_t lo = 0, hi = meshes;
+            while (hi - lo > 1) {
+              const uint32_t mid = (lo + hi) >> 1;
+              if (__ldg(ray_off + mid) <= r) lo = mid;
+              else hi = mid;
             }
+            m = lo;
           }
+          node = __ldg(roots + m);
+          best = kMiss;
+          best_leaf = 0;
+          bt = R.tmax;
+          sp = 0;
         }
-        if (ANY && best != kMiss) {
-          done = true;
+      }
+    }
+    if (!__any_sync(FULL_MASK, active)) {
+      if (drained) break;
+      continue;
+    }
+    if (!active) continue;
+
+    const uint4 *np = reinterpret_cast<const uint4 *>(nodes + node);
+    const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+    const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
+    const float sx = scale_of((int8_t)(w0.w & 0xFF)), sy = scale_of((int8_t)((w0.w >> 8) & 0xFF)),
+                sz = scale_of((int8_t)((w0.w >> 16) & 0xFF));
+    const uint32_t imask = w0.w >> 24;
+    const uint32_t child_base = w1.x, leaf_base = w1.y;
+    const uint32_t meta_lo = w1.z, meta_hi = w1.w;
+    float An[3], Af[3], Bq[3];
+    uint32_t qn[3][2], qf[3][2];
+    {
+      const float pa[3] = {px, py, pz}, oa[3] = {R.ox, R.oy, R.oz}, ia[3] = {R.ix, R.iy, R.iz};
+      const float sa[3] = {sx, sy, sz};
+      const uint32_t ql[3][2] = {{w2.x, w2.y}, {w2.z, w2.w}, {w3.x, w3.y}};
+      const uint32_t qh[3][2] = {{w3.z, w3.w}, {w4.x, w4.y}, {w4.z, w4.w}};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float dlo = __fsub_rd(pa[a], oa[a]), dhi = __fsub_ru(pa[a], oa[a]);
+        const bool pos = !(ia[a] < 0.0f);
+        An[a] = __fmul_rd(pos ? dlo : dhi, ia[a]);
+        Af[a] = __fmul_ru(pos ? dhi : dlo, ia[a]);
+        Bq[a] = __fmul_rn(sa[a], ia[a]);
+        qn[a][0] = pos ? ql[a][0] : qh[a][0];
+        qn[a][1] = pos ? ql[a][1] : qh[a][1];
+        qf[a][0] = pos ? qh[a][0] : ql[a][0];
+        qf[a][1] = pos ? qh[a][1] : ql[a][1];
+      }
+    }
+    float ctn[8];
+    uint32_t inner_hit = 0, leaf_hit = 0;  // slot bits
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const uint32_t meta = ((c < 4 ? meta_lo : meta_hi) >> (8 * (c & 3))) & 0xFF;
+      ctn[c] = 0.0f;
+      if (meta == 0xFF) continue;
+      const int h = c >> 2;
+      const uint32_t sel = 0x7540u | (uint32_t)(c & 3);
+      float tn = R.tmin, tf = bt;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float fn = __fsub_rn(__uint_as_float(__byte_perm(qn[a][h], 0x4B000000u, sel)), 8388608.0f);
+        const float ff = __fsub_rn(__uint_as_float(__byte_perm(qf[a][h], 0x4B000000u, sel)), 8388608.0f);
+        tn = fmaxf(tn, __fmaf_rd(fn, Bq[a], An[a]));
+        tf = fminf(tf, __fmaf_ru(ff, Bq[a], Af[a]));
+      }
+      tn = __fmul_rn(tn, kBoxLo);
+      tf = __fmul_rn(tf, kBoxHi);
+      if (tn <= tf && tn <= bt) {
+        if ((imask >> c) & 1u) {
+          inner_hit |= 1u << c;
+          ctn[c] = tn;
         } else {
-          // drop inner children now behind the best hit; descend into the nearest
-          int nearest = -1;
-          float nt = 0.0f;
-#pragma unroll
-          for (int c = 0; c < 8; ++c) {
-            if (!((imask >> c) & 1u) || !((hitmask >> rank_of[c]) & 1u)) continue;
-            if (ctn[c] > bt) {
-              hitmask &= ~(1u << rank_of[c]);
-            } else if (nearest < 0 || ctn[c] < nt) {
-              nearest = (int)rank_of[c];
-              nt = ctn[c];
-            }
-          }
-          if (nearest >= 0) {
-            hitmask &= ~(1u << nearest);
-            if (hitmask) {
-              if (sp < kWideStack) {
-                stack[sp++] = make_uint2(child_base, hitmask);
-              } else {
-                atomicCAS(err, 0u, 5u);  // traversal stack overflow
-                done = true;
-              }
-            }
-            node = child_base + (uint32_t)nearest;
-          } else if (sp > 0) {
-            uint2 &top = stack[sp - 1];
-            const uint32_t rr = __ffs(top.y) - 1;
-            top.y &= top.y - 1;
-            node = top.x + rr;
-            if (top.y == 0) --sp;
-          } else {
-            done = true;
-          }
+          leaf_hit |= 1u << c;
         }
       }
     }
-    if (active) {
-      Hit h;
-      h.prim = best;
-      h.t = __int_as_float(0x7f800000);
+    // deferred triangle tests: lanes with leaf hits run them together
+    while (leaf_hit) {
+      const int c = __ffs(leaf_hit) - 1;
+      leaf_hit &= leaf_hit - 1u;
+      const uint32_t meta = ((c < 4 ? meta_lo : meta_hi) >> (8 * (c & 3))) & 0xFF;
+      wide_leaf_test(leaf, leaf_base + meta, R, best, best_leaf, bt);
+    }
+    bool finished = false;
+    if (ANY && best != kMiss) {
+      finished = true;
+    } else {
+      int nearest = -1;
+      float nt = 0.0f;
+      uint32_t rest = 0;  // inner-child ranks
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (!((inner_hit >> c) & 1u) || ctn[c] > bt) continue;
+        const uint32_t rank = ((c < 4 ? meta_lo : meta_hi) >> (8 * (c & 3))) & 0xFF;
+        rest |= 1u << rank;
+        if (nearest < 0 || ctn[c] < nt) {
+          nearest = (int)rank;
+          nt = ctn[c];
+        }
+      }
+      if (nearest >= 0) {
+        rest &= ~(1u << nearest);
+        if (rest) {
+          if (sp < kWideStack) {
+            stack[sp++] = make_uint2(child_base, rest);
+          } else {
+            atomicCAS(err, 0u, 5u);  // traversal stack overflow
+            finished = true;
+          }
+        }
+        node = child_base + (uint32_t)nearest;
+      } else if (sp > 0) {
+        uint2 &top = stack[sp - 1];
+        const uint32_t rr = __ffs(top.y) - 1;
+        top.y &= top.y - 1;
+        node = top.x + rr;
+        if (top.y == 0) --sp;
+      } else {
+        finished = true;
+      }
+    }
+    if (finished) {
+      Hit out;
+      out.prim = best;
+      out.t = __int_as_float(0x7f800000);
       if (best != kMiss) {
         const float4 a = __ldg(leaf + 3 * (size_t)best_leaf), b = __ldg(leaf + 3 * (size_t)best_leaf + 1),
                      c = __ldg(leaf + 3 * (size_t)best_leaf + 2);
         const float v0[3] = {a.x, a.y, a.z}, v1[3] = {b.x, b.y, b.z}, v2[3] = {c.x, c.y, c.z};
-        h.t = refine_t(R, v0, v1, v2);
+        out.t = refine_t(R, v0, v1, v2);
       }
-      hits[r] = h;
+      hits[r] = out;
+      active = false;
     }
   }
 }
@@ -419,11 +443,6 @@ __global__ void __launch_bounds__(kWideThreads, MINB) k_trace_wide(const WideNod
 using namespace gprtcu;
 
 uint32_t gprtcu_spin_budget(void);
-
-// Wide traversal register cap: 8 = at most 64 registers (8 CTAs/SM; the
-// default, measured faster), else none.
-static int g_wide_occupancy = 8;
-extern "C" GPRTCU_API void gprtcuDebugWideOccupancy(int ctasPerSm) { g_wide_occupancy = ctasPerSm; }
 
 namespace {
 
@@ -498,30 +517,19 @@ extern "C" GPRTCU_API gprtcuStatus gprtcuWideTrace(const gprtcuWideBvh *bvh, con
   ScratchHeader *hdr = (ScratchHeader *)scratch;
   unsigned long long *counter = reinterpret_cast<unsigned long long *>(&hdr->ticket[0]);
   GPRTCU_TRY(cudaMemsetAsync(scratch, 0, sizeof(ScratchHeader), stream));
-  const int blocks = gprtcu_num_sms() * 8;
+  const int blocks = gprtcu_num_sms() * 8;  // 64 registers: 8 CTAs of 128 threads per SM
   const uint64_t need = (numRays + kWideThreads - 1) / kWideThreads;
   const int grid = (int)(need < (uint64_t)blocks ? need : blocks);
-#define GPRTCU_WTRACE(A, B, M)                                                                              \
-  k_trace_wide<A, B, M><<<grid, kWideThreads, 0, stream>>>((const WideNode *)bvh->nodes,                      \
-                                                           (const float4 *)bvh->leafTris, bvh->roots, rayOffsets, \
-                                                           numMeshes, (const float4 *)rays, numRays, (Hit *)hits, \
-                                                           counter, &hdr->status)
-  if (g_wide_occupancy == 8) {
-    if (numMeshes > 1) {
-      if (anyHit) GPRTCU_WTRACE(true, true, 8);
-      else GPRTCU_WTRACE(false, true, 8);
-    } else {
-      if (anyHit) GPRTCU_WTRACE(true, false, 8);
-      else GPRTCU_WTRACE(false, false, 8);
-    }
+#define GPRTCU_WTRACE(A, B)                                                                                       \
+  k_trace_wide<A, B><<<grid, kWideThreads, 0, stream>>>((const WideNode *)bvh->nodes, (const float4 *)bvh->leafTris, \
+                                                        bvh->roots, rayOffsets, numMeshes, (const float4 *)rays,   \
+                                                        numRays, (Hit *)hits, counter, &hdr->status)
+  if (numMeshes > 1) {
+    if (anyHit) GPRTCU_WTRACE(true, true);
+    else GPRTCU_WTRACE(false, true);
   } else {
-    if (numMeshes > 1) {
-      if (anyHit) GPRTCU_WTRACE(true, true, 1);
-      else GPRTCU_WTRACE(false, true, 1);
-    } else {
-      if (anyHit) GPRTCU_WTRACE(true, false, 1);
-      else GPRTCU_WTRACE(false, false, 1);
-    }
+    if (anyHit) GPRTCU_WTRACE(true, false);
+    else GPRTCU_WTRACE(false, false);
   }
 #undef GPRTCU_WTRACE
   GPRTCU_TRY(cudaGetLastError());

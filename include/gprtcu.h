@@ -314,8 +314,6 @@ GPRTCU_API void gprtcuDebugScanSkipTile(int64_t tile);
 /* Scan kernel selection for tests: 0 = TMA-staged tile-per-CTA kernel when
  * in/out are 16-byte aligned (default), 1 = register-staged tile per CTA. */
 GPRTCU_API void gprtcuDebugScanImpl(int impl);
-/* Wide traversal register cap for tuning: 8 = at most 64 registers, else none. */
-GPRTCU_API void gprtcuDebugWideOccupancy(int ctasPerSm);
 
 #ifdef __cplusplus
 }
