@@ -41,11 +41,18 @@ static_assert(sizeof(WideNode) == 80, "80-byte wide node");
 struct WorkItem {
   uint32_t mesh;
   int32_t bref;  // binary inner node (mesh-local) or ~slot for a one-leaf mesh
-  uint32_t wide;
-  uint32_t pad;
 };
 
-enum { Q_HEAD = 0, Q_TAIL = 1, Q_DONE = 2, Q_WIDE = 3, Q_LEAF = 4 };
+// Collapse counters: the current level's items are queue[LO, HI); TAIL is
+// the next free queue slot (= the number of wide nodes so far: a wide node's
+// index is its queue slot), LEAF the next free wide leaf slot, TICKET the
+// level kernel's CTA done-counter.
+enum { C_LO = 0, C_HI = 1, C_TAIL = 2, C_LEAF = 3, C_TICKET = 4 };
+
+// Levels a collapse runs: a binary node splits its keys at the highest
+// differing bit of (30-bit code, 30-bit index), so binary and therefore wide
+// depth stay below 62.
+constexpr int kWideMaxLevels = 62;
 
 __device__ __forceinline__ float box_area(const float *b) {
   const float dx = b[3] - b[0], dy = b[4] - b[1], dz = b[5] - b[2];
@@ -63,121 +70,120 @@ __device__ __forceinline__ int frame_exponent(double ext) {
   return e < -126 ? -126 : (e > 127 ? 127 : e);
 }
 
-__global__ void k_wide_init(const uint32_t *tri_off, uint32_t meshes, uint32_t n, WorkItem *queue, uint32_t *ready,
-                            uint32_t *roots, uint32_t *counters) {
+__global__ void k_wide_init(const uint32_t *tri_off, uint32_t meshes, uint32_t n, WorkItem *queue, uint32_t *roots,
+                            uint32_t *counters) {
   for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < meshes; m += gridDim.x * blockDim.x) {
     const uint32_t cnt = tri_off ? tri_off[m + 1] - tri_off[m] : n;
-    queue[m] = WorkItem{m, cnt == 1 ? ~0 : 0, m, 0};
-    ready[m] = 1;
+    queue[m] = WorkItem{m, cnt == 1 ? ~0 : 0};
     roots[m] = m;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    counters[Q_TAIL] = meshes;
-    counters[Q_WIDE] = meshes;
+    counters[C_LO] = 0;
+    counters[C_HI] = meshes;
+    counters[C_TAIL] = meshes;
+    counters[C_LEAF] = 0;
+    counters[C_TICKET] = 0;
   }
 }
 
-// Persistent top-down collapse.  Every thread is a worker: it takes the next
-// queue slot, waits (bounded) until that item is published or all work is
-// done, expands the binary node greedily -- the inner child of largest
-// surface area is replaced by its two children until there are eight -- then
-// writes the quantised wide node, copies its leaf triangles and publishes its
-// inner children as new items.  All work is done when the number of finished
-// items equals the number of items ever published (read in that order).
-__global__ void __launch_bounds__(128) k_wide_collapse(const Bvh2Node *bvh2, const float4 *leaf_tris,
-                                                       const uint32_t *tri_off, uint32_t n, WideNode *wnodes,
-                                                       float4 *wleaf, WorkItem *queue, uint32_t *ready,
-                                                       uint32_t *counters, uint32_t budget, ScratchHeader *hdr) {
-  while (true) {
-    const uint32_t idx = atomicAdd(&counters[Q_HEAD], 1u);
-    // At most n items ever exist (one per wide node: a root per mesh plus one
-    // per binary inner node), and queue/ready hold exactly n entries.
-    if (idx >= n) return;
-    uint32_t spins = 0;
-    bool have = false;
-    while (true) {
-      if (ld_acquire_u32(&ready[idx])) {
-        have = true;
-        break;
-      }
-      const uint32_t done = ld_acquire_u32(&counters[Q_DONE]);
-      const uint32_t tail = ld_relaxed_u32(&counters[Q_TAIL]);
-      if (done == tail && idx >= tail) break;
-      if (++spins > budget) {
-        record_error(hdr, GPRTCU_ERR_TIMEOUT);
-        break;
-      }
-      __nanosleep(64);
-    }
-    if (!have) return;
-    // Published by another SM: read through L2, not a possibly stale L1 line.
-    const uint4 raw = __ldcg(reinterpret_cast<const uint4 *>(queue + idx));
-    const WorkItem it{raw.x, (int32_t)raw.y, raw.z, 0u};
-    const uint32_t m = it.mesh;
-    const uint32_t b = tri_off ? tri_off[m] : 0u;
-    const Bvh2Node *mb = bvh2 + (b - m);
-    // children: ref (>= 0 inner local, < 0 ~leaf slot) and exact boxes
+// One level of the top-down collapse.  Every item of the level (a binary
+// node that becomes a wide node) is expanded greedily -- the inner child of
+// largest surface area is replaced by its two children until there are
+// eight --, written as a quantised wide node at its queue slot, its leaf
+// triangles copied to the wide leaf array and its inner children appended
+// to the queue as the next level's items.  A warp allocates its children's
+// queue slots and leaf slots with one atomic add each (prefix sums across
+// the lanes); the last CTA to finish advances [LO, HI) to the items just
+// appended.  The levels run as successive launches, so nothing waits on
+// another thread's progress.
+__global__ void __launch_bounds__(128) k_wide_level(const Bvh2Node *bvh2, const float4 *leaf_tris,
+                                                    const uint32_t *tri_off, WideNode *wnodes, float4 *wleaf,
+                                                    WorkItem *queue, uint32_t *counters) {
+  const uint32_t lo = counters[C_LO], hi = counters[C_HI];
+  const int lane = threadIdx.x & 31;
+  const uint32_t total = hi - lo;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); i0 < total; i0 += stride) {
+    const uint32_t idx = lo + i0 + lane;
+    const bool valid = i0 + lane < total;
     int ref[8];
     float box[8][6];
     int cnt = 0;
-    if (it.bref < 0) {
-      const uint32_t slot = (uint32_t)~it.bref;
-      const float4 a = leaf_tris[3 * (size_t)(b + slot)], c = leaf_tris[3 * (size_t)(b + slot) + 1],
-                   d = leaf_tris[3 * (size_t)(b + slot) + 2];
-      ref[0] = it.bref;
-      box[0][0] = fminf(a.x, fminf(c.x, d.x));
-      box[0][1] = fminf(a.y, fminf(c.y, d.y));
-      box[0][2] = fminf(a.z, fminf(c.z, d.z));
-      box[0][3] = fmaxf(a.x, fmaxf(c.x, d.x));
-      box[0][4] = fmaxf(a.y, fmaxf(c.y, d.y));
-      box[0][5] = fmaxf(a.z, fmaxf(c.z, d.z));
-      cnt = 1;
-    } else {
-      const Bvh2Node nd = mb[it.bref];
-      for (int c = 0; c < 2; ++c) {
-        ref[c] = nd.ref[c];
-        for (int k = 0; k < 6; ++k) box[c][k] = nd.box[6 * c + k];
-      }
-      cnt = 2;
-      while (cnt < 8) {
-        int best = -1;
-        float ba = -1.0f;
-        for (int c = 0; c < cnt; ++c)
-          if (ref[c] >= 0) {
-            const float a = box_area(box[c]);
-            if (a > ba) {
-              ba = a;
-              best = c;
+    uint32_t m = 0, b = 0;
+    if (valid) {
+      const WorkItem it = queue[idx];
+      m = it.mesh;
+      b = tri_off ? tri_off[m] : 0u;
+      const Bvh2Node *mb = bvh2 + (b - m);
+      if (it.bref < 0) {
+        const uint32_t slot = (uint32_t)~it.bref;
+        const float4 a = leaf_tris[3 * (size_t)(b + slot)], c = leaf_tris[3 * (size_t)(b + slot) + 1],
+                     d = leaf_tris[3 * (size_t)(b + slot) + 2];
+        ref[0] = it.bref;
+        box[0][0] = fminf(a.x, fminf(c.x, d.x));
+        box[0][1] = fminf(a.y, fminf(c.y, d.y));
+        box[0][2] = fminf(a.z, fminf(c.z, d.z));
+        box[0][3] = fmaxf(a.x, fmaxf(c.x, d.x));
+        box[0][4] = fmaxf(a.y, fmaxf(c.y, d.y));
+        box[0][5] = fmaxf(a.z, fmaxf(c.z, d.z));
+        cnt = 1;
+      } else {
+        const Bvh2Node nd = mb[it.bref];
+        for (int c = 0; c < 2; ++c) {
+          ref[c] = nd.ref[c];
+          for (int k = 0; k < 6; ++k) box[c][k] = nd.box[6 * c + k];
+        }
+        cnt = 2;
+        while (cnt < 8) {
+          int best = -1;
+          float ba = -1.0f;
+          for (int c = 0; c < cnt; ++c)
+            if (ref[c] >= 0) {
+              const float a = box_area(box[c]);
+              if (a > ba) {
+                ba = a;
+                best = c;
+              }
             }
-          }
-        if (best < 0) break;
-        const Bvh2Node ch = mb[ref[best]];
-        ref[best] = ch.ref[0];
-        for (int k = 0; k < 6; ++k) box[best][k] = ch.box[k];
-        ref[cnt] = ch.ref[1];
-        for (int k = 0; k < 6; ++k) box[cnt][k] = ch.box[6 + k];
-        ++cnt;
+          if (best < 0) break;
+          const Bvh2Node ch = mb[ref[best]];
+          ref[best] = ch.ref[0];
+          for (int k = 0; k < 6; ++k) box[best][k] = ch.box[k];
+          ref[cnt] = ch.ref[1];
+          for (int k = 0; k < 6; ++k) box[cnt][k] = ch.box[6 + k];
+          ++cnt;
+        }
       }
     }
-    int n_inner = 0, n_leaf = 0;
+    uint32_t n_inner = 0, n_leaf = 0;
     for (int c = 0; c < cnt; ++c) (ref[c] >= 0 ? n_inner : n_leaf)++;
-    const uint32_t child_base = n_inner ? atomicAdd(&counters[Q_WIDE], (uint32_t)n_inner) : 0u;
-    const uint32_t leaf_base = n_leaf ? atomicAdd(&counters[Q_LEAF], (uint32_t)n_leaf) : 0u;
+    // warp-aggregated allocation of child queue slots and leaf slots
+    const uint32_t inc_i = warp_incl_scan(n_inner, lane), inc_l = warp_incl_scan(n_leaf, lane);
+    const uint32_t tot_i = __shfl_sync(FULL_MASK, inc_i, 31), tot_l = __shfl_sync(FULL_MASK, inc_l, 31);
+    uint32_t base_i = 0, base_l = 0;
+    if (lane == 0) {
+      if (tot_i) base_i = atomicAdd(&counters[C_TAIL], tot_i);
+      if (tot_l) base_l = atomicAdd(&counters[C_LEAF], tot_l);
+    }
+    base_i = __shfl_sync(FULL_MASK, base_i, 0);
+    base_l = __shfl_sync(FULL_MASK, base_l, 0);
+    if (!valid) continue;
+    const uint32_t child_base = base_i + inc_i - n_inner, leaf_base = base_l + inc_l - n_leaf;
     WideNode w;
-    float lo[3] = {box[0][0], box[0][1], box[0][2]}, hi[3] = {box[0][3], box[0][4], box[0][5]};
+    float lo3[3] = {box[0][0], box[0][1], box[0][2]}, hi3[3] = {box[0][3], box[0][4], box[0][5]};
     for (int c = 1; c < cnt; ++c)
       for (int k = 0; k < 3; ++k) {
-        lo[k] = fminf(lo[k], box[c][k]);
-        hi[k] = fmaxf(hi[k], box[c][3 + k]);
+        lo3[k] = fminf(lo3[k], box[c][k]);
+        hi3[k] = fmaxf(hi3[k], box[c][3 + k]);
       }
-    w.px = lo[0];
-    w.py = lo[1];
-    w.pz = lo[2];
+    w.px = lo3[0];
+    w.py = lo3[1];
+    w.pz = lo3[2];
     int e[3];
-    double s[3];
+    double sc[3];
     for (int k = 0; k < 3; ++k) {
-      e[k] = frame_exponent((double)hi[k] - (double)lo[k]);
-      s[k] = ldexp(1.0, e[k]);
+      e[k] = frame_exponent((double)hi3[k] - (double)lo3[k]);
+      sc[k] = ldexp(1.0, e[k]);
     }
     w.ex = (int8_t)e[0];
     w.ey = (int8_t)e[1];
@@ -196,14 +202,15 @@ __global__ void __launch_bounds__(128) k_wide_collapse(const Bvh2Node *bvh2, con
         continue;
       }
       for (int k = 0; k < 3; ++k) {
-        double ql = floor(((double)box[c][k] - (double)lo[k]) / s[k]);
-        double qh = ceil(((double)box[c][3 + k] - (double)lo[k]) / s[k]);
+        double ql = floor(((double)box[c][k] - (double)lo3[k]) / sc[k]);
+        double qh = ceil(((double)box[c][3 + k] - (double)lo3[k]) / sc[k]);
         w.qlo[k][c] = (uint8_t)(ql < 0.0 ? 0.0 : (ql > 255.0 ? 255.0 : ql));
         w.qhi[k][c] = (uint8_t)(qh < 0.0 ? 0.0 : (qh > 255.0 ? 255.0 : qh));
       }
       if (ref[c] >= 0) {
         w.imask |= (uint8_t)(1u << c);
         w.meta[c] = (uint8_t)ri;
+        queue[child_base + ri] = WorkItem{m, ref[c]};  // the next level's item; its wide node index
         ++ri;
       } else {
         const uint32_t slot = (uint32_t)~ref[c];
@@ -216,20 +223,22 @@ __global__ void __launch_bounds__(128) k_wide_collapse(const Bvh2Node *bvh2, con
       }
     }
     const uint4 *wp = reinterpret_cast<const uint4 *>(&w);
-    uint4 *op = reinterpret_cast<uint4 *>(wnodes + it.wide);
+    uint4 *op = reinterpret_cast<uint4 *>(wnodes + idx);
     for (int k = 0; k < 5; ++k) op[k] = wp[k];
-    // publish inner children as new work items, in rank order
-    ri = 0;
-    for (int c = 0; c < cnt; ++c)
-      if (ref[c] >= 0) {
-        const uint32_t q = atomicAdd(&counters[Q_TAIL], 1u);
-        queue[q] = WorkItem{m, ref[c], child_base + (uint32_t)ri, 0};
-        __threadfence();
-        st_relaxed_u32(&ready[q], 1u);
-        ++ri;
-      }
+  }
+  // the last CTA to finish moves the level window to the appended items
+  __shared__ bool s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
     __threadfence();
-    atomicAdd(&counters[Q_DONE], 1u);
+    s_last = atomicAdd(&counters[C_TICKET], 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x == 0) {
+    __threadfence();
+    counters[C_LO] = hi;
+    counters[C_HI] = ld_relaxed_u32(&counters[C_TAIL]);
+    counters[C_TICKET] = 0;
   }
 }
 
@@ -442,12 +451,11 @@ __global__ void __launch_bounds__(kWideThreads, 8)
 
 using namespace gprtcu;
 
-uint32_t gprtcu_spin_budget(void);
 
 namespace {
 
 struct WideScratch {
-  size_t counters, queue, ready, total;
+  size_t counters, queue, total;
 };
 
 WideScratch wide_layout(uint32_t meshes, uint32_t n) {
@@ -455,8 +463,6 @@ WideScratch wide_layout(uint32_t meshes, uint32_t n) {
   size_t off = sizeof(ScratchHeader);
   L.counters = off;
   off += 256;
-  L.ready = off;
-  off += gprtcu_align256((size_t)n * 4);
   L.queue = off;
   off += gprtcu_align256((size_t)n * sizeof(WorkItem));
   L.total = off;
@@ -484,20 +490,20 @@ extern "C" GPRTCU_API gprtcuStatus gprtcuWideBuild(const gprtcuLbvh *binary, con
   const WideScratch L = wide_layout(numMeshes, n);
   if (scratchBytes < L.total) return GPRTCU_ERR_SCRATCH_TOO_SMALL;
   char *s = (char *)scratch;
-  GPRTCU_TRY(cudaMemsetAsync(s, 0, L.queue, stream));  // header, counters, ready flags
+  GPRTCU_TRY(cudaMemsetAsync(s, 0, L.queue, stream));  // header, counters
   uint32_t *counters = (uint32_t *)(s + L.counters);
-  uint32_t *ready = (uint32_t *)(s + L.ready);
   WorkItem *queue = (WorkItem *)(s + L.queue);
   const uint32_t *toff = numMeshes > 1 ? triOffsets : nullptr;
-  k_wide_init<<<(numMeshes + 255) / 256, 256, 0, stream>>>(toff, numMeshes, n, queue, ready, out->roots, counters);
+  k_wide_init<<<(numMeshes + 255) / 256, 256, 0, stream>>>(toff, numMeshes, n, queue, out->roots, counters);
   GPRTCU_TRY(cudaGetLastError());
-  k_wide_collapse<<<gprtcu_num_sms() * 8, 128, 0, stream>>>((const Bvh2Node *)binary->bvh2,
-                                                            (const float4 *)binary->leafTris, toff, n,
-                                                            (WideNode *)out->nodes, (float4 *)out->leafTris, queue,
-                                                            ready, counters, gprtcu_spin_budget(),
-                                                            (ScratchHeader *)s);
-  GPRTCU_TRY(cudaGetLastError());
-  if (out->numNodes) GPRTCU_TRY(cudaMemcpyAsync(out->numNodes, counters + Q_WIDE, 4, cudaMemcpyDeviceToDevice, stream));
+  // One launch per level; a launch whose level is empty returns at once.
+  const int grid = gprtcu_num_sms() * 8;
+  for (int level = 0; level < kWideMaxLevels; ++level) {
+    k_wide_level<<<grid, 128, 0, stream>>>((const Bvh2Node *)binary->bvh2, (const float4 *)binary->leafTris, toff,
+                                           (WideNode *)out->nodes, (float4 *)out->leafTris, queue, counters);
+    GPRTCU_TRY(cudaGetLastError());
+  }
+  if (out->numNodes) GPRTCU_TRY(cudaMemcpyAsync(out->numNodes, counters + C_TAIL, 4, cudaMemcpyDeviceToDevice, stream));
   return GPRTCU_OK;
 }
 
