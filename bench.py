@@ -59,9 +59,10 @@ SORT_N = 268_435_456
 SCAN_N = 1_073_741_824
 WORKLOAD = ("large combined, batched + quantised: {tris:,} fp32 triangles in {meshes:,} meshes, {rays:,} "
             "closest-hit rays; batched LBVH build + 8-wide uint8-quantised collapse + wide trace in one CUDA graph")
-# DRAM bytes of one k_trace_wide launch on this workload, from the ncu capture
-# summarised in profiles/k_trace_wide_large.md (None until captured).
-TRACE_WIDE_DRAM_BYTES = None
+# DRAM bytes (read + write) of one k_trace_wide launch on the default large
+# workload, from the one-pass ncu capture summarised in
+# profiles/k_trace_wide_large.md; reported only for that workload.
+TRACE_WIDE_DRAM_BYTES = 9_045_743_000 + 1_101_867_000
 
 
 def measured_peaks():
@@ -199,6 +200,23 @@ def sortscan(args, dev, peak, rank):
 
 
 
+def max_over_ranks(x, device, world):
+    """The largest x over all ranks (the slowest rank's time); every rank
+    calls it at the same point."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank, ms_per_step, world):
+    """Millions of units per second for all ranks together, each rank having
+    processed units_per_rank in the slowest rank's ms_per_step."""
+    return world * units_per_rank / (ms_per_step * 1e-3) / 1e6
+
+
 def cpu_sample_run(sample):
     """The CPU oracle (test infrastructure) over a list of (pos, tri, rays)
     meshes: a full build and a closest-hit trace of every mesh.  Returns
@@ -307,11 +325,8 @@ def run_b200(args, world, rank, local):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x):
-        t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def slowest(x):
+        return max_over_ranks(x, dev, world)
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     sc = workloads.LargeScene(meshes=args.meshes, n=args.triangles, seed_offset=rank, device=dev)
@@ -334,8 +349,8 @@ def run_b200(args, world, rank, local):
             e1.record(stream)
         barrier()
     clocks = clk.summary()
-    step_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev)) / args.steps
-    value = world * sc.nrays / (step_ms * 1e-3) / 1e6
+    step_ms = slowest(sum(a.elapsed_time(b) for a, b in ev)) / args.steps
+    value = whole_job_rate(sc.nrays, step_ms, world)
 
     # the step's parts, eager, for the roofline and the build rate
     trace_ms = float(np.mean(workloads.time_steps(sc.trace_quantised, args.steps, 1, flush)))
@@ -345,7 +360,7 @@ def run_b200(args, world, rank, local):
     plain_steps = min(args.steps, args.plain_steps)
     plain_ms = None
     if plain_steps > 0:
-        plain_ms = max_over_ranks(np.mean(workloads.time_steps(sc.plain, plain_steps, 1, flush)))
+        plain_ms = slowest(np.mean(workloads.time_steps(sc.plain, plain_steps, 1, flush)))
     g.replay()
     torch.cuda.synchronize()
     same_bat = bool(torch.equal(sc.h_plain, sc.h_bat)) if plain_ms is not None else None
@@ -373,8 +388,8 @@ def run_b200(args, world, rank, local):
         g.replay()
         hits_p.copy_(sc.h_q, non_blocking=True)
 
-    e2e_ms = max_over_ranks(np.sum(workloads.time_steps(e2e_step, args.steps, max(1, args.warmup), flush))) / args.steps
-    e2e_v = world * sc.nrays / (e2e_ms * 1e-3) / 1e6
+    e2e_ms = slowest(np.sum(workloads.time_steps(e2e_step, args.steps, max(1, args.warmup), flush))) / args.steps
+    e2e_v = whole_job_rate(sc.nrays, e2e_ms, world)
     e2e_ok = bool(torch.equal(hits_p, sc.h_q.cpu()))
     nrays, ntri, meshes = sc.nrays, sc.n, sc.meshes
     del host, hits_p, g
@@ -417,7 +432,9 @@ def run_b200(args, world, rank, local):
             "roofline": {"kernel": "k_trace_wide (closest hit, batched)", "bound": "hbm", "achieved": achieved,
                          "peak": peak, "peak_kind": peak_kind + " hbm_gbs (copy)", "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": TRACE_WIDE_DRAM_BYTES,
+                         "traffic": TRACE_WIDE_DRAM_BYTES if (ntri, meshes) == (67_108_864, 16_384) else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one full-size "
+                                           "launch (profiles/k_trace_wide_large.md)",
                          "algorithmic_bytes": "40 B/ray (32 B ray in + 8 B hit out) x %d rays per launch" % nrays,
                          "launch_ms": trace_ms},
             "build": {"value": ntri / (build_ms * 1e-3) / 1e6, "unit": "Mprims/s", "ms": build_ms,
