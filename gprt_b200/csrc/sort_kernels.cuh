@@ -24,6 +24,7 @@
 // keys for the histograms.
 #pragma once
 #include <array>
+#include <type_traits>
 #include <utility>
 
 #include "common.cuh"
@@ -108,6 +109,18 @@ template <int BITS> __device__ __forceinline__ unsigned warp_peers(uint32_t d, b
     m &= bit ? bb : ~bb;
   }
   return valid ? m : 0u;
+}
+
+// The same for a full warp of valid keys.
+template <int BITS> __device__ __forceinline__ unsigned warp_peers(uint32_t d) {
+  unsigned m = FULL_MASK;
+#pragma unroll
+  for (int b = 0; b < BITS; ++b) {
+    const bool bit = (d >> b) & 1u;
+    const unsigned bb = __ballot_sync(FULL_MASK, bit);
+    m &= bit ? bb : ~bb;
+  }
+  return m;
 }
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -235,8 +248,7 @@ __global__ void __launch_bounds__(WARPS * 32, (PassCfg<K, V, RB, WARPS, ITEMS>::
   V *s_vals = reinterpret_cast<V *>(smem + C::KEY_BYTES);
   uint32_t *s_hist = reinterpret_cast<uint32_t *>(smem + C::KEY_BYTES + C::VAL_BYTES);  // [WARPS][RADIX]
   uint32_t *s_goff = s_hist + WARPS * RADIX;
-  uint32_t *s_tstart = s_goff + RADIX;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(s_tstart + RADIX);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(s_goff + 2 * RADIX);
   __shared__ uint32_t s_tile, s_abort;
   __shared__ uint32_t s_tmp[32];
 
@@ -277,8 +289,11 @@ __global__ void __launch_bounds__(WARPS * 32, (PassCfg<K, V, RB, WARPS, ITEMS>::
   for (int i = tid; i < WARPS * RADIX; i += THREADS) s_hist[i] = 0;
   for (int i = tid; i < RADIX; i += THREADS) status_next[(uint64_t)tile * RADIX + i] = 0;
   if (!bulk) {
-    for (int i = tid; i < TILE; i += THREADS)
-      if ((uint32_t)i < tile_n) s_keys[i] = src_k[tile_start + i];
+    // The last tile is padded with all-ones keys: they rank after every real
+    // key (stable order puts them last within the top digit), so the real
+    // keys fill tile-sorted slots [0, tile_n) and no loop needs a bounds test
+    // before the scatter; the top digit's count leaves the padding out.
+    for (int i = tid; i < TILE; i += THREADS) s_keys[i] = (uint32_t)i < tile_n ? src_k[tile_start + i] : ~(K)0;
   } else if (!mbar_wait(&bars[0], 0, MBAR_WAIT_BUDGET)) {
     s_abort = 1;
   }
@@ -297,31 +312,24 @@ __global__ void __launch_bounds__(WARPS * 32, (PassCfg<K, V, RB, WARPS, ITEMS>::
   const uint32_t lt = lanemask_lt();
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
-    const uint32_t pos = warp * WK + i * 32 + lane;
-    const bool valid = pos < tile_n;
-    k[i] = valid ? s_keys[pos] : (K)0;
-    const uint32_t d = valid ? digit_of(k[i], shift, mask) : 0u;
-    const unsigned peers = warp_peers<RB>(d, valid);
-    uint32_t base = 0;
-    if (valid) base = wh[d];
+    k[i] = s_keys[warp * WK + i * 32 + lane];
+    const uint32_t d = digit_of(k[i], shift, mask);
+    const unsigned peers = warp_peers<RB>(d);
+    const uint32_t base = wh[d];
     __syncwarp();
-    if (valid && lane == 31 - __clz(peers)) wh[d] = base + __popc(peers);
+    if (lane == 31 - __clz(peers)) wh[d] = base + __popc(peers);
     __syncwarp();
     rank[i] = base + __popc(peers & lt);
   }
   __syncthreads();
 
-  // ---- per digit: warp-exclusive offsets, tile count, publish, look-back.
+  // ---- per digit: tile count, publish, tile-exclusive start, look-back;
+  // then each warp's first slot of the digit in the tile-sorted order.
   uint32_t tcount = 0;
   if (tid < RADIX) {
-    uint32_t run = 0;
 #pragma unroll 4
-    for (int w = 0; w < WARPS; ++w) {
-      uint32_t c = s_hist[w * RADIX + tid];
-      s_hist[w * RADIX + tid] = run;
-      run += c;
-    }
-    tcount = run;
+    for (int w = 0; w < WARPS; ++w) tcount += s_hist[w * RADIX + tid];
+    if ((uint32_t)tid == mask) tcount -= TILE - tile_n;  // padding of the last tile
     st_relaxed_u32(status + (uint64_t)tile * RADIX + tid, (tile == 0 ? LB_INC : LB_AGG) | tcount);
   }
   const uint32_t tstart = block_excl_scan_digits<RADIX>(tcount, s_tmp);
@@ -336,14 +344,14 @@ __global__ void __launch_bounds__(WARPS * 32, (PassCfg<K, V, RB, WARPS, ITEMS>::
       uint32_t spins = 0;
       bool done = false;
       while (!done && ok) {
-        uint32_t s[8];
+        uint32_t sw[8];
 #pragma unroll
         for (int c = 0; c < 8; ++c)
-          s[c] = j - c >= 0 ? ld_relaxed_u32(status + (uint64_t)(j - c) * RADIX + tid) : LB_INC;
+          sw[c] = j - c >= 0 ? ld_relaxed_u32(status + (uint64_t)(j - c) * RADIX + tid) : LB_INC;
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
           if (done || !ok) break;
-          uint32_t x = s[c];
+          uint32_t x = sw[c];
           while ((x & ~LB_VALUE) == 0) {
             if (++spins > a.budget) {
               ok = false;
@@ -365,10 +373,16 @@ __global__ void __launch_bounds__(WARPS * 32, (PassCfg<K, V, RB, WARPS, ITEMS>::
       st_relaxed_u32(status + (uint64_t)tile * RADIX + tid, ok ? (LB_INC | (excl + tcount)) : LB_POISON);
       if (!ok) s_abort = 1;
     }
-    s_tstart[tid] = tstart;
     // global position of tile-sorted slot p of this digit = s_goff[d] + p
     // (mod 2^32; the true value is below 2^30)
     s_goff[tid] = a.hist[pass * RADIX + tid] + excl - tstart;
+    uint32_t run = tstart;
+#pragma unroll 4
+    for (int w = 0; w < WARPS; ++w) {
+      const uint32_t c = s_hist[w * RADIX + tid];
+      s_hist[w * RADIX + tid] = run;
+      run += c;
+    }
   }
   __syncthreads();
   if (s_abort) {
@@ -380,12 +394,8 @@ __global__ void __launch_bounds__(WARPS * 32, (PassCfg<K, V, RB, WARPS, ITEMS>::
   uint32_t q[ITEMS];
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
-    const uint32_t pos = warp * WK + i * 32 + lane;
-    if (pos < tile_n) {
-      const uint32_t d = digit_of(k[i], shift, mask);
-      q[i] = s_tstart[d] + s_hist[warp * RADIX + d] + rank[i];
-      s_keys[q[i]] = k[i];
-    }
+    q[i] = s_hist[warp * RADIX + digit_of(k[i], shift, mask)] + rank[i];
+    s_keys[q[i]] = k[i];
   }
   __syncthreads();
 #pragma unroll
@@ -410,16 +420,10 @@ __global__ void __launch_bounds__(WARPS * 32, (PassCfg<K, V, RB, WARPS, ITEMS>::
       return;
     }
 #pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-      const uint32_t pos = warp * WK + i * 32 + lane;
-      if (pos < tile_n) v[i] = s_vals[pos];
-    }
+    for (int i = 0; i < ITEMS; ++i) v[i] = s_vals[warp * WK + i * 32 + lane];  // padding slots: unused
     __syncthreads();
 #pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-      const uint32_t pos = warp * WK + i * 32 + lane;
-      if (pos < tile_n) s_vals[q[i]] = v[i];
-    }
+    for (int i = 0; i < ITEMS; ++i) s_vals[q[i]] = v[i];
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
