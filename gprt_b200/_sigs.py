@@ -34,6 +34,8 @@ SIGNATURES = {
     "gprtcuLbvhScratchSize": ([u32], sz),
     "gprtcuLbvhBuildTriangles": ([vp, vp, u32, i32, vp, vp, sz, vp], st),
     "gprtcuLbvhBuildPoints": ([vp, u32, i32, vp, vp, sz, vp], st),
+    "gprtcuLbvhBuildEdges": ([vp, vp, u32, i32, vp, vp, sz, vp], st),
+    "gprtcuLbvhRefitTriangles": ([vp, vp, vp, u32, vp, vp, sz, vp], st),
     "gprtcuTraceScratchSize": ([], sz),
     "gprtcuTraceClosest": ([vp, vp, u64, vp, vp, sz, vp], st),
     "gprtcuTraceAny": ([vp, vp, u64, vp, vp, sz, vp], st),

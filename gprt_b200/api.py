@@ -251,6 +251,28 @@ def lbvh_build_points(pos, bvh=None, code_kind=0):
     return bvh
 
 
+def lbvh_build_edges(pos, edges, bvh=None, code_kind=0):
+    """Edge LBVH over float32 positions [V,3] and uint32/int32 endpoints [N,2]."""
+    _need_cuda(pos, edges)
+    n = edges.shape[0]
+    if bvh is None:
+        bvh = Lbvh(n, pos.device, with_traversal=False)
+    st = lib().gprtcuLbvhBuildEdges(_ptr(pos), _ptr(edges), n, code_kind, ctypes.byref(bvh.desc), _ptr(bvh.scratch),
+                                    bvh.scratch.numel(), _stream())
+    _check(st, "gprtcuLbvhBuildEdges")
+    return bvh
+
+
+def lbvh_refit_triangles(pos, tri, bvh, tri_off=None):
+    """Refit an existing triangle LBVH (Lbvh, or BatchLbvh with its offsets) to moved vertices."""
+    _need_cuda(pos, tri)
+    meshes = 1 if tri_off is None else tri_off.numel() - 1
+    st = lib().gprtcuLbvhRefitTriangles(_ptr(pos), _ptr(tri), _ptr(tri_off), meshes, ctypes.byref(bvh.desc),
+                                        _ptr(bvh.scratch), bvh.scratch.numel(), _stream())
+    _check(st, "gprtcuLbvhRefitTriangles")
+    return bvh
+
+
 def trace(bvh, rays, hits=None, anyhit=False, scr=None):
     """rays: float32 [R, 8] {org.xyz, tmin, dir.xyz, tmax}; returns hits int32 [R, 2] {prim, t bits}."""
     _need_cuda(rays)

@@ -133,11 +133,31 @@ struct MeshMap {
   }
 };
 
+// Edge endpoints (getEdgeBounds / getEdgeCentroid, gprt/development/
+// gprt_lbvh.hlsl:112-119,131-136): v[0..2] = p1, v[3..5] = v[6..8] = p2.
+__device__ __forceinline__ void load_edge(const float *pos, const uint32_t *edge, uint32_t id, float v[9]) {
+  const uint32_t i0 = edge[2 * (size_t)id], i1 = edge[2 * (size_t)id + 1];
+  const float *p0 = pos + 3 * (size_t)i0, *p1 = pos + 3 * (size_t)i1;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    v[k] = p0[k];
+    v[3 + k] = v[6 + k] = p1[k];
+  }
+}
+
+// KIND: 0 triangles (tri = uint3 indices), 1 points, 2 edges (tri = uint2 indices).
 template <int KIND>
 __device__ __forceinline__ void prim_box(const float *pos, const uint32_t *tri, uint64_t id, float v[9], float b[6]) {
   if (KIND == 0) {
     load_tri(pos, tri, (uint32_t)id, v);
     tri_box(v, b);
+  } else if (KIND == 2) {
+    load_edge(pos, tri, (uint32_t)id, v);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      b[k] = fminf(v[k], v[3 + k]);
+      b[3 + k] = fmaxf(v[k], v[3 + k]);
+    }
   } else {
 #pragma unroll
     for (int k = 0; k < 3; ++k) v[k] = v[3 + k] = v[6 + k] = b[k] = b[3 + k] = pos[3 * (size_t)id + k];
@@ -202,7 +222,8 @@ __global__ void __launch_bounds__(256) k_bounds(const float *pos, const uint32_t
 }
 
 // Codes of centroids (p1 + p2 + p3) / 3 (gprt/development/gprt_lbvh.hlsl:
-// 139-146, 262-277), or of the points themselves, normalised to the mesh's
+// 139-146, 262-277), (p1 + p2) / 2 for edges (:131-136, 245-260), or of the
+// points themselves, normalised to the mesh's
 // box.  One mesh: codes[i] and ids[i] = i.  Many meshes: 64-bit sort keys
 // (mesh << 32 | code) and mesh-local ids.
 template <int KIND, bool BATCHED>
@@ -230,6 +251,11 @@ __global__ void __launch_bounds__(256) k_codes(const float *pos, const uint32_t 
       load_tri(pos, tri, (uint32_t)i, v);
 #pragma unroll
       for (int k = 0; k < 3; ++k) c[k] = __fdiv_rn(__fadd_rn(__fadd_rn(v[k], v[3 + k]), v[6 + k]), 3.0f);
+    } else if (KIND == 2) {
+      float v[9];
+      load_edge(pos, tri, (uint32_t)i, v);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) c[k] = __fdiv_rn(__fadd_rn(v[k], v[3 + k]), 2.0f);
     } else {
 #pragma unroll
       for (int k = 0; k < 3; ++k) c[k] = pos[3 * (size_t)i + k];
@@ -328,9 +354,13 @@ __global__ void __launch_bounds__(256) k_refit(const float *pos, const uint32_t 
   if (s >= mm.n) return;
   uint32_t m = 0;
   if (BATCHED) {
-    const uint64_t key = keys[s];  // (mesh << 32 | code), sorted
-    m = (uint32_t)(key >> 32);
-    if (codes_out) codes_out[s] = (uint32_t)key;
+    if (keys) {
+      const uint64_t key = keys[s];  // (mesh << 32 | code), sorted
+      m = (uint32_t)(key >> 32);
+      if (codes_out) codes_out[s] = (uint32_t)key;
+    } else {
+      m = mm.mesh_of_prim(s);  // refit of an existing batch: no keys
+    }
   }
   const uint64_t b = BATCHED ? mm.begin(m) : 0;
   const int64_t N = BATCHED ? mm.count(m) : mm.n;
@@ -450,21 +480,23 @@ void launch_build(const float *pos, const uint32_t *tri, MeshMap mm, int codeKin
     if (mm.n > mm.meshes)
       k_karras<BATCHED><<<(unsigned)((mm.n - mm.meshes + 255) / 256), 256, 0, stream>>>(out->codes, keys, mm, nodes,
                                                                                          (Bvh2Node *)out->bvh2);
+    // the traversal layout (bvh2, leafTris) exists for triangles only
     k_refit<KIND, BATCHED><<<(unsigned)((mm.n + 255) / 256), 256, 0, stream>>>(
-        pos, tri, out->ids, keys, mm, nodes, out->aabbs, (Bvh2Node *)out->bvh2, (float4 *)out->leafTris, out->codes,
-        arrivals, out->rootBox);
+        pos, tri, out->ids, keys, mm, nodes, out->aabbs, KIND == 0 ? (Bvh2Node *)out->bvh2 : nullptr,
+        KIND == 0 ? (float4 *)out->leafTris : nullptr, out->codes, arrivals, out->rootBox);
   }
 }
 
 gprtcuStatus lbvh_build(int kind, const float *pos, const uint32_t *tri, const uint32_t *prim_off, uint32_t meshes,
                         uint32_t n, int codeKind, gprtcuLbvh *out, void *scratch, size_t scratchBytes,
                         cudaStream_t stream) {
-  if (!out || !pos || (kind == 0 && !tri)) return GPRTCU_ERR_INVALID_ARG;
+  if (!out || !pos || (kind != 1 && !tri)) return GPRTCU_ERR_INVALID_ARG;
+  if (kind == 2 && meshes > 1) return GPRTCU_ERR_INVALID_ARG;
   if (n == 0 || meshes == 0 || meshes > n) return GPRTCU_ERR_INVALID_ARG;
   if (meshes > 1 && !prim_off) return GPRTCU_ERR_INVALID_ARG;
   if (n > (1u << 30) - 1) return GPRTCU_ERR_TOO_LARGE;
   if (!out->codes || !out->ids || !out->nodes) return GPRTCU_ERR_INVALID_ARG;
-  if (n > meshes && !out->aabbs && !out->bvh2) return GPRTCU_ERR_INVALID_ARG;  // the refit needs one box store
+  if (n > meshes && !out->aabbs && (kind != 0 || !out->bvh2)) return GPRTCU_ERR_INVALID_ARG;  // one box store
   if (out->bvh2 && ((uintptr_t)out->bvh2 & 15)) return GPRTCU_ERR_INVALID_ARG;
   if (out->leafTris && ((uintptr_t)out->leafTris & 15)) return GPRTCU_ERR_INVALID_ARG;
   if (codeKind != 0 && codeKind != 1) return GPRTCU_ERR_INVALID_ARG;
@@ -489,6 +521,7 @@ gprtcuStatus lbvh_build(int kind, const float *pos, const uint32_t *tri, const u
     }
     if (kind == 0 && batched) launch_build<0, true>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
     else if (kind == 0) launch_build<0, false>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
+    else if (kind == 2) launch_build<2, false>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
     else if (batched) launch_build<1, true>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
     else launch_build<1, false>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
     GPRTCU_TRY(cudaGetLastError());
@@ -512,6 +545,46 @@ extern "C" GPRTCU_API gprtcuStatus gprtcuLbvhBuildPoints(const float *positions,
                                                          gprtcuStream stream) {
   return lbvh_build(1, positions, nullptr, nullptr, 1, numPoints, codeKind, bvh, scratch, scratchBytes,
                     (cudaStream_t)stream);
+}
+
+extern "C" GPRTCU_API gprtcuStatus gprtcuLbvhBuildEdges(const float *positions, const uint32_t *edges,
+                                                        uint32_t numEdges, int codeKind, gprtcuLbvh *bvh, void *scratch,
+                                                        size_t scratchBytes, gprtcuStream stream) {
+  return lbvh_build(2, positions, edges, nullptr, 1, numEdges, codeKind, bvh, scratch, scratchBytes,
+                    (cudaStream_t)stream);
+}
+
+// Refit of an existing triangle LBVH (one mesh, or a batch when triOffsets is
+// given) after its vertices moved: the topology and the leaf order are kept,
+// the leaf-order triangles, the traversal nodes' boxes and the reference-
+// layout boxes are recomputed bottom-up.
+extern "C" GPRTCU_API gprtcuStatus gprtcuLbvhRefitTriangles(const float *positions, const uint32_t *triangles,
+                                                            const uint32_t *triOffsets, uint32_t numMeshes,
+                                                            gprtcuLbvh *bvh, void *scratch, size_t scratchBytes,
+                                                            gprtcuStream stream_) {
+  cudaStream_t stream = (cudaStream_t)stream_;
+  if (!bvh || !positions || !triangles || numMeshes == 0 || (numMeshes > 1 && !triOffsets)) return GPRTCU_ERR_INVALID_ARG;
+  const uint32_t n = bvh->numPrims;
+  if (n == 0 || numMeshes > n || !bvh->ids || !bvh->nodes) return GPRTCU_ERR_INVALID_ARG;
+  if (n > numMeshes && !bvh->aabbs && !bvh->bvh2) return GPRTCU_ERR_INVALID_ARG;
+  if (!scratch || ((uintptr_t)scratch & 255)) return GPRTCU_ERR_INVALID_ARG;
+  const LbvhScratch L = lbvh_scratch_layout(n, numMeshes);
+  if (scratchBytes < L.keys) return GPRTCU_ERR_SCRATCH_TOO_SMALL;
+  char *s = (char *)scratch;
+  GPRTCU_TRY(cudaMemsetAsync(s, 0, L.keys, stream));  // header and arrival counters
+  uint32_t *arrivals = (uint32_t *)(s + L.arrivals);
+  const MeshMap mm{numMeshes > 1 ? triOffsets : nullptr, numMeshes, n};
+  const unsigned grid = (unsigned)((n + 255) / 256);
+  if (numMeshes > 1)
+    k_refit<0, true><<<grid, 256, 0, stream>>>(positions, triangles, bvh->ids, nullptr, mm, (int4 *)bvh->nodes,
+                                               bvh->aabbs, (Bvh2Node *)bvh->bvh2, (float4 *)bvh->leafTris, nullptr,
+                                               arrivals, bvh->rootBox);
+  else
+    k_refit<0, false><<<grid, 256, 0, stream>>>(positions, triangles, bvh->ids, nullptr, mm, (int4 *)bvh->nodes,
+                                                bvh->aabbs, (Bvh2Node *)bvh->bvh2, (float4 *)bvh->leafTris, nullptr,
+                                                arrivals, bvh->rootBox);
+  GPRTCU_TRY(cudaGetLastError());
+  return GPRTCU_OK;
 }
 
 extern "C" GPRTCU_API size_t gprtcuBatchScratchSize(uint32_t numMeshes, uint32_t totalTriangles) {

@@ -195,6 +195,25 @@ GPRTCU_API gprtcuStatus gprtcuLbvhBuildTriangles(const float *positions, const u
 GPRTCU_API gprtcuStatus gprtcuLbvhBuildPoints(const float *positions, uint32_t numPoints, int codeKind,
                                               gprtcuLbvh *bvh, void *scratch, size_t scratchBytes,
                                               gprtcuStream stream);
+/* Edge (segment) LBVH: edges uint32[n][2] index positions float[][3].  The
+ * reference's build supports edges (GPRT_LBVH_EDGES; ComputeEdgeBounds,
+ * ComputeEdgeMortonCodes, BuildEdgeHierarchy, gprt/development/
+ * gprt_lbvh.hlsl:112-136,202-260,370-398; dispatched by gprtLBVHBuild,
+ * gprt/development/gprt_lbvh.h:184-186) though its header has no create call
+ * for them.  Centroid (p1 + p2) / 2.  Fills codes, ids, nodes, aabbs and
+ * sceneBounds (the traversal layout is for triangles only). */
+GPRTCU_API gprtcuStatus gprtcuLbvhBuildEdges(const float *positions, const uint32_t *edges, uint32_t numEdges,
+                                             int codeKind, gprtcuLbvh *bvh, void *scratch, size_t scratchBytes,
+                                             gprtcuStream stream);
+/* Refit-only update of a triangle LBVH after its vertices moved (the
+ * semantics of gprtAccelUpdate, gprt/gprt_host.h:1508-1529): topology and leaf
+ * order are kept; leaf-order triangles, traversal-node boxes, reference-layout
+ * boxes and rootBox are recomputed bottom-up.  triOffsets/numMeshes as for
+ * gprtcuBatchBuildTriangles (NULL/1 for one mesh).  Scratch: the size of the
+ * build's (gprtcuLbvhScratchSize / gprtcuBatchScratchSize). */
+GPRTCU_API gprtcuStatus gprtcuLbvhRefitTriangles(const float *positions, const uint32_t *triangles,
+                                                 const uint32_t *triOffsets, uint32_t numMeshes, gprtcuLbvh *bvh,
+                                                 void *scratch, size_t scratchBytes, gprtcuStream stream);
 
 /* ------------------------------------------------------------------------
  * Trace.  Software replacement for the closest-hit / any-hit semantics of

@@ -58,6 +58,7 @@ def lib():
         L.orc_refit_tri.argtypes = [vp, vp, vp, u32, vp, vp]
         L.orc_lbvh_build_tri.argtypes = [vp, vp, u32, i32, vp, vp, vp, vp, vp]
         L.orc_lbvh_build_points.argtypes = [vp, u32, i32, vp, vp, vp, vp, vp]
+        L.orc_lbvh_build_edges.argtypes = [vp, vp, u32, i32, vp, vp, vp, vp, vp]
         L.orc_isect_tri32.argtypes = [vp, vp, vp, vp, vp]
         L.orc_isect_tri32.restype = i32
         L.orc_refine_t32.argtypes = [vp, vp, vp, vp]
@@ -149,6 +150,32 @@ def lbvh_build_points(pos, kind=0):
     return dict(scene=scene, codes=codes, ids=ids, nodes=nodes, aabbs=aabbs)
 
 
+def lbvh_build_edges(pos, edges, kind=0):
+    pos = np.ascontiguousarray(pos, dtype=np.float32)
+    edges = np.ascontiguousarray(edges, dtype=np.uint32)
+    n = edges.shape[0]
+    scene = np.zeros(6, np.float32)
+    codes = np.zeros(n, np.uint32)
+    ids = np.zeros(n, np.uint32)
+    nn = max(2 * n - 1, 0)
+    nodes = np.full((nn, 4), -1, np.int32)
+    aabbs = np.zeros((nn, 6), np.float32)
+    lib().orc_lbvh_build_edges(_p(pos), _p(edges), n, kind, _p(scene), _p(codes), _p(ids), _p(nodes), _p(aabbs))
+    return dict(scene=scene, codes=codes, ids=ids, nodes=nodes, aabbs=aabbs)
+
+
+def refit_tri(pos, tri, ids, nodes):
+    """Bottom-up boxes of an existing topology (nodes int32 [2n-1,4] with
+    parents, ids uint32 [n]) over the given vertices; returns (nodes, aabbs)."""
+    pos = np.ascontiguousarray(pos, dtype=np.float32)
+    tri = np.ascontiguousarray(tri, dtype=np.uint32)
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    nodes = np.ascontiguousarray(nodes, dtype=np.int32).copy()
+    aabbs = np.zeros((nodes.shape[0], 6), np.float32)
+    lib().orc_refit_tri(_p(pos), _p(tri), _p(ids), ids.size, _p(nodes), _p(aabbs))
+    return nodes, aabbs
+
+
 def karras(codes):
     codes = np.ascontiguousarray(codes, dtype=np.uint32)
     n = codes.size
@@ -158,12 +185,13 @@ def karras(codes):
 
 
 def ref_lbvh_build(pos, tri=None):
-    """The reference's programs run serially (kind: triangles if tri given, else points)."""
+    """The reference's programs run serially (kind: triangles if tri is [n,3],
+    edges if tri is [n,2], points if tri is None)."""
     pos = np.ascontiguousarray(pos, dtype=np.float32)
     if tri is not None:
         tri = np.ascontiguousarray(tri, dtype=np.uint32)
         n = tri.shape[0]
-        kind = 0
+        kind = 0 if tri.shape[1] == 3 else 2
     else:
         n = pos.shape[0]
         kind = 1

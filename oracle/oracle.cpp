@@ -338,6 +338,30 @@ extern "C" void orc_lbvh_build_points(const float *pos, uint32_t n, int kind, fl
   orc_refit_tri(pos, tri.data(), ids, n, nodes, aabbs);
 }
 
+// Edge variant: ComputeEdgeBounds / ComputeEdgeMortonCodes /
+// BuildEdgeHierarchy (gprt/development/gprt_lbvh.hlsl:112-119,131-136,202-213,
+// 245-260,370-398): a leaf box is the min/max of the two endpoints (the
+// triangle box of the triple (p1, p2, p2) has the same bits), the code that of
+// (p1 + p2) / 2.
+extern "C" void orc_lbvh_build_edges(const float *pos, const uint32_t *edges, uint32_t n, int kind, float scene[6],
+                                     uint32_t *codes, uint32_t *ids, int32_t *nodes, float *aabbs) {
+  std::vector<uint32_t> tri(3 * (size_t)n);
+  for (uint32_t i = 0; i < n; ++i) {
+    tri[3 * i] = edges[2 * i];
+    tri[3 * i + 1] = tri[3 * i + 2] = edges[2 * i + 1];
+  }
+  orc_tri_bounds(pos, tri.data(), n, scene);
+  for (uint32_t i = 0; i < n; ++i) {
+    f3 p1 = ld3(pos, edges[2 * i]), p2 = ld3(pos, edges[2 * i + 1]);
+    f3 c = {(p1.x + p2.x) / 2.0f, (p1.y + p2.y) / 2.0f, (p1.z + p2.z) / 2.0f};
+    codes[i] = code_of(c, scene, kind);
+    ids[i] = i;
+  }
+  orc_sort(codes, 4, ids, 4, n);
+  orc_karras(codes, n, nodes);
+  orc_refit_tri(pos, tri.data(), ids, n, nodes, aabbs);
+}
+
 extern "C" void orc_lbvh_build_tri(const float *pos, const uint32_t *tri, uint32_t n, int kind, float scene[6],
                                    uint32_t *codes, uint32_t *ids, int32_t *nodes, float *aabbs) {
   orc_tri_bounds(pos, tri, n, scene);

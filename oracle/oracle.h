@@ -84,6 +84,8 @@ void orc_karras(const uint32_t *codes, uint32_t n, int32_t *nodes);
 void orc_refit_tri(const float *pos, const uint32_t *tri, const uint32_t *ids, uint32_t n, int32_t *nodes,
                    float *aabbs);
 /* Full build: bounds, codes, stable pair sort, karras, refit. */
+void orc_lbvh_build_edges(const float *pos, const uint32_t *edges, uint32_t n, int kind, float scene[6],
+                          uint32_t *codes, uint32_t *ids, int32_t *nodes, float *aabbs);
 void orc_lbvh_build_tri(const float *pos, const uint32_t *tri, uint32_t n, int kind, float scene[6],
                         uint32_t *codes, uint32_t *ids, int32_t *nodes, float *aabbs);
 

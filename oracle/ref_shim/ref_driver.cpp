@@ -22,6 +22,9 @@ void MakeNodes(LBVHData record, uint3 DispatchThreadID);
 void SplitNodes(LBVHData record, uint3 DispatchThreadID);
 void BuildTriangleHierarchy(LBVHData record, uint3 DispatchThreadID);
 void BuildPointHierarchy(LBVHData record, uint3 DispatchThreadID);
+void ComputeEdgeBounds(LBVHData record, uint3 DispatchThreadID);
+void ComputeEdgeMortonCodes(LBVHData record, uint3 DispatchThreadID);
+void BuildEdgeHierarchy(LBVHData record, uint3 DispatchThreadID);
 
 static gprt::Buffer buf(const void *p, uint64_t bytes) { return gprt::Buffer{(unsigned char *)p, bytes}; }
 
@@ -36,7 +39,8 @@ static void sort_pairs(uint32_t *codes, uint32_t *ids, uint32_t n) {
   }
 }
 
-// kind: 0 = triangles (pos float3[npos], tri uint3[n]), 1 = points (pos float3[n]).
+// kind: 0 = triangles (pos float3[npos], tri uint3[n]), 1 = points (pos float3[n]),
+// 2 = edges (pos float3[npos], tri uint2[n]).
 // Outputs: scene[6], codes[n], ids[n], nodes int4[2n-1], aabbs float3[2(2n-1)].
 extern "C" void ref_lbvh_build(int kind, const float *pos, uint32_t npos, const uint32_t *tri, uint32_t n,
                                float *scene, uint32_t *codes, uint32_t *ids, int32_t *nodes, float *aabbs) {
@@ -47,6 +51,7 @@ extern "C" void ref_lbvh_build(int kind, const float *pos, uint32_t npos, const 
   r.numInner = n - 1;
   r.positions = buf(pos, (uint64_t)npos * 12);
   r.triangles = buf(tri, kind == 0 ? (uint64_t)n * 12 : 0);
+  r.edges = buf(tri, kind == 2 ? (uint64_t)n * 8 : 0);
   r.mortonCodes = buf(codes, (uint64_t)n * 4);
   r.ids = buf(ids, (uint64_t)n * 4);
   r.nodes = buf(nodes, (uint64_t)r.numNodes * 16);
@@ -57,11 +62,13 @@ extern "C" void ref_lbvh_build(int kind, const float *pos, uint32_t npos, const 
   aabbs[3] = aabbs[4] = aabbs[5] = -FLT_MAX;
   for (uint32_t i = 0; i < n; ++i) {
     if (kind == 0) ComputeTriangleBounds(r, uint3(i, 0, 0));
+    else if (kind == 2) ComputeEdgeBounds(r, uint3(i, 0, 0));
     else ComputePointBounds(r, uint3(i, 0, 0));
   }
   for (int k = 0; k < 6; ++k) scene[k] = aabbs[k];
   for (uint32_t i = 0; i < n; ++i) {
     if (kind == 0) ComputeTriangleMortonCodes(r, uint3(i, 0, 0));
+    else if (kind == 2) ComputeEdgeMortonCodes(r, uint3(i, 0, 0));
     else ComputePointMortonCodes(r, uint3(i, 0, 0));
   }
   sort_pairs(codes, ids, n);
@@ -69,6 +76,7 @@ extern "C" void ref_lbvh_build(int kind, const float *pos, uint32_t npos, const 
   for (uint32_t i = 0; i < r.numInner; ++i) SplitNodes(r, uint3(i, 0, 0));
   for (uint32_t i = 0; i < n; ++i) {
     if (kind == 0) BuildTriangleHierarchy(r, uint3(i, 0, 0));
+    else if (kind == 2) BuildEdgeHierarchy(r, uint3(i, 0, 0));
     else BuildPointHierarchy(r, uint3(i, 0, 0));
   }
 }

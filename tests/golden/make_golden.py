@@ -7,8 +7,9 @@
                     reference sources (oracle/Makefile target `ref`) and run
                     serially in gprtLBVHBuild's order: scene box, Morton codes,
                     sorted (code, id) pairs, int4 nodes, float3 box pairs, for
-                    seeded triangle soups and for a t04-style point set with
-                    coordinates in [-1e38, 1e38] (tests/t04-swBVH/hostCode.cpp:47-56).
+                    seeded triangle soups, seeded edge sets and a t04-style
+                    point set with coordinates in [-1e38, 1e38]
+                    (tests/t04-swBVH/hostCode.cpp:47-56).
 * hilbert_ref.npz -- gprt/hilbert.h hilbert_c2i(3, 10, .) on seeded and corner
                     coordinates.
 * sortscan.npz   -- the reference tests' own host oracles restated with numpy:
@@ -62,6 +63,17 @@ def main():
     out["pts42_pos"] = pts
     for k, v in r.items():
         out["pts42_" + k] = v
+    # edges (ComputeEdgeBounds / ComputeEdgeMortonCodes / BuildEdgeHierarchy),
+    # from their own generator so the cases above keep their bits
+    erng = np.random.default_rng(777)
+    for n in (1, 2, 3, 64, 1000):
+        pos = erng.random((n + 5, 3), dtype=np.float32)
+        edges = erng.integers(0, n + 5, size=(n, 2)).astype(np.uint32)
+        r = oracle.ref_lbvh_build(pos, edges)
+        out["edge%d_pos" % n] = pos
+        out["edge%d_edges" % n] = edges
+        for k, v in r.items():
+            out["edge%d_%s" % (n, k)] = v
     np.savez_compressed(os.path.join(HERE, "lbvh_ref.npz"), **out)
 
     R = oracle.ref()

@@ -32,6 +32,8 @@ def test_lbvh_matches_reference_fixtures(lbvh_gold):
     for c in cases:
         if c.startswith("pts"):
             r = oracle.lbvh_build_points(g[c + "_pos"])
+        elif c.startswith("edge"):
+            r = oracle.lbvh_build_edges(g[c + "_pos"], g[c + "_edges"])
         else:
             r = oracle.lbvh_build_tri(g[c + "_pos"], g[c + "_tri"])
         for k in ("scene", "codes", "ids", "nodes", "aabbs"):
@@ -142,3 +144,17 @@ def test_karras_structure_invariants():
             parent_count[r] += 1
         assert parent_count[0] == 0 and (parent_count[1:] == 1).all()
         assert nodes[0, 2] == -1
+
+
+def test_edge_lbvh_matches_reference_fixtures(lbvh_gold):
+    # ComputeEdgeBounds / ComputeEdgeMortonCodes / BuildEdgeHierarchy run from
+    # the reference's own sources (tests/golden/make_golden.py)
+    g = lbvh_gold
+    cases = sorted({k.rsplit("_", 1)[0] for k in g.files if k.startswith("edge") and k.endswith("_nodes")})
+    assert len(cases) >= 5
+    for c in cases:
+        r = oracle.lbvh_build_edges(g[c + "_pos"], g[c + "_edges"])
+        for k in ("scene", "codes", "ids", "nodes", "aabbs"):
+            exp = g[c + "_" + k].reshape(r[k].shape)
+            assert np.array_equal(np.ascontiguousarray(r[k]).view(np.uint32),
+                                  np.ascontiguousarray(exp).view(np.uint32)), (c, k)
