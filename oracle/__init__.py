@@ -59,6 +59,12 @@ def lib():
         L.orc_lbvh_build_tri.argtypes = [vp, vp, u32, i32, vp, vp, vp, vp, vp]
         L.orc_lbvh_build_points.argtypes = [vp, u32, i32, vp, vp, vp, vp, vp]
         L.orc_lbvh_build_edges.argtypes = [vp, vp, u32, i32, vp, vp, vp, vp, vp]
+        L.orc_lbvh_build_boxes.argtypes = [vp, u32, i32, vp, vp, vp, vp, vp]
+        L.orc_lss_intersect.argtypes = [vp, vp, vp, i32, i32, i32, vp, vp]
+        L.orc_lss_intersect.restype = i32
+        L.orc_lss_bounds.argtypes = [vp, vp, u32, i32, i32, vp]
+        L.orc_sphere_bounds.argtypes = [vp, u32, vp]
+        L.orc_trace_user_brute.argtypes = [i32, vp, vp, u32, i32, i32, i32, vp, u64, vp]
         L.orc_isect_tri32.argtypes = [vp, vp, vp, vp, vp]
         L.orc_isect_tri32.restype = i32
         L.orc_refine_t32.argtypes = [vp, vp, vp, vp]
@@ -202,6 +208,84 @@ def ref_lbvh_build(pos, tri=None):
     aabbs = np.zeros((2 * n - 1, 6), np.float32)
     ref().ref_lbvh_build(kind, _p(pos), pos.shape[0], _p(tri), n, _p(scene), _p(codes), _p(ids), _p(nodes),
                          _p(aabbs))
+    return dict(scene=scene, codes=codes, ids=ids, nodes=nodes, aabbs=aabbs)
+
+
+USER_HIT_DTYPE = np.dtype([("prim", np.uint32), ("t", np.float32), ("u", np.float32)])
+
+
+def lss_intersect(ray, v0, v1, cap0=True, cap1=True, exit_test=False):
+    """intersectRayLSS restated: (hit, t, u) for one ray {o, tmin, d, tmax} and
+    two float4 {xyz, radius} ends."""
+    a = [np.ascontiguousarray(v, dtype=np.float32) for v in (ray, v0, v1)]
+    t = np.zeros(1, np.float32)
+    u = np.zeros(1, np.float32)
+    hit = lib().orc_lss_intersect(_p(a[0]), _p(a[1]), _p(a[2]), int(cap0), int(cap1), int(exit_test), _p(t), _p(u))
+    return bool(hit), float(t[0]), float(u[0])
+
+
+def ref_lss_intersect(ray, v0, v1, cap0=True, cap1=True, exit_test=False):
+    """The reference's own intersectRayLSS (compiled from its sources)."""
+    a = [np.ascontiguousarray(v, dtype=np.float32) for v in (ray, v0, v1)]
+    t = np.zeros(1, np.float32)
+    u = np.zeros(1, np.float32)
+    R = ref()
+    R.ref_lss_intersect.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int] * 3 + [ctypes.c_void_p] * 2
+    R.ref_lss_intersect.restype = ctypes.c_int
+    hit = R.ref_lss_intersect(_p(a[0]), _p(a[1]), _p(a[2]), int(cap0), int(cap1), int(exit_test), _p(t), _p(u))
+    return bool(hit), t[0], u[0]
+
+
+def ref_lss_aabb(v0, v1, cap0, cap1):
+    """The reference's own computeLssAabb: [lo.xyz, hi.xyz]."""
+    a = [np.ascontiguousarray(v, dtype=np.float32) for v in (v0, v1)]
+    lo = np.zeros(3, np.float32)
+    hi = np.zeros(3, np.float32)
+    R = ref()
+    R.ref_lss_aabb.argtypes = [ctypes.c_void_p] * 2 + [ctypes.c_int] * 2 + [ctypes.c_void_p] * 2
+    R.ref_lss_aabb(_p(a[0]), _p(a[1]), int(cap0), int(cap1), _p(lo), _p(hi))
+    return np.concatenate([lo, hi])
+
+
+def lss_bounds(verts, idx, cap0=True, cap1=True):
+    verts = np.ascontiguousarray(verts, dtype=np.float32)
+    idx = np.ascontiguousarray(idx, dtype=np.uint32)
+    out = np.zeros((idx.shape[0], 6), np.float32)
+    lib().orc_lss_bounds(_p(verts), _p(idx), idx.shape[0], int(cap0), int(cap1), _p(out))
+    return out
+
+
+def sphere_bounds(spheres):
+    spheres = np.ascontiguousarray(spheres, dtype=np.float32)
+    out = np.zeros((spheres.shape[0], 6), np.float32)
+    lib().orc_sphere_bounds(_p(spheres), spheres.shape[0], _p(out))
+    return out
+
+
+def trace_user_brute(kind, prims, rays, idx=None, cap0=True, cap1=True, exit_test=False):
+    """Closest hit over every sphere (kind 0, prims float4[n]) or LSS (kind 1,
+    prims = vertices float4[], idx uint2[n]); ties to the lowest id."""
+    prims = np.ascontiguousarray(prims, dtype=np.float32)
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    idxa = None if idx is None else np.ascontiguousarray(idx, dtype=np.uint32)
+    n = prims.shape[0] if kind == 0 else idxa.shape[0]
+    hits = np.zeros(rays.shape[0], USER_HIT_DTYPE)
+    lib().orc_trace_user_brute(kind, _p(prims), _p(idxa), n, int(cap0), int(cap1), int(exit_test), _p(rays),
+                               rays.shape[0], _p(hits))
+    return hits
+
+
+def lbvh_build_boxes(boxes, kind=0):
+    """LBVH over primitive boxes [n][6] {lo, hi} (oracle layout dict)."""
+    boxes = np.ascontiguousarray(boxes, dtype=np.float32)
+    n = boxes.shape[0]
+    scene = np.zeros(6, np.float32)
+    codes = np.zeros(n, np.uint32)
+    ids = np.zeros(n, np.uint32)
+    nn = max(2 * n - 1, 0)
+    nodes = np.full((nn, 4), -1, np.int32)
+    aabbs = np.zeros((nn, 6), np.float32)
+    lib().orc_lbvh_build_boxes(_p(boxes), n, kind, _p(scene), _p(codes), _p(ids), _p(nodes), _p(aabbs))
     return dict(scene=scene, codes=codes, ids=ids, nodes=nodes, aabbs=aabbs)
 
 

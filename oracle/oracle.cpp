@@ -640,3 +640,231 @@ extern "C" int orc_num_threads(void) {
   return 1;
 #endif
 }
+
+// ============================================================================
+// Spheres and linearly swept spheres (LSS): the software counterparts of the
+// reference's AABB primitives (gprt/gprt_fallbacks.slang).  Each float op is
+// written out in the reference's evaluation order; dot(a, b) is
+// (a.x*b.x + a.y*b.y) + a.z*b.z and rcp(x) is 1/x.
+// ============================================================================
+static inline float dot3(f3 a, f3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+
+// intersectRayLSS (gprt/gprt_fallbacks.slang:45-144).
+static bool lss_intersect(f3 ro, f3 rd, f3 p0, f3 p1, float r0, float r1, bool cap0, bool cap1, float tmin,
+                          float tmax, bool exit_test, float *t_out, float *u_out) {
+  *t_out = 0.0f;
+  *u_out = 0.0f;
+  const f3 d = rd;
+  const f3 mid = {0.5f * (p0.x + p1.x), 0.5f * (p0.y + p1.y), 0.5f * (p0.z + p1.z)};
+  const float rmid = 0.5f * (r0 + r1);
+  const float dd = dot3(d, d);
+  const float inv_dd = 1.0f / dd;
+  const float align = dot3(d, f3{mid.x - ro.x, mid.y - ro.y, mid.z - ro.z}) * inv_dd;
+  ro = f3{ro.x + align * d.x, ro.y + align * d.y, ro.z + align * d.z};
+  const f3 off = {ro.x - mid.x, ro.y - mid.y, ro.z - mid.z};
+  const f3 axis = {p1.x - p0.x, p1.y - p0.y, p1.z - p0.z};
+  const float rdel = r1 - r0;
+  const float a = dd;
+  const float b = dot3(axis, d);
+  const float c = dot3(axis, axis) - rdel * rdel;
+  const float dq = dot3(d, off);
+  const float e = dot3(axis, off) + rmid * rdel;
+  const float f = dot3(off, off) - rmid * rmid;
+  const float At = b * b - a * c;
+  const float Bt = b * e - c * dq;
+  const float Ct = e * e - c * f;
+  const float disc = Bt * Bt - At * Ct;
+  const bool is_sphere = axis.x == 0 && axis.y == 0 && axis.z == 0 && rdel == 0;
+  const bool use_start_sphere = !cap1;
+  const bool shell_degenerate = (c <= 0) && (rdel != 0);
+  const bool invalid = (r0 <= 0 && r1 <= 0) || std::isnan(r0) || std::isnan(r1) || std::isnan(p0.x) ||
+                       std::isnan(p1.x) || std::isinf(r0) || std::isinf(p0.x);
+  if ((!is_sphere && !shell_degenerate && disc < 0) || invalid) return false;
+  const float sq = std::sqrt(disc);
+  const float inv_at = 1.0f / At;
+  const float t0 = (-Bt + (exit_test ? -sq : sq)) * inv_at;
+  const float inv_c = 1.0f / c;
+  const float u0 = (b * t0 + e) * inv_c;
+  if (std::fabs(u0) <= 0.5f && (u0 * rdel >= -rmid) && !is_sphere && !shell_degenerate) {
+    const float ht = t0 + align, hu = u0 + 0.5f;
+    if (ht <= tmin || ht >= tmax) return false;
+    *t_out = ht;
+    *u_out = hu;
+    return true;
+  }
+  const bool start_cap = is_sphere ? use_start_sphere : (u0 < 0.0f);
+  if ((start_cap && !cap0) || (!start_cap && !cap1)) return false;
+  const float Bs = -dq + (start_cap ? -b : b) * 0.5f;
+  const float BsBs = Bs * Bs;
+  const float Cs = f + 0.25f * c - (start_cap ? -e : e);
+  const float AsCs = a * Cs;
+  if (BsBs < AsCs) return false;
+  const float sqc = std::sqrt(BsBs - AsCs);
+  const float cap_t = (Bs - (exit_test ? -sqc : sqc)) * inv_dd;
+  *t_out = cap_t + align;
+  *u_out = start_cap ? 0.0f : 1.0f;
+  if (*t_out <= tmin || *t_out >= tmax) return false;
+  return true;
+}
+
+extern "C" int orc_lss_intersect(const float *ray, const float *v0, const float *v1, int cap0, int cap1, int exit_test,
+                                 float *t, float *u) {
+  return lss_intersect(f3{ray[0], ray[1], ray[2]}, f3{ray[4], ray[5], ray[6]}, f3{v0[0], v0[1], v0[2]},
+                       f3{v1[0], v1[1], v1[2]}, v0[3], v1[3], cap0 != 0, cap1 != 0, ray[3], ray[7], exit_test != 0, t,
+                       u)
+             ? 1
+             : 0;
+}
+
+// computeLssAabb (gprt/gprt_fallbacks.slang:168-213) and LSSBounds
+// (:215-235): vertices float4 {xyz, radius}, indices uint2 per segment;
+// aabbs [n][6] {lo.xyz, hi.xyz}.
+static void lss_aabb(f3 v0, float r0, bool cap0, f3 v1, float r1, bool cap1, float *lo, float *hi) {
+  f3 blo0 = v0, bhi0 = v0, blo1 = v1, bhi1 = v1;
+  f3 cme = {0, 0, 0}, cpe = {0, 0, 0};
+  if (!cap0 || !cap1) {
+    const float rd = r1 - r0;
+    const f3 n = {v0.x - v1.x, v0.y - v1.y, v0.z - v1.z};
+    const f3 nsq = {n.x * n.x, n.y * n.y, n.z * n.z};
+    const float l2 = (nsq.x + nsq.y) + nsq.z;
+    const float l2inv = 1.0f / l2;
+    const f3 X = {1.f - nsq.x * l2inv, 1.f - nsq.y * l2inv, 1.f - nsq.z * l2inv};
+    const float Y = 1.f - rd * rd * l2inv;
+    const f3 e = {std::sqrt(std::fabs(X.x * Y)), std::sqrt(std::fabs(X.y * Y)), std::sqrt(std::fabs(X.z * Y))};
+    const f3 c = {rd * n.x * l2inv, rd * n.y * l2inv, rd * n.z * l2inv};
+    cme = {c.x - e.x, c.y - e.y, c.z - e.z};
+    cpe = {c.x + e.x, c.y + e.y, c.z + e.z};
+  }
+  if (r0 < 0.0f) {
+    const float s = r0 * (1.0f / (r1 - r0));
+    blo0 = {blo0.x + s * (v0.x - v1.x), blo0.y + s * (v0.y - v1.y), blo0.z + s * (v0.z - v1.z)};
+    bhi0 = blo0;
+  } else if (cap0) {
+    blo0 = {blo0.x + -r0, blo0.y + -r0, blo0.z + -r0};
+    bhi0 = {bhi0.x + r0, bhi0.y + r0, bhi0.z + r0};
+  } else {
+    blo0 = {blo0.x + r0 * cme.x, blo0.y + r0 * cme.y, blo0.z + r0 * cme.z};
+    bhi0 = {bhi0.x + r0 * cpe.x, bhi0.y + r0 * cpe.y, bhi0.z + r0 * cpe.z};
+  }
+  if (r1 < 0.0f) {
+    const float s = r1 * (1.0f / (r1 - r0));
+    blo1 = {blo1.x + s * (v0.x - v1.x), blo1.y + s * (v0.y - v1.y), blo1.z + s * (v0.z - v1.z)};
+    bhi1 = blo1;
+  } else if (cap1) {
+    blo1 = {blo1.x + -r1, blo1.y + -r1, blo1.z + -r1};
+    bhi1 = {bhi1.x + r1, bhi1.y + r1, bhi1.z + r1};
+  } else {
+    blo1 = {blo1.x + r1 * cme.x, blo1.y + r1 * cme.y, blo1.z + r1 * cme.z};
+    bhi1 = {bhi1.x + r1 * cpe.x, bhi1.y + r1 * cpe.y, bhi1.z + r1 * cpe.z};
+  }
+  lo[0] = std::fmin(blo0.x, blo1.x);
+  lo[1] = std::fmin(blo0.y, blo1.y);
+  lo[2] = std::fmin(blo0.z, blo1.z);
+  hi[0] = std::fmax(bhi0.x, bhi1.x);
+  hi[1] = std::fmax(bhi0.y, bhi1.y);
+  hi[2] = std::fmax(bhi0.z, bhi1.z);
+}
+
+extern "C" void orc_lss_bounds(const float *verts, const uint32_t *idx, uint32_t n, int cap0, int cap1, float *aabbs) {
+  for (uint32_t i = 0; i < n; ++i) {
+    const float *a = verts + 4 * (size_t)idx[2 * i], *b = verts + 4 * (size_t)idx[2 * i + 1];
+    lss_aabb(f3{a[0], a[1], a[2]}, a[3], cap0 != 0, f3{b[0], b[1], b[2]}, b[3], cap1 != 0, aabbs + 6 * (size_t)i,
+             aabbs + 6 * (size_t)i + 3);
+  }
+}
+
+// SphereBounds (gprt/gprt_fallbacks.slang:263-283): spheres float4 {center, radius}.
+extern "C" void orc_sphere_bounds(const float *spheres, uint32_t n, float *aabbs) {
+  const float M = 3.402823466e38f;
+  for (uint32_t i = 0; i < n; ++i) {
+    const float *s = spheres + 4 * (size_t)i;
+    const float r = std::fmax(s[3], 0.0f);
+    for (int k = 0; k < 3; ++k) {
+      aabbs[6 * (size_t)i + k] = std::fmin(M, s[k] - r);
+      aabbs[6 * (size_t)i + 3 + k] = std::fmax(-M, s[k] + r);
+    }
+  }
+}
+
+// Closest hit over every primitive (SphereIntersection / LSSIntersection,
+// gprt/gprt_fallbacks.slang:146-166,245-261): the intersection is tested
+// against the ray's own [tmin, tmax]; the closest t wins, ties to the lowest
+// id.  kind 0: spheres (prims = float4 per sphere, the LSS test with both
+// ends equal and both caps on); kind 1: LSS (prims = vertices, idx = uint2).
+struct orc_uhit {
+  uint32_t prim;
+  float t;
+  float u;
+};
+extern "C" void orc_trace_user_brute(int kind, const float *prims, const uint32_t *idx, uint32_t n, int cap0, int cap1,
+                                     int exit_test, const float *rays, uint64_t nrays, orc_uhit *hits) {
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t r = 0; r < (int64_t)nrays; ++r) {
+    const float *ray = rays + 8 * r;
+    uint32_t best = 0xFFFFFFFFu;
+    float bt = 0.0f, bu = 0.0f;
+    for (uint32_t i = 0; i < n; ++i) {
+      const float *a = kind == 0 ? prims + 4 * (size_t)i : prims + 4 * (size_t)idx[2 * i];
+      const float *b = kind == 0 ? a : prims + 4 * (size_t)idx[2 * i + 1];
+      const bool c0 = kind == 0 ? true : cap0 != 0, c1 = kind == 0 ? true : cap1 != 0;
+      float t, u;
+      if (lss_intersect(f3{ray[0], ray[1], ray[2]}, f3{ray[4], ray[5], ray[6]}, f3{a[0], a[1], a[2]},
+                        f3{b[0], b[1], b[2]}, a[3], b[3], c0, c1, ray[3], ray[7], exit_test != 0, &t, &u) &&
+          (best == 0xFFFFFFFFu || t < bt)) {
+        best = i;
+        bt = t;
+        bu = u;
+      }
+    }
+    hits[r].prim = best;
+    hits[r].t = best == 0xFFFFFFFFu ? INFINITY : bt;
+    hits[r].u = best == 0xFFFFFFFFu ? 0.0f : bu;
+  }
+}
+
+// LBVH over given boxes [n][6] (the primitives' AABBs): centroid
+// (lo + hi) * 0.5, otherwise the same codes, sort, topology and refit.
+extern "C" void orc_lbvh_build_boxes(const float *boxes, uint32_t n, int kind, float scene[6], uint32_t *codes,
+                                     uint32_t *ids, int32_t *nodes, float *aabbs) {
+  const float M = 3.402823466e38f;
+  float s[6] = {M, M, M, -M, -M, -M};
+  for (uint32_t i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) {
+      s[k] = std::fmin(s[k], boxes[6 * (size_t)i + k]);
+      s[3 + k] = std::fmax(s[3 + k], boxes[6 * (size_t)i + 3 + k]);
+    }
+  std::memcpy(scene, s, sizeof(s));
+  for (uint32_t i = 0; i < n; ++i) {
+    const float *b = boxes + 6 * (size_t)i;
+    f3 c = {(b[0] + b[3]) * 0.5f, (b[1] + b[4]) * 0.5f, (b[2] + b[5]) * 0.5f};
+    codes[i] = code_of(c, scene, kind);
+    ids[i] = i;
+  }
+  orc_sort(codes, 4, ids, 4, n);
+  orc_karras(codes, n, nodes);
+  if (n == 0) return;
+  const int64_t N = n, inner = N - 1;
+  for (int64_t k = 0; k < 2 * N - 1; ++k)
+    for (int a = 0; a < 3; ++a) {
+      aabbs[6 * k + a] = 1e38f;
+      aabbs[6 * k + 3 + a] = -1e38f;
+    }
+  for (int64_t i = 0; i < N; ++i) {
+    std::memcpy(&aabbs[6 * (inner + i)], boxes + 6 * (size_t)ids[i], 24);
+    nodes[4 * (inner + i) + 3] = (int32_t)ids[i];
+  }
+  std::vector<uint8_t> seen(inner > 0 ? inner : 1, 0);
+  for (int64_t i = 0; i < N; ++i) {
+    int64_t cur = nodes[4 * (inner + i) + 2];
+    while (cur >= 0) {
+      if (seen[cur]++ == 0) break;
+      int64_t l = nodes[4 * cur], r = nodes[4 * cur + 1];
+      float *b = &aabbs[6 * cur];
+      for (int a = 0; a < 3; ++a) {
+        b[a] = std::fmin(b[a], std::fmin(aabbs[6 * l + a], aabbs[6 * r + a]));
+        b[3 + a] = std::fmax(b[3 + a], std::fmax(aabbs[6 * l + 3 + a], aabbs[6 * r + 3 + a]));
+      }
+      cur = nodes[4 * cur + 2];
+    }
+  }
+}

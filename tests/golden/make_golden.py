@@ -12,6 +12,9 @@
                     (tests/t04-swBVH/hostCode.cpp:47-56).
 * hilbert_ref.npz -- gprt/hilbert.h hilbert_c2i(3, 10, .) on seeded and corner
                     coordinates.
+* lss_ref.npz    -- intersectRayLSS and computeLssAabb of gprt/gprt_fallbacks.slang
+                    compiled from the reference sources, on seeded rays, spheres
+                    and swept-sphere segments, every cap / exit-test combination.
 * sortscan.npz   -- the reference tests' own host oracles restated with numpy:
                     std::sort / std::sort-by-key (tests/t02-bufferSort/hostCode.cpp:59,115),
                     the serial exclusive sum (tests/t03-bufferScans/hostCode.cpp:53-58)
@@ -34,6 +37,59 @@ def tri_soup(rng, n, sigma=0.002):
     pos = (np.repeat(c, 3, axis=0) + rng.normal(0.0, sigma, (3 * n, 3))).astype(np.float32)
     tri = np.arange(3 * n, dtype=np.uint32).reshape(n, 3)
     return pos, tri
+
+
+def lss_case_inputs(n=4000, seed=99):
+    """Seeded rays and sphere / swept-sphere segments: spheres, tapered and
+    constant-radius segments, a negative start radius; rays aimed near the
+    primitive so most hit."""
+    r = np.random.default_rng(seed)
+    rays = np.zeros((n, 8), np.float32)
+    v0 = np.zeros((n, 4), np.float32)
+    v1 = np.zeros((n, 4), np.float32)
+    for i in range(n):
+        kind = i % 4
+        c0 = r.normal(size=3) * 0.5
+        if kind == 0:
+            c1, r0 = c0.copy(), abs(r.normal()) * 0.5 + 0.01
+            r1 = r0
+        else:
+            c1 = c0 + r.normal(size=3) * 0.5
+            r0, r1 = abs(r.normal()) * 0.3 + 0.01, abs(r.normal()) * 0.3 + 0.01
+            if kind == 2:
+                r1 = r0
+            if kind == 3:
+                r0 = -0.1 * r0
+        o = r.normal(size=3)
+        o = o / np.linalg.norm(o) * 3.0
+        target = 0.5 * (c0 + c1) + r.normal(size=3) * 0.3
+        d = target - o
+        d /= np.linalg.norm(d)
+        rays[i] = [*o, 0.0, *d, np.inf]
+        v0[i] = [*c0, r0]
+        v1[i] = [*c1, r1]
+    return rays, v0, v1
+
+
+def lss_cases():
+    # the reference's intersectRayLSS and computeLssAabb (gprt/gprt_fallbacks.slang)
+    # compiled from its sources, on every combination of caps and exit test
+    rays, v0, v1 = lss_case_inputs()
+    out = {"rays": rays, "v0": v0, "v1": v1}
+    for cap0 in (0, 1):
+        for cap1 in (0, 1):
+            for ex in (0, 1):
+                hit = np.zeros(len(rays), np.uint8)
+                t = np.zeros(len(rays), np.float32)
+                u = np.zeros(len(rays), np.float32)
+                for i in range(len(rays)):
+                    h, tt, uu = oracle.ref_lss_intersect(rays[i], v0[i], v1[i], cap0, cap1, ex)
+                    hit[i], t[i], u[i] = h, tt, uu
+                key = "c%d%d_x%d" % (cap0, cap1, ex)
+                out[key + "_hit"], out[key + "_t"], out[key + "_u"] = hit, t, u
+            box = np.stack([oracle.ref_lss_aabb(v0[i], v1[i], cap0, cap1) for i in range(len(rays))])
+            out["c%d%d_aabb" % (cap0, cap1)] = box
+    np.savez_compressed(os.path.join(HERE, "lss_ref.npz"), **out)
 
 
 def main():
@@ -75,6 +131,8 @@ def main():
         for k, v in r.items():
             out["edge%d_%s" % (n, k)] = v
     np.savez_compressed(os.path.join(HERE, "lbvh_ref.npz"), **out)
+
+    lss_cases()
 
     R = oracle.ref()
     co = rng.integers(0, 1024, size=(4096, 3)).astype(np.uint32)

@@ -158,3 +158,31 @@ def test_edge_lbvh_matches_reference_fixtures(lbvh_gold):
             exp = g[c + "_" + k].reshape(r[k].shape)
             assert np.array_equal(np.ascontiguousarray(r[k]).view(np.uint32),
                                   np.ascontiguousarray(exp).view(np.uint32)), (c, k)
+
+
+def test_sphere_and_swept_sphere_math_matches_reference_fixture():
+    # intersectRayLSS / computeLssAabb (gprt/gprt_fallbacks.slang:45-144,168-213)
+    # compiled from the reference sources: hit flag, t and u bit-exact, boxes
+    # bit-exact, for every combination of end caps and exit test
+    g = np.load(os.path.join(GOLD, "lss_ref.npz"))
+    rays, v0, v1 = g["rays"], g["v0"], g["v1"]
+    total_hits = 0
+    for cap0 in (0, 1):
+        for cap1 in (0, 1):
+            box = oracle.lss_bounds(np.concatenate([v0, v1]),
+                                    np.stack([np.arange(len(v0)), len(v0) + np.arange(len(v0))], 1), cap0, cap1)
+            assert np.array_equal(_bits(box), _bits(g["c%d%d_aabb" % (cap0, cap1)]))
+            for ex in (0, 1):
+                key = "c%d%d_x%d" % (cap0, cap1, ex)
+                for i in range(len(rays)):
+                    hit, t, u = oracle.lss_intersect(rays[i], v0[i], v1[i], cap0, cap1, ex)
+                    assert hit == bool(g[key + "_hit"][i]), (key, i)
+                    if hit:
+                        total_hits += 1
+                        assert np.float32(t).view(np.uint32) == g[key + "_t"][i].view(np.uint32), (key, i)
+                        assert np.float32(u).view(np.uint32) == g[key + "_u"][i].view(np.uint32), (key, i)
+    assert total_hits > 5000
+    # SphereBounds (gprt/gprt_fallbacks.slang:263-283): center -/+ max(r, 0)
+    s = np.array([[0.5, -1.0, 2.0, 0.25], [1.0, 1.0, 1.0, -3.0]], np.float32)
+    assert np.array_equal(oracle.sphere_bounds(s), np.array([[0.25, -1.25, 1.75, 0.75, -0.75, 2.25],
+                                                             [1, 1, 1, 1, 1, 1]], np.float32))
