@@ -36,6 +36,11 @@ SIGNATURES = {
     "gprtcuLbvhBuildPoints": ([vp, u32, i32, vp, vp, sz, vp], st),
     "gprtcuLbvhBuildEdges": ([vp, vp, u32, i32, vp, vp, sz, vp], st),
     "gprtcuLbvhRefitTriangles": ([vp, vp, vp, u32, vp, vp, sz, vp], st),
+    "gprtcuSphereBounds": ([vp, u32, vp, vp], st),
+    "gprtcuLssBounds": ([vp, vp, u32, i32, i32, vp, vp], st),
+    "gprtcuLbvhBuildBoxes": ([vp, u32, i32, vp, vp, sz, vp], st),
+    "gprtcuTraceSpheres": ([vp, vp, vp, u64, i32, i32, vp, vp, vp, sz, vp], st),
+    "gprtcuTraceLss": ([vp, vp, vp, i32, i32, vp, u64, i32, i32, vp, vp, vp, sz, vp], st),
     "gprtcuTraceScratchSize": ([], sz),
     "gprtcuTraceClosest": ([vp, vp, u64, vp, vp, sz, vp], st),
     "gprtcuTraceAny": ([vp, vp, u64, vp, vp, sz, vp], st),

@@ -287,6 +287,66 @@ def trace(bvh, rays, hits=None, anyhit=False, scr=None):
     return hits
 
 
+# ---------------------------------------------------------------- spheres / LSS
+def sphere_bounds(spheres, out=None):
+    """Boxes [n, 6] of spheres float32 [n, 4] {center, radius}."""
+    _need_cuda(spheres)
+    n = spheres.shape[0]
+    if out is None:
+        out = torch.empty((n, 6), dtype=torch.float32, device=spheres.device)
+    _check(lib().gprtcuSphereBounds(_ptr(spheres), n, _ptr(out), _stream()), "gprtcuSphereBounds")
+    return out
+
+
+def lss_bounds(verts, idx, endcap0=True, endcap1=True, out=None):
+    """Boxes [n, 6] of swept-sphere segments (verts float32 [V, 4], idx int32 [n, 2])."""
+    _need_cuda(verts, idx)
+    n = idx.shape[0]
+    if out is None:
+        out = torch.empty((n, 6), dtype=torch.float32, device=verts.device)
+    _check(lib().gprtcuLssBounds(_ptr(verts), _ptr(idx), n, int(endcap0), int(endcap1), _ptr(out), _stream()),
+           "gprtcuLssBounds")
+    return out
+
+
+def lbvh_build_boxes(boxes, bvh=None, code_kind=0):
+    """LBVH with traversal nodes over primitive boxes [n, 6]."""
+    _need_cuda(boxes)
+    n = boxes.shape[0]
+    if bvh is None:
+        bvh = Lbvh(n, boxes.device)
+    st = lib().gprtcuLbvhBuildBoxes(_ptr(boxes), n, code_kind, ctypes.byref(bvh.desc), _ptr(bvh.scratch),
+                                    bvh.scratch.numel(), _stream())
+    _check(st, "gprtcuLbvhBuildBoxes")
+    return bvh
+
+
+def trace_spheres(bvh, spheres, rays, hits=None, u=None, anyhit=False, exit_test=False, scr=None):
+    _need_cuda(spheres, rays)
+    nr = rays.shape[0]
+    if hits is None:
+        hits = torch.empty((nr, 2), dtype=torch.int32, device=rays.device)
+    if scr is None:
+        scr = scratch(lib().gprtcuTraceScratchSize(), rays.device)
+    _check(lib().gprtcuTraceSpheres(ctypes.byref(bvh.desc), _ptr(spheres), _ptr(rays), nr, int(anyhit), int(exit_test),
+                                    _ptr(hits), _ptr(u), _ptr(scr), scr.numel(), _stream()), "gprtcuTraceSpheres")
+    return hits
+
+
+def trace_lss(bvh, verts, idx, rays, endcap0=True, endcap1=True, hits=None, u=None, anyhit=False, exit_test=False,
+              scr=None):
+    _need_cuda(verts, idx, rays)
+    nr = rays.shape[0]
+    if hits is None:
+        hits = torch.empty((nr, 2), dtype=torch.int32, device=rays.device)
+    if scr is None:
+        scr = scratch(lib().gprtcuTraceScratchSize(), rays.device)
+    _check(lib().gprtcuTraceLss(ctypes.byref(bvh.desc), _ptr(verts), _ptr(idx), int(endcap0), int(endcap1), _ptr(rays),
+                                nr, int(anyhit), int(exit_test), _ptr(hits), _ptr(u), _ptr(scr), scr.numel(),
+                                _stream()), "gprtcuTraceLss")
+    return hits
+
+
 def hits_numpy(hits):
     """Device hits -> numpy structured array {prim uint32, t float32}."""
     import numpy as np

@@ -145,10 +145,16 @@ __device__ __forceinline__ void load_edge(const float *pos, const uint32_t *edge
   }
 }
 
-// KIND: 0 triangles (tri = uint3 indices), 1 points, 2 edges (tri = uint2 indices).
+// KIND: 0 triangles (tri = uint3 indices), 1 points, 2 edges (tri = uint2
+// indices), 3 boxes (pos = float[n][6] {lo, hi}, the AABBs of user primitives).
 template <int KIND>
 __device__ __forceinline__ void prim_box(const float *pos, const uint32_t *tri, uint64_t id, float v[9], float b[6]) {
-  if (KIND == 0) {
+  if (KIND == 3) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) b[k] = pos[6 * (size_t)id + k];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) v[k] = 0.0f;
+  } else if (KIND == 0) {
     load_tri(pos, tri, (uint32_t)id, v);
     tri_box(v, b);
   } else if (KIND == 2) {
@@ -256,6 +262,9 @@ __global__ void __launch_bounds__(256) k_codes(const float *pos, const uint32_t 
       load_edge(pos, tri, (uint32_t)i, v);
 #pragma unroll
       for (int k = 0; k < 3; ++k) c[k] = __fdiv_rn(__fadd_rn(v[k], v[3 + k]), 2.0f);
+    } else if (KIND == 3) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) c[k] = __fmul_rn(__fadd_rn(pos[6 * (size_t)i + k], pos[6 * (size_t)i + 3 + k]), 0.5f);
     } else {
 #pragma unroll
       for (int k = 0; k < 3; ++k) c[k] = pos[3 * (size_t)i + k];
@@ -480,9 +489,10 @@ void launch_build(const float *pos, const uint32_t *tri, MeshMap mm, int codeKin
     if (mm.n > mm.meshes)
       k_karras<BATCHED><<<(unsigned)((mm.n - mm.meshes + 255) / 256), 256, 0, stream>>>(out->codes, keys, mm, nodes,
                                                                                          (Bvh2Node *)out->bvh2);
-    // the traversal layout (bvh2, leafTris) exists for triangles only
+    // traversal nodes for triangles and user-primitive boxes; leaf-order
+    // triangles for triangles only
     k_refit<KIND, BATCHED><<<(unsigned)((mm.n + 255) / 256), 256, 0, stream>>>(
-        pos, tri, out->ids, keys, mm, nodes, out->aabbs, KIND == 0 ? (Bvh2Node *)out->bvh2 : nullptr,
+        pos, tri, out->ids, keys, mm, nodes, out->aabbs, (KIND == 0 || KIND == 3) ? (Bvh2Node *)out->bvh2 : nullptr,
         KIND == 0 ? (float4 *)out->leafTris : nullptr, out->codes, arrivals, out->rootBox);
   }
 }
@@ -490,13 +500,13 @@ void launch_build(const float *pos, const uint32_t *tri, MeshMap mm, int codeKin
 gprtcuStatus lbvh_build(int kind, const float *pos, const uint32_t *tri, const uint32_t *prim_off, uint32_t meshes,
                         uint32_t n, int codeKind, gprtcuLbvh *out, void *scratch, size_t scratchBytes,
                         cudaStream_t stream) {
-  if (!out || !pos || (kind != 1 && !tri)) return GPRTCU_ERR_INVALID_ARG;
-  if (kind == 2 && meshes > 1) return GPRTCU_ERR_INVALID_ARG;
+  if (!out || !pos || ((kind == 0 || kind == 2) && !tri)) return GPRTCU_ERR_INVALID_ARG;
+  if (kind >= 2 && meshes > 1) return GPRTCU_ERR_INVALID_ARG;
   if (n == 0 || meshes == 0 || meshes > n) return GPRTCU_ERR_INVALID_ARG;
   if (meshes > 1 && !prim_off) return GPRTCU_ERR_INVALID_ARG;
   if (n > (1u << 30) - 1) return GPRTCU_ERR_TOO_LARGE;
   if (!out->codes || !out->ids || !out->nodes) return GPRTCU_ERR_INVALID_ARG;
-  if (n > meshes && !out->aabbs && (kind != 0 || !out->bvh2)) return GPRTCU_ERR_INVALID_ARG;  // one box store
+  if (n > meshes && !out->aabbs && ((kind != 0 && kind != 3) || !out->bvh2)) return GPRTCU_ERR_INVALID_ARG;
   if (out->bvh2 && ((uintptr_t)out->bvh2 & 15)) return GPRTCU_ERR_INVALID_ARG;
   if (out->leafTris && ((uintptr_t)out->leafTris & 15)) return GPRTCU_ERR_INVALID_ARG;
   if (codeKind != 0 && codeKind != 1) return GPRTCU_ERR_INVALID_ARG;
@@ -522,6 +532,7 @@ gprtcuStatus lbvh_build(int kind, const float *pos, const uint32_t *tri, const u
     if (kind == 0 && batched) launch_build<0, true>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
     else if (kind == 0) launch_build<0, false>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
     else if (kind == 2) launch_build<2, false>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
+    else if (kind == 3) launch_build<3, false>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
     else if (batched) launch_build<1, true>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
     else launch_build<1, false>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
     GPRTCU_TRY(cudaGetLastError());
@@ -551,6 +562,13 @@ extern "C" GPRTCU_API gprtcuStatus gprtcuLbvhBuildEdges(const float *positions, 
                                                         uint32_t numEdges, int codeKind, gprtcuLbvh *bvh, void *scratch,
                                                         size_t scratchBytes, gprtcuStream stream) {
   return lbvh_build(2, positions, edges, nullptr, 1, numEdges, codeKind, bvh, scratch, scratchBytes,
+                    (cudaStream_t)stream);
+}
+
+extern "C" GPRTCU_API gprtcuStatus gprtcuLbvhBuildBoxes(const float *aabbs, uint32_t numBoxes, int codeKind,
+                                                        gprtcuLbvh *bvh, void *scratch, size_t scratchBytes,
+                                                        gprtcuStream stream) {
+  return lbvh_build(3, aabbs, nullptr, nullptr, 1, numBoxes, codeKind, bvh, scratch, scratchBytes,
                     (cudaStream_t)stream);
 }
 

@@ -242,6 +242,36 @@ GPRTCU_API gprtcuStatus gprtcuTraceAny(const gprtcuLbvh *bvh, const float *rays,
                                        void *scratch, size_t scratchBytes, gprtcuStream stream);
 
 /* ------------------------------------------------------------------------
+ * Spheres and linearly swept spheres (LSS) as software-BVH primitives.  The
+ * reference builds hardware AABB structures over the boxes of its
+ * SphereBounds / LSSBounds programs and intersects with intersectRayLSS
+ * (gprt/gprt_fallbacks.slang:45-144,168-283; gprtSphereAccelCreate /
+ * gprtLSSAccelCreate, gprt/gprt_host.h).  Here: the same bounds, an LBVH over
+ * them (gprtcuLbvhBuildBoxes: codes of the box centres, then as for
+ * triangles; fills codes, ids, nodes, aabbs, sceneBounds, rootBox and the
+ * bvh2 traversal nodes; leafTris unused), and a traversal that runs the same
+ * intersection at the leaves.  Spheres: float4 {center, radius}.  LSS:
+ * vertices float4 {position, radius}, indices uint32[n][2], end caps on or off
+ * for the whole set.  exitTest reports the exit point instead of the entry.
+ * Hits: {primitive index, t}; hitU (optional, one float per ray) receives the
+ * curve parameter u (0 for spheres).  Closest hit: smallest t in the ray's
+ * (tmin, tmax), ties to the lowest index.  Results are bit-identical to the
+ * reference's intersectRayLSS / computeLssAabb compiled for the host.
+ * ------------------------------------------------------------------------ */
+GPRTCU_API gprtcuStatus gprtcuSphereBounds(const float *spheres, uint32_t n, float *aabbs, gprtcuStream stream);
+GPRTCU_API gprtcuStatus gprtcuLssBounds(const float *vertices, const uint32_t *indices, uint32_t n, int endcap0,
+                                        int endcap1, float *aabbs, gprtcuStream stream);
+GPRTCU_API gprtcuStatus gprtcuLbvhBuildBoxes(const float *aabbs, uint32_t numBoxes, int codeKind, gprtcuLbvh *bvh,
+                                             void *scratch, size_t scratchBytes, gprtcuStream stream);
+GPRTCU_API gprtcuStatus gprtcuTraceSpheres(const gprtcuLbvh *bvh, const float *spheres, const float *rays,
+                                           uint64_t numRays, int anyHit, int exitTest, gprtcuHit *hits, float *hitU,
+                                           void *scratch, size_t scratchBytes, gprtcuStream stream);
+GPRTCU_API gprtcuStatus gprtcuTraceLss(const gprtcuLbvh *bvh, const float *vertices, const uint32_t *indices,
+                                       int endcap0, int endcap1, const float *rays, uint64_t numRays, int anyHit,
+                                       int exitTest, gprtcuHit *hits, float *hitU, void *scratch, size_t scratchBytes,
+                                       gprtcuStream stream);
+
+/* ------------------------------------------------------------------------
  * Batched build and trace: many meshes in one set of launches.  No
  * counterpart in the reference beyond repeated gprtLBVHBuild calls
  * (gprt/development/gprt_lbvh.h:170-195), one per mesh.
