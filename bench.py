@@ -32,6 +32,8 @@ The JSON line's value is whole-job Mrays/s of that step.  It also carries:
   small_lbvh    plain LBVH build + trace, 262,144 triangles, 1,048,576 rays
   wide_bvh      binary against quantised wide BVH, 16,777,216 triangles and
                 rays, closest and any hit
+  spheres, lss  4,194,304 spheres / swept-sphere segments (hair strands):
+                bounds + box LBVH build and closest-hit trace of 4,194,304 rays
   sort, scan    268,435,456 Zipf(1.1) uint32 key/payload pairs and a
                 1,073,741,824-element uint32 exclusive sum, GB/s of
                 algorithmic traffic against the measured HBM bandwidth
@@ -410,6 +412,10 @@ def run_b200(args, world, rank, local):
         ws = workloads.WideScene(device=dev)
         extra["wide_bvh"] = ws.run(steps=2, warmup=1, flush=flush)
         del ws
+        for kind in ("spheres", "lss"):
+            us = workloads.UserScene(kind, device=dev)
+            extra[kind] = us.run(steps=3, warmup=1, flush=flush)
+            del us
         torch.cuda.empty_cache()
         del flush
         torch.cuda.empty_cache()

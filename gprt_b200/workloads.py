@@ -241,3 +241,62 @@ def large_cpu_sample(min_tris=1 << 21, meshes=16_384, n=67_108_864, rays_per_tri
         rays = scenes.device_rays_range(ray_seed, lo * rays_per_tri, hi * rays_per_tri, *box)
         out.append((pos, tri, rays))
     return out
+
+
+class UserScene:
+    """Spheres (radius uniform in [0.0005, 0.002], centres uniform in the unit
+    cube) or swept-sphere hair strands (random walks of 16 segments, radius
+    tapering from [0.0005, 0.0015] to half), n primitives, nrays rays as in
+    PlainScene; bounds + box LBVH + closest-hit trace."""
+
+    def __init__(self, kind="spheres", n=4_194_304, nrays=4_194_304, seed=7, device="cuda"):
+        dev = torch.device(device)
+        rng = np.random.default_rng(seed)
+        self.kind, self.n, self.nrays = kind, n, nrays
+        if kind == "spheres":
+            s = np.empty((n, 4), np.float32)
+            s[:, :3] = rng.random((n, 3), dtype=np.float32)
+            s[:, 3] = rng.uniform(0.0005, 0.002, n).astype(np.float32)
+            self.prims = torch.from_numpy(s).to(dev)
+            self.idx = None
+        else:
+            segs = 16
+            strands = n // segs
+            start = rng.random((strands, 1, 3))
+            steps = rng.normal(0.0, 0.004, (strands, segs, 3))
+            p = np.concatenate([start, start + np.cumsum(steps, axis=1)], axis=1)
+            r0 = rng.uniform(0.0005, 0.0015, (strands, 1))
+            r = r0 * (1.0 - 0.5 * np.arange(segs + 1)[None, :] / segs)
+            v = np.concatenate([p, r[:, :, None]], axis=2).reshape(-1, 4).astype(np.float32)
+            base = (np.arange(strands) * (segs + 1))[:, None] + np.arange(segs)[None, :]
+            idx = np.stack([base, base + 1], axis=2).reshape(-1, 2).astype(np.int32)
+            self.prims = torch.from_numpy(v).to(dev)
+            self.idx = torch.from_numpy(idx).to(dev)
+            self.n = idx.shape[0]
+        self.rays = api.gen_rays(nrays, seed=seed + 1, device=dev)
+        self.boxes = torch.empty((self.n, 6), dtype=torch.float32, device=dev)
+        self.bvh = api.Lbvh(self.n, dev)
+        self.hits = torch.empty((nrays, 2), dtype=torch.int32, device=dev)
+        self.u = torch.empty(nrays, dtype=torch.float32, device=dev)
+        self.tscr = api.scratch(lib().gprtcuTraceScratchSize(), dev)
+
+    def build(self):
+        if self.idx is None:
+            api.sphere_bounds(self.prims, out=self.boxes)
+        else:
+            api.lss_bounds(self.prims, self.idx, out=self.boxes)
+        api.lbvh_build_boxes(self.boxes, self.bvh)
+
+    def trace(self):
+        if self.idx is None:
+            api.trace_spheres(self.bvh, self.prims, self.rays, self.hits, self.u, scr=self.tscr)
+        else:
+            api.trace_lss(self.bvh, self.prims, self.idx, self.rays, hits=self.hits, u=self.u, scr=self.tscr)
+
+    def run(self, steps=3, warmup=1, flush=None):
+        tb = float(np.mean(time_steps(self.build, steps, warmup, flush)))
+        tt = float(np.mean(time_steps(self.trace, steps, warmup, flush)))
+        return {"primitives": self.n, "rays": self.nrays, "build_ms": tb, "trace_ms": tt,
+                "build_mprims_s": self.n / tb / 1e3, "trace_mrays_s": self.nrays / tt / 1e3,
+                "step_mrays_s": self.nrays / (tb + tt) / 1e3,
+                "hit_fraction": float((self.hits[:, 0] != -1).float().mean().item())}
