@@ -347,6 +347,50 @@ def trace_lss(bvh, verts, idx, rays, endcap0=True, endcap1=True, hits=None, u=No
     return hits
 
 
+# ---------------------------------------------------------------- instancing
+INSTANCE_DTYPE = [("transform", "<f4", (12,)), ("custom_mask", "<u4"), ("geom_flags", "<u4"), ("blas", "<u8")]
+
+
+def instances_tensor(records, device="cuda"):
+    """Device copy (uint8 [n, 64]) of a numpy array of INSTANCE_DTYPE records."""
+    import numpy as np
+    rec = np.ascontiguousarray(records, dtype=np.dtype(INSTANCE_DTYPE))
+    return torch.from_numpy(rec.view(np.uint8).reshape(-1, 64).copy()).to(device)
+
+
+class Tlas:
+    """Top level over instances: world-to-object matrices, world boxes and a
+    box LBVH over them (see gprtcuInstancesPrepare)."""
+
+    def __init__(self, instances, root_boxes, meshes):
+        n = instances.shape[0]
+        dev = instances.device
+        self.instances = instances
+        self.w2o = torch.empty((n, 12), dtype=torch.float32, device=dev)
+        self.boxes = torch.empty((n, 6), dtype=torch.float32, device=dev)
+        _check(lib().gprtcuInstancesPrepare(_ptr(instances), n, _ptr(root_boxes), meshes, _ptr(self.w2o),
+                                            _ptr(self.boxes), _stream()), "gprtcuInstancesPrepare")
+        self.bvh = lbvh_build_boxes(self.boxes)
+
+
+def trace_instances(tlas, blas, rays, tri_off=None, meshes=1, ray_mask=0xFF, hits=None, inst=None, anyhit=False,
+                    scr=None):
+    """Closest/any hit through a Tlas over the meshes of `blas` (Lbvh or BatchLbvh)."""
+    _need_cuda(rays)
+    nr = rays.shape[0]
+    if hits is None:
+        hits = torch.empty((nr, 2), dtype=torch.int32, device=rays.device)
+    if inst is None:
+        inst = torch.empty(nr, dtype=torch.int32, device=rays.device)
+    if scr is None:
+        scr = scratch(lib().gprtcuTraceScratchSize(), rays.device)
+    _check(lib().gprtcuTraceInstances(ctypes.byref(tlas.bvh.desc), _ptr(tlas.instances), _ptr(tlas.w2o),
+                                      ctypes.byref(blas.desc), _ptr(tri_off), meshes, _ptr(rays), nr, ray_mask,
+                                      int(anyhit), _ptr(hits), _ptr(inst), _ptr(scr), scr.numel(), _stream()),
+           "gprtcuTraceInstances")
+    return hits, inst
+
+
 def hits_numpy(hits):
     """Device hits -> numpy structured array {prim uint32, t float32}."""
     import numpy as np

@@ -272,6 +272,43 @@ GPRTCU_API gprtcuStatus gprtcuTraceLss(const gprtcuLbvh *bvh, const float *verti
                                        gprtcuStream stream);
 
 /* ------------------------------------------------------------------------
+ * Two-level instancing.  Replaces gprtInstanceAccelCreate + TraceRay over an
+ * instance acceleration structure (gprt/gprt_host.h:1418; instance record
+ * gprt::Instance, gprt/gprt_shared.h:92-101) in software: a top-level LBVH
+ * over the instances' world boxes, bottom levels = the meshes of a batched
+ * LBVH (gprtcuBatchBuildTriangles; triOffsets/numMeshes as there) or of one
+ * LBVH (numMeshes = 1).  The record keeps the reference's 64-byte layout;
+ * `blas` (accelAddress there) is the mesh index.  geometryIndexAndFlags is
+ * not used.
+ *   gprtcuInstancesPrepare: per instance, worldToObject float[n][12] (the
+ *     inverse transform, computed in double and rounded once) and worldBoxes
+ *     float[n][6] (the mesh's rootBox mapped to world space, rounded outward;
+ *     empty for a singular transform or a mesh index out of range, so such
+ *     instances are never hit).  Build the top level over worldBoxes with
+ *     gprtcuLbvhBuildBoxes.
+ *   gprtcuTraceInstances: an instance is visible when (mask & rayMask) != 0.
+ *     Closest hit: smallest t, ties to the lowest (instance, primitive); hits
+ *     report mesh-local primitive ids, hitInstance (optional) the instance
+ *     index.  The ray enters an instance as ((w0*x + w1*y) + w2*z) + w3 per
+ *     component in float, keeping tmin/tmax (an affine map keeps the ray
+ *     parameter); t is refined in that object space. */
+typedef struct {
+  float transform[12];            /* row-major 3x4 object-to-world */
+  uint32_t customIndexAndMask;    /* instanceCustomIndex (bits 0-23) | mask (bits 24-31) */
+  uint32_t geometryIndexAndFlags; /* not used */
+  uint64_t blas;                  /* mesh index of the bottom-level batch */
+} gprtcuInstance;
+GPRTCU_API gprtcuStatus gprtcuInstancesPrepare(const gprtcuInstance *instances, uint32_t numInstances,
+                                               const float *blasRootBoxes, uint32_t numMeshes, float *worldToObject,
+                                               float *worldBoxes, gprtcuStream stream);
+GPRTCU_API gprtcuStatus gprtcuTraceInstances(const gprtcuLbvh *tlas, const gprtcuInstance *instances,
+                                             const float *worldToObject, const gprtcuLbvh *blas,
+                                             const uint32_t *triOffsets, uint32_t numMeshes, const float *rays,
+                                             uint64_t numRays, uint32_t rayMask, int anyHit, gprtcuHit *hits,
+                                             uint32_t *hitInstance, void *scratch, size_t scratchBytes,
+                                             gprtcuStream stream);
+
+/* ------------------------------------------------------------------------
  * Batched build and trace: many meshes in one set of launches.  No
  * counterpart in the reference beyond repeated gprtLBVHBuild calls
  * (gprt/development/gprt_lbvh.h:170-195), one per mesh.

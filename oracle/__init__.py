@@ -65,6 +65,9 @@ def lib():
         L.orc_lss_bounds.argtypes = [vp, vp, u32, i32, i32, vp]
         L.orc_sphere_bounds.argtypes = [vp, u32, vp]
         L.orc_trace_user_brute.argtypes = [i32, vp, vp, u32, i32, i32, i32, vp, u64, vp]
+        L.orc_instance_inverse.argtypes = [vp, vp]
+        L.orc_instance_inverse.restype = i32
+        L.orc_trace_instances_brute.argtypes = [vp, u32, vp, vp, vp, u32, vp, u64, u32, vp]
         L.orc_isect_tri32.argtypes = [vp, vp, vp, vp, vp]
         L.orc_isect_tri32.restype = i32
         L.orc_refine_t32.argtypes = [vp, vp, vp, vp]
@@ -287,6 +290,32 @@ def lbvh_build_boxes(boxes, kind=0):
     aabbs = np.zeros((nn, 6), np.float32)
     lib().orc_lbvh_build_boxes(_p(boxes), n, kind, _p(scene), _p(codes), _p(ids), _p(nodes), _p(aabbs))
     return dict(scene=scene, codes=codes, ids=ids, nodes=nodes, aabbs=aabbs)
+
+
+INSTANCE_DTYPE = np.dtype([("transform", np.float32, (12,)), ("custom_mask", np.uint32),
+                           ("geom_flags", np.uint32), ("blas", np.uint64)])
+INST_HIT_DTYPE = np.dtype([("prim", np.uint32), ("t", np.float32), ("inst", np.uint32)])
+
+
+def instance_inverse(m):
+    """World-to-object 3x4 matrix of a row-major object-to-world one (None if singular)."""
+    m = np.ascontiguousarray(m, dtype=np.float32).reshape(12)
+    w = np.zeros(12, np.float32)
+    return w if lib().orc_instance_inverse(_p(m), _p(w)) else None
+
+
+def trace_instances_brute(instances, pos, tri, tri_off, rays, ray_mask=0xFF):
+    """Closest hit over every triangle of every visible instance; ties to the
+    lowest (instance, primitive); mesh-local primitive ids."""
+    inst = np.ascontiguousarray(instances, dtype=INSTANCE_DTYPE)
+    pos = np.ascontiguousarray(pos, dtype=np.float32)
+    tri = np.ascontiguousarray(tri, dtype=np.uint32)
+    off = np.ascontiguousarray(tri_off, dtype=np.uint32)
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    hits = np.zeros(rays.shape[0], INST_HIT_DTYPE)
+    lib().orc_trace_instances_brute(_p(inst), inst.size, _p(pos), _p(tri), _p(off), off.size - 1, _p(rays),
+                                    rays.shape[0], ray_mask, _p(hits))
+    return hits
 
 
 def trace_brute(pos, tri, rays):

@@ -868,3 +868,110 @@ extern "C" void orc_lbvh_build_boxes(const float *boxes, uint32_t n, int kind, f
     }
   }
 }
+
+// ============================================================================
+// Two-level instancing: instances of the meshes of a batch, each with a
+// row-major 3x4 object-to-world transform (the reference's gprt::Instance,
+// gprt/gprt_shared.h:92-101: transform, customIndex:24, mask:8,
+// geometryIndex:24, flags:8, accelAddress -- here the mesh index).
+// ============================================================================
+struct orc_instance {
+  float m[12];
+  uint32_t custom_mask;
+  uint32_t geom_flags;
+  uint64_t blas;
+};
+struct orc_ihit {
+  uint32_t prim;
+  float t;
+  uint32_t inst;
+};
+
+// World-to-object matrix: the inverse of [A | t] by adjugate and determinant
+// in double, in a fixed operation order, each entry rounded once to float.
+// False (and zeros) when A is singular.
+extern "C" int orc_instance_inverse(const float *m, float *w) {
+  const double a00 = m[0], a01 = m[1], a02 = m[2], t0 = m[3];
+  const double a10 = m[4], a11 = m[5], a12 = m[6], t1 = m[7];
+  const double a20 = m[8], a21 = m[9], a22 = m[10], t2 = m[11];
+  const double c00 = a11 * a22 - a12 * a21, c01 = a12 * a20 - a10 * a22, c02 = a10 * a21 - a11 * a20;
+  const double c10 = a02 * a21 - a01 * a22, c11 = a00 * a22 - a02 * a20, c12 = a01 * a20 - a00 * a21;
+  const double c20 = a01 * a12 - a02 * a11, c21 = a02 * a10 - a00 * a12, c22 = a00 * a11 - a01 * a10;
+  const double det = (a00 * c00 + a01 * c01) + a02 * c02;
+  if (!(det != 0.0) || !std::isfinite(det)) {
+    for (int k = 0; k < 12; ++k) w[k] = 0.0f;
+    return 0;
+  }
+  const double i00 = c00 / det, i01 = c10 / det, i02 = c20 / det;
+  const double i10 = c01 / det, i11 = c11 / det, i12 = c21 / det;
+  const double i20 = c02 / det, i21 = c12 / det, i22 = c22 / det;
+  const double u0 = -((i00 * t0 + i01 * t1) + i02 * t2);
+  const double u1 = -((i10 * t0 + i11 * t1) + i12 * t2);
+  const double u2 = -((i20 * t0 + i21 * t1) + i22 * t2);
+  const double r[12] = {i00, i01, i02, u0, i10, i11, i12, u1, i20, i21, i22, u2};
+  for (int k = 0; k < 12; ++k) w[k] = (float)r[k];
+  return 1;
+}
+
+// The ray in an instance's object space: origin and direction through the
+// world-to-object matrix, each component ((w0*x + w1*y) + w2*z) (+ w3), in
+// float; tmin / tmax unchanged (an affine map keeps the ray parameter).
+static inline void ray_to_object(const float *w, const float *ray, float *out) {
+  for (int i = 0; i < 3; ++i) {
+    out[i] = ((w[4 * i] * ray[0] + w[4 * i + 1] * ray[1]) + w[4 * i + 2] * ray[2]) + w[4 * i + 3];
+    out[4 + i] = (w[4 * i] * ray[4] + w[4 * i + 1] * ray[5]) + w[4 * i + 2] * ray[6];
+  }
+  out[3] = ray[3];
+  out[7] = ray[7];
+}
+
+// Closest hit over every triangle of every visible instance ((mask & rayMask)
+// != 0, non-singular transform): ties to the lowest (instance, primitive).
+// Primitive ids are mesh-local; t is the refined plane-equation distance in
+// the winning instance's object space.
+extern "C" void orc_trace_instances_brute(const orc_instance *inst, uint32_t ninst, const float *pos,
+                                          const uint32_t *tri, const uint32_t *tri_off, uint32_t meshes,
+                                          const float *rays, uint64_t nrays, uint32_t ray_mask, orc_ihit *hits) {
+  std::vector<float> w(12 * (size_t)ninst);
+  std::vector<uint8_t> ok(ninst);
+  for (uint32_t i = 0; i < ninst; ++i) ok[i] = (uint8_t)orc_instance_inverse(inst[i].m, &w[12 * (size_t)i]);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t r = 0; r < (int64_t)nrays; ++r) {
+    const float *ray = rays + 8 * r;
+    uint32_t best = 0xFFFFFFFFu, binst = 0xFFFFFFFFu;
+    float bt = 0.0f;
+    float bro[8] = {0};
+    for (uint32_t i = 0; i < ninst; ++i) {
+      if (!ok[i] || !((inst[i].custom_mask >> 24) & ray_mask)) continue;
+      const uint32_t m = (uint32_t)inst[i].blas;
+      if (m >= meshes) continue;
+      float ro[8];
+      ray_to_object(&w[12 * (size_t)i], ray, ro);
+      RayPre p;
+      ray_pre(ro, p);
+      const uint32_t b = tri_off ? tri_off[m] : 0u, e = tri_off ? tri_off[m + 1] : 0u;
+      for (uint32_t k = b; k < e; ++k) {
+        const float *va, *vb, *vc;
+        tri_verts(pos, tri, k, va, vb, vc);
+        float t;
+        const uint32_t local = k - b;
+        if (isect32(p, va, vb, vc, &t) &&
+            (best == 0xFFFFFFFFu || t < bt || (t == bt && (i < binst || (i == binst && local < best))))) {
+          best = local;
+          binst = i;
+          bt = t;
+          std::memcpy(bro, ro, sizeof(ro));
+        }
+      }
+    }
+    hits[r].prim = best;
+    hits[r].inst = binst;
+    if (best != 0xFFFFFFFFu) {
+      const float *va, *vb, *vc;
+      tri_verts(pos, tri, tri_off[(uint32_t)inst[binst].blas] + best, va, vb, vc);
+      hits[r].t = orc_refine_t32(bro, va, vb, vc);
+    } else {
+      hits[r].t = INFINITY;
+    }
+  }
+}
