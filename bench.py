@@ -34,6 +34,9 @@ The JSON line's value is whole-job Mrays/s of that step.  It also carries:
                 rays, closest and any hit
   spheres, lss  4,194,304 spheres / swept-sphere segments (hair strands):
                 bounds + box LBVH build and closest-hit trace of 4,194,304 rays
+  instances     two-level scene: 16,384 instances of 64 meshes (4,194,304
+                triangles), top-level rebuild and closest-hit trace of
+                16,777,216 rays
   sort, scan    268,435,456 Zipf(1.1) uint32 key/payload pairs and a
                 1,073,741,824-element uint32 exclusive sum, GB/s of
                 algorithmic traffic against the measured HBM bandwidth
@@ -416,6 +419,9 @@ def run_b200(args, world, rank, local):
             us = workloads.UserScene(kind, device=dev)
             extra[kind] = us.run(steps=3, warmup=1, flush=flush)
             del us
+        isc = workloads.InstanceScene(device=dev)
+        extra["instances"] = isc.run(steps=3, warmup=1, flush=flush)
+        del isc
         torch.cuda.empty_cache()
         del flush
         torch.cuda.empty_cache()

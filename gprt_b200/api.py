@@ -365,12 +365,19 @@ class Tlas:
     def __init__(self, instances, root_boxes, meshes):
         n = instances.shape[0]
         dev = instances.device
-        self.instances = instances
+        self.instances, self.root_boxes, self.meshes = instances, root_boxes, meshes
         self.w2o = torch.empty((n, 12), dtype=torch.float32, device=dev)
         self.boxes = torch.empty((n, 6), dtype=torch.float32, device=dev)
-        _check(lib().gprtcuInstancesPrepare(_ptr(instances), n, _ptr(root_boxes), meshes, _ptr(self.w2o),
-                                            _ptr(self.boxes), _stream()), "gprtcuInstancesPrepare")
-        self.bvh = lbvh_build_boxes(self.boxes)
+        self.bvh = Lbvh(n, dev)
+        self.build()
+
+    def build(self):
+        """Recompute matrices, world boxes and the top-level LBVH in place
+        (after the instance records or the bottom-level boxes changed)."""
+        n = self.instances.shape[0]
+        _check(lib().gprtcuInstancesPrepare(_ptr(self.instances), n, _ptr(self.root_boxes), self.meshes,
+                                            _ptr(self.w2o), _ptr(self.boxes), _stream()), "gprtcuInstancesPrepare")
+        lbvh_build_boxes(self.boxes, self.bvh)
 
 
 def trace_instances(tlas, blas, rays, tri_off=None, meshes=1, ray_mask=0xFF, hits=None, inst=None, anyhit=False,

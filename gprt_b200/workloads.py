@@ -300,3 +300,57 @@ class UserScene:
                 "build_mprims_s": self.n / tb / 1e3, "trace_mrays_s": self.nrays / tt / 1e3,
                 "step_mrays_s": self.nrays / (tb + tt) / 1e3,
                 "hit_fraction": float((self.hits[:, 0] != -1).float().mean().item())}
+
+
+class InstanceScene:
+    """Two-level scene: a batch of `meshes` bottom-level meshes (Gaussian
+    mixture triangles, log-uniform sizes summing to `n`), `instances` placements
+    of them (mesh i mod meshes; random rotation, uniform scale in [0.5, 2],
+    translation uniform in [0, 24]^3; masks cycling 0x01, 0x02, 0x04, 0x08) and
+    nrays rays aimed at the world box as in PlainScene.  A step re-prepares the
+    instances, rebuilds the top-level LBVH and traces every ray (mask 0xFF)."""
+
+    def __init__(self, meshes=64, n=4_194_304, instances=16_384, nrays=16_777_216, seed=11, device="cuda"):
+        dev = torch.device(device)
+        rng = np.random.default_rng(seed)
+        self.meshes, self.n, self.ninst, self.nrays = meshes, n, instances, nrays
+        self.off = np.zeros(meshes + 1, np.int64)
+        self.off[1:] = np.cumsum(large_sizes(meshes, n, seed=seed))
+        self.pos, self.tri = api.gen_mixture(n, clusters=meshes, seed=seed, edge_sigma=0.002, device=dev)
+        self.blas = api.BatchLbvh(self.off, dev, with_aabbs=False)
+        rec = np.zeros(instances, np.dtype(api.INSTANCE_DTYPE))
+        q, _ = np.linalg.qr(rng.normal(size=(instances, 3, 3)))
+        m = np.zeros((instances, 3, 4))
+        m[:, :, :3] = q * rng.uniform(0.5, 2.0, (instances, 1, 1))
+        m[:, :, 3] = rng.uniform(0.0, 24.0, (instances, 3))
+        rec["transform"] = m.reshape(instances, 12)
+        rec["custom_mask"] = ((1 << (np.arange(instances) % 4)) << 24) | np.arange(instances)
+        rec["blas"] = np.arange(instances) % meshes
+        self.records = rec
+        self.instances = api.instances_tensor(rec, dev)
+        self.blas_ms = float(np.mean(time_steps(self.build_blas, 3, 1)))
+        self.tlas = api.Tlas(self.instances, self.blas.root, meshes)
+        b = self.tlas.boxes
+        world = torch.cat([b[:, :3].min(0).values, b[:, 3:].max(0).values]).contiguous()
+        self.rays = api.gen_rays(nrays, seed=seed + 1, boxes=world, device=dev)
+        self.hits = torch.empty((nrays, 2), dtype=torch.int32, device=dev)
+        self.hit_inst = torch.empty(nrays, dtype=torch.int32, device=dev)
+        self.tscr = api.scratch(lib().gprtcuTraceScratchSize(), dev)
+
+    def build_blas(self):
+        api.batch_build_triangles(self.pos, self.tri, self.blas)
+
+    def build_tlas(self):
+        self.tlas.build()
+
+    def trace(self):
+        api.trace_instances(self.tlas, self.blas, self.rays, self.blas.tri_off, self.meshes, 0xFF, self.hits,
+                            self.hit_inst, scr=self.tscr)
+
+    def run(self, steps=3, warmup=1, flush=None):
+        tb = float(np.mean(time_steps(self.build_tlas, steps, warmup, flush)))
+        tt = float(np.mean(time_steps(self.trace, steps, warmup, flush)))
+        return {"meshes": self.meshes, "triangles": self.n, "instances": self.ninst, "rays": self.nrays,
+                "blas_build_ms": self.blas_ms, "tlas_build_ms": tb, "trace_ms": tt,
+                "trace_mrays_s": self.nrays / tt / 1e3, "step_mrays_s": self.nrays / (tb + tt) / 1e3,
+                "hit_fraction": float((self.hits[:, 0] != -1).float().mean().item())}
