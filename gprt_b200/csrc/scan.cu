@@ -10,8 +10,12 @@
 //   * 64-bit status words {flag:32 | value:32}, so the aggregate is not
 //     capped at 2^30 as it is with the reference's 2-bit-flag packing
 //     (gprt/gprt_scan.slang:60-63, gprt/gprt_host.h:2231);
-//   * warp-wide look-back over 32 predecessors per probe, with a bounded
-//     wait that poisons the chain instead of hanging.
+//   * warp-wide look-back over 32 or 128 predecessors per probe, with a
+//     bounded wait that poisons the chain instead of hanging;
+//   * for large aligned inputs, a persistent warp-specialised kernel
+//     (k_scan_reread) that publishes each tile's aggregate as soon as the
+//     tile lands and reads the tile a second time, from L2, once its prefix
+//     is known, so no tile holds shared memory while it waits.
 // Traffic: 4 B read + 4 B written per element; HBM-bound.
 #include "common.cuh"
 
@@ -352,6 +356,266 @@ __global__ void __launch_bounds__(WARPS * 32) k_scan_tma(const uint32_t *in, uin
   }
 }
 
+// Persistent scan that reads each tile twice: once from HBM to publish its
+// aggregate, once more (from L2) after its look-back has resolved.
+//
+// In the tile-per-CTA kernels a tile holds its 32 KB of shared memory from
+// the moment its load is issued until its store has read it, and most of that
+// time is look-back: the tile waits for the slowest load among its
+// predecessors, and HBM load latency has a long tail under full load (B200,
+// 2^30 elements: median 3 us, p99 9 us; look-back 8 us of a 14 us tile life).
+// Shared memory per SM then caps the loads in flight below what the HBM
+// needs.  Here a tile holds no shared memory while it waits:
+//   warp 0   producer: takes a ticket and loads the tile into one of RS
+//            "reduce" stages (bulk copy, L2 evict_last);
+//   warp 1   reducer: sums the tile (one partial per scanner warp), frees the
+//            stage, publishes the aggregate at once, and queues {tile,
+//            partials} in one of PQ pending slots;
+//   warps 2,3 look-back (even / odd pending slots): resolve the tile's
+//            exclusive prefix, publish the inclusive value, then load the
+//            tile again into one of SS "scan" stages (L2 evict_first) — it
+//            was read microseconds ago and is still in L2;
+//   warps 4..11 scanners: eight rows of 128 elements each, scanned with all
+//            eight rows' shuffles interleaved, then one bulk store (L2
+//            evict_first).
+// HBM traffic stays 4 B read + 4 B written per element; the second read is
+// L2 traffic.  Stages hand over through mbarriers: r_full/r_empty (producer
+// <-> reducer), p_full/p_empty (reducer -> look-back -> scanners -> reducer),
+// s_full/s_empty (look-back <-> scanners).  Progress: a tile's aggregate is
+// published before its reducer can block, and every wait is on an earlier
+// iteration of this CTA or on a smaller ticket, so the smallest unfinished
+// tile can always advance.  Every wait is bounded; a wait that gives up
+// records GPRTCU_ERR_TIMEOUT and the warp leaves its loop.
+constexpr int RR_SCAN_WARPS = 8;
+constexpr int RR_THREADS = (4 + RR_SCAN_WARPS) * 32;
+constexpr int RR_RS = 3, RR_SS = 4, RR_PQ = 8;
+constexpr size_t RR_SMEM = (size_t)(RR_RS + RR_SS) * SCAN_TILE * 4;
+constexpr uint32_t RR_END = 0xFFFFFFFFu;
+struct RrPending {
+  uint32_t tile, prefix, part[RR_SCAN_WARPS];
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *in, uint32_t *out, uint64_t n,
+                                                               uint64_t ntiles, ScratchHeader *hdr, uint64_t *status,
+                                                               uint32_t *d_total, uint32_t budget, int64_t skip_tile) {
+  constexpr int RS = RR_RS, SS = RR_SS, PQ = RR_PQ, SW = RR_SCAN_WARPS;
+  constexpr uint32_t TILE = SCAN_TILE, TB = SCAN_TILE * 4;
+  static_assert(PQ % 2 == 0, "pending slot q always belongs to look-back warp q % 2");
+  static_assert(SS >= 3, "a scan stage is released one iteration late; the end marker needs two more");
+  static_assert(TILE == SW * 8 * 128, "each scanner warp owns 8 rows of 128 elements");
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ uint64_t r_full[RS], r_empty[RS], p_full[PQ], p_empty[PQ], s_full[SS], s_empty[SS];
+  __shared__ RrPending pend[PQ];
+  __shared__ uint32_t r_tile[RS], s_tile[SS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  unsigned char *rbuf = smem, *sbuf = smem + (size_t)RS * TB;
+  if (tid == 0) {
+    for (int i = 0; i < RS; ++i) {
+      mbar_init(&r_full[i], 32);
+      mbar_init(&r_empty[i], 1);
+    }
+    for (int i = 0; i < PQ; ++i) {
+      mbar_init(&p_full[i], 1);
+      mbar_init(&p_empty[i], 1);
+    }
+    for (int i = 0; i < SS; ++i) {
+      mbar_init(&s_full[i], 32);
+      mbar_init(&s_empty[i], 1);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+  // Bring tile t into a stage: bulk copy of its whole-uint4 part, plain loads
+  // and zeros for the rest of a partial last tile.  All 32 lanes arrive.
+  auto load_tile = [&](uint32_t *sb, uint32_t t, uint64_t *bar, uint64_t pol) {
+    const uint64_t base = (uint64_t)t * TILE;
+    const uint64_t r = n - base < (uint64_t)TILE ? n - base : (uint64_t)TILE;
+    const uint32_t a = (uint32_t)(r & ~3ull);
+    if (r < (uint64_t)TILE)
+      for (uint32_t k = a + lane; k < TILE; k += 32) sb[k] = k < r ? in[base + k] : 0u;
+    if (lane == 0 && a) {
+      mbar_arrive_expect_tx(bar, a * 4);
+      bulk_g2s_hint(sb, in + base, a * 4, bar, pol);
+    } else {
+      mbar_arrive(bar);
+    }
+  };
+  if (warp == 0) {
+    const uint64_t pol = l2_policy_evict_last();
+    for (uint32_t i = 0;; ++i) {
+      const int s = i % RS;
+      if (i >= RS && !mbar_wait(&r_empty[s], ((i / RS) - 1) & 1, MBAR_WAIT_BUDGET)) break;
+      uint32_t t = 0;
+      if (lane == 0) t = atomicAdd(&hdr->ticket[0], 1u);
+      t = __shfl_sync(FULL_MASK, t, 0);
+      if (lane == 0) r_tile[s] = t < ntiles ? t : RR_END;
+      if (t >= ntiles) {
+        mbar_arrive(&r_full[s]);
+        return;
+      }
+      load_tile(reinterpret_cast<uint32_t *>(rbuf + (size_t)s * TB), t, &r_full[s], pol);
+    }
+  } else if (warp == 1) {
+    for (uint32_t i = 0;; ++i) {
+      const int s = i % RS, q = i % PQ;
+      if (!mbar_wait(&r_full[s], (i / RS) & 1, MBAR_WAIT_BUDGET)) break;
+      const uint32_t t = r_tile[s];
+      if (t == RR_END) {
+        for (uint32_t j = i; j < i + 2; ++j) {  // one end marker for each look-back warp
+          const int qj = j % PQ;
+          if (j >= PQ && !mbar_wait(&p_empty[qj], ((j / PQ) - 1) & 1, MBAR_WAIT_BUDGET)) {
+            if (lane == 0) record_error(hdr, GPRTCU_ERR_TIMEOUT);
+            return;
+          }
+          if (lane == 0) {
+            pend[qj].tile = RR_END;
+            mbar_arrive(&p_full[qj]);
+          }
+        }
+        return;
+      }
+      const uint4 *b = reinterpret_cast<const uint4 *>(rbuf + (size_t)s * TB);
+      uint32_t part[SW];
+#pragma unroll
+      for (int w = 0; w < SW; ++w) {
+        uint32_t p = 0;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const uint4 v = b[(w * 8 + r) * 32 + lane];
+          p += (v.x + v.y) + (v.z + v.w);
+        }
+        part[w] = p;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int w = 0; w < SW; ++w) part[w] += __shfl_xor_sync(FULL_MASK, part[w], o);
+      __syncwarp();
+      uint32_t agg = 0;
+#pragma unroll
+      for (int w = 0; w < SW; ++w) agg += part[w];
+      if (lane == 0) {
+        mbar_arrive(&r_empty[s]);
+        if ((int64_t)t != skip_tile) st_relaxed_u64(&status[t], (t == 0 ? ST_INC : ST_AGG) | agg);
+      }
+      if (i >= PQ && !mbar_wait(&p_empty[q], ((i / PQ) - 1) & 1, MBAR_WAIT_BUDGET)) break;
+      if (lane == 0) {
+        pend[q].tile = t;
+#pragma unroll
+        for (int w = 0; w < SW; ++w) pend[q].part[w] = part[w];
+        mbar_arrive(&p_full[q]);
+      }
+    }
+  } else if (warp < 4) {
+    const uint64_t pol = l2_policy_evict_first();
+    for (uint32_t i = warp - 2;; i += 2) {
+      const int q = i % PQ, ss = i % SS;
+      if (!mbar_wait(&p_full[q], (i / PQ) & 1, MBAR_WAIT_BUDGET)) break;
+      const uint32_t t = pend[q].tile;
+      uint32_t excl = 0;
+      if (t != RR_END) {
+        uint32_t agg = 0;
+#pragma unroll
+        for (int w = 0; w < SW; ++w) agg += pend[q].part[w];
+        bool ok = true;
+        if ((int64_t)t == skip_tile) {
+          ok = false;  // fault injection: this tile never publishes
+        } else if (t > 0) {
+          ok = scan_lookback128(status, t, lane, budget, excl);
+          if (lane == 0) st_relaxed_u64(&status[t], ok ? (ST_INC | (uint32_t)(excl + agg)) : ST_POISON);
+        }
+        if (!ok && lane == 0) record_error(hdr, GPRTCU_ERR_TIMEOUT);
+        if (lane == 0 && t == ntiles - 1) {
+          hdr->total = excl + agg;
+          if (d_total) *d_total = excl + agg;
+        }
+      }
+      if (i >= SS && !mbar_wait(&s_empty[ss], ((i / SS) - 1) & 1, MBAR_WAIT_BUDGET)) break;
+      if (lane == 0) {
+        s_tile[ss] = t;
+        if (t != RR_END) pend[q].prefix = excl;
+      }
+      if (t == RR_END) {
+        mbar_arrive(&s_full[ss]);
+        return;
+      }
+      load_tile(reinterpret_cast<uint32_t *>(sbuf + (size_t)ss * TB), t, &s_full[ss], pol);
+    }
+  } else {
+    const int w = warp - 4;
+    const bool leader = tid == 4 * 32;
+    const uint64_t pol = l2_policy_evict_first();
+    int prev = -1;
+    for (uint32_t i = 0;; ++i) {
+      const int ss = i % SS, q = i % PQ;
+      if (!mbar_wait(&s_full[ss], (i / SS) & 1, MBAR_WAIT_BUDGET)) {
+        if (leader) record_error(hdr, GPRTCU_ERR_TIMEOUT);
+        break;
+      }
+      const uint32_t t = s_tile[ss];
+      if (t == RR_END) break;
+      uint32_t carry = pend[q].prefix;
+      for (int k = 0; k < w; ++k) carry += pend[q].part[k];
+      uint4 *wb = reinterpret_cast<uint4 *>(sbuf + (size_t)ss * TB) + w * 8 * 32;
+      uint4 v[8];
+      uint32_t sum[8], inc[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        v[r] = wb[r * 32 + lane];
+        sum[r] = (v[r].x + v[r].y) + (v[r].z + v[r].w);
+        inc[r] = sum[r];
+      }
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1)
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const uint32_t y = __shfl_up_sync(FULL_MASK, inc[r], o);
+          if (lane >= o) inc[r] += y;
+        }
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const uint32_t p = carry + inc[r] - sum[r];
+        uint4 o;
+        if (MODE == 0) {
+          o.x = p;
+          o.y = o.x + v[r].x;
+          o.z = o.y + v[r].y;
+          o.w = o.z + v[r].z;
+        } else {
+          o.x = p + v[r].x;
+          o.y = o.x + v[r].y;
+          o.z = o.y + v[r].z;
+          o.w = o.z + v[r].w;
+        }
+        wb[r * 32 + lane] = o;
+        carry += __shfl_sync(FULL_MASK, inc[r], 31);
+      }
+      fence_proxy_async_smem();
+      named_bar_sync(1, SW * 32);
+      const uint64_t base = (uint64_t)t * TILE;
+      const uint64_t r = n - base < (uint64_t)TILE ? n - base : (uint64_t)TILE;
+      const uint32_t a = (uint32_t)(r & ~3ull);
+      const uint32_t *sb = reinterpret_cast<const uint32_t *>(sbuf + (size_t)ss * TB);
+      if (r < (uint64_t)TILE) {
+        for (uint32_t k = a + (tid - 4 * 32); k < r; k += SW * 32) out[base + k] = sb[k];
+        named_bar_sync(1, SW * 32);
+      }
+      if (leader) {
+        mbar_arrive(&p_empty[q]);
+        if (a) bulk_s2g_hint(out + base, sb, a * 4, pol);
+        bulk_commit();
+        bulk_wait_read<1>();  // the previous tile's store has read its stage
+        if (prev >= 0) mbar_arrive(&s_empty[prev]);
+      }
+      prev = ss;
+    }
+    if (leader) bulk_wait<0>();
+    return;
+  }
+  if (lane == 0) record_error(hdr, GPRTCU_ERR_TIMEOUT);  // a wait above gave up
+}
+
 
 // Partition / select by sign (gprt/gprt_scan.slang:118-133,270-283;
 // known-answer layout tests/t03-bufferScans/hostCode.cpp:98-160,172-241).
@@ -485,8 +749,14 @@ using namespace gprtcu;
 
 static uint32_t g_spin_budget = DEFAULT_SPIN_BUDGET;
 static int64_t g_skip_tile = -1;
-// 0: TMA-staged tile-per-CTA scan when aligned; 1: register tile-per-CTA scan.
+// 0: automatic; 1: register tile per CTA; 2: TMA-staged tile per CTA;
+// 3: persistent re-read kernel.  1-3 are test overrides (2 and 3 need
+// 16-byte aligned in/out, else 1 runs).
 static int g_scan_impl = 0;
+// From this size up the persistent re-read kernel is the faster one (B200:
+// 2^20 elements 12 vs 16 us, 2^30 1.50 vs 2.34 ms); below it the
+// tile-per-CTA kernel needs no 224 KB CTAs.
+static const uint64_t kRereadMinN = 1ull << 20;
 extern "C" GPRTCU_API void gprtcuDebugScanImpl(int impl) { g_scan_impl = impl; }
 
 
@@ -499,6 +769,29 @@ static const uint64_t kScanMaxN = 1ull << 40;
 extern "C" GPRTCU_API size_t gprtcuScanScratchSize(uint64_t n) {
   uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
   return sizeof(ScratchHeader) + gprtcu_align256(tiles * sizeof(uint64_t));
+}
+
+// CTAs of the re-read kernel that fit on the device at once (one per SM on
+// B200); 0 if it does not fit.  Sets the shared-memory attribute once per device.
+static int reread_ctas() {
+  static int cached[64];
+  static bool done[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+  if (!done[dev]) {
+    int occ = 0;
+    if (cudaFuncSetAttribute(k_scan_reread<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RR_SMEM) ==
+            cudaSuccess &&
+        cudaFuncSetAttribute(k_scan_reread<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RR_SMEM) ==
+            cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_scan_reread<0>, RR_THREADS, RR_SMEM) == cudaSuccess)
+      cached[dev] = occ * gprtcu_num_sms();
+    else
+      cached[dev] = 0;
+    cudaGetLastError();
+    done[dev] = true;
+  }
+  return cached[dev];
 }
 
 template <int THREADS, int VECS, int LBW>
@@ -531,9 +824,13 @@ static gprtcuStatus scan_launch(const uint32_t *in, uint32_t *out, uint64_t n, i
   uint64_t *status = (uint64_t *)((char *)scratch + sizeof(ScratchHeader));
   const bool vec = (((uintptr_t)in | (uintptr_t)out) & 15) == 0;
   const bool nc = (const void *)in != (const void *)out;
-  // Kernel choice: impl 0 = TMA-staged 8192-element tiles (aligned buffers),
-  // impl 1 = register-staged 8192-element tiles (any alignment).
-  const int impl = vec ? g_scan_impl : 1;
+  // Kernel choice (all on 8192-element tiles): the persistent re-read kernel
+  // for large aligned buffers, the TMA-staged tile-per-CTA kernel for smaller
+  // aligned ones, the register-staged kernel for any alignment.
+  int impl = vec ? g_scan_impl : 1;
+  if (impl == 0) impl = n >= kRereadMinN ? 3 : 2;
+  const int rr_ctas = impl == 3 ? reread_ctas() : 0;
+  if (impl == 3 && rr_ctas == 0) impl = 2;
   const uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
   if (scratch_bytes < sizeof(ScratchHeader) + tiles * sizeof(uint64_t)) return GPRTCU_ERR_SCRATCH_TOO_SMALL;
   GPRTCU_TRY(cudaMemsetAsync(scratch, 0, sizeof(ScratchHeader) + tiles * sizeof(uint64_t), stream));
@@ -541,7 +838,15 @@ static gprtcuStatus scan_launch(const uint32_t *in, uint32_t *out, uint64_t n, i
     if (d_total) GPRTCU_TRY(cudaMemsetAsync(d_total, 0, sizeof(uint32_t), stream));
     return GPRTCU_OK;
   }
-  if (impl == 0) {
+  if (impl == 3) {
+    const unsigned grid = (unsigned)(tiles < (uint64_t)rr_ctas ? tiles : (uint64_t)rr_ctas);
+    if (inclusive)
+      k_scan_reread<1><<<grid, RR_THREADS, RR_SMEM, stream>>>(in, out, n, tiles, hdr, status, d_total, g_spin_budget,
+                                                             g_skip_tile);
+    else
+      k_scan_reread<0><<<grid, RR_THREADS, RR_SMEM, stream>>>(in, out, n, tiles, hdr, status, d_total, g_spin_budget,
+                                                             g_skip_tile);
+  } else if (impl == 2) {
     // TMA-staged tile-per-CTA kernel (32 KB dynamic shared memory per CTA).
     if (inclusive)
       k_scan_tma<1><<<(unsigned)tiles, TS_THREADS, TS_SMEM, stream>>>(in, out, n, tiles, hdr, status, d_total,

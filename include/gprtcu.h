@@ -397,8 +397,11 @@ GPRTCU_API gprtcuStatus gprtcuGenRays(uint64_t numRays, uint64_t seed, const uin
  * ------------------------------------------------------------------------ */
 GPRTCU_API void gprtcuDebugSetSpinBudget(uint32_t polls);
 GPRTCU_API void gprtcuDebugScanSkipTile(int64_t tile);
-/* Scan kernel selection for tests: 0 = TMA-staged tile-per-CTA kernel when
- * in/out are 16-byte aligned (default), 1 = register-staged tile per CTA. */
+/* Scan kernel selection for tests: 0 = automatic (default: the persistent
+ * re-read kernel for n >= 2^20 and the TMA-staged tile-per-CTA kernel below,
+ * when in/out are 16-byte aligned; else the register-staged kernel),
+ * 1 = register-staged tile per CTA, 2 = TMA-staged tile per CTA,
+ * 3 = persistent re-read kernel (2 and 3 need 16-byte aligned in/out). */
 GPRTCU_API void gprtcuDebugScanImpl(int impl);
 
 #ifdef __cplusplus

@@ -22,7 +22,7 @@ def _run_scan(torch, x, inclusive=False, alias=False, offset=0):
     return out.cpu().numpy().view(np.uint32), int(total.cpu().numpy().view(np.uint32)[0])
 
 
-@pytest.fixture(params=[0, 1], ids=["tma_staged", "register_staged"])
+@pytest.fixture(params=[0, 1, 2, 3], ids=["automatic", "register_staged", "tma_staged", "persistent_reread"])
 def scan_impl(request, cuda):
     import gprt_b200
     gprt_b200.lib().gprtcuDebugScanImpl(request.param)
