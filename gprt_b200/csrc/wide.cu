@@ -14,7 +14,8 @@
 //   leaf_base  first leaf child's index in the wide leaf array (contiguous)
 //   meta[c]    0xFF empty; else the child's rank among the inner (imask) or
 //              leaf children
-//   qlo/qhi    per axis, per child: floor((lo - p) / s), ceil((hi - p) / s)
+//   qlo/qhi    per axis, per child: floor((lo - p) / s), ceil((hi - p) / s);
+//              an empty slot holds the inverted box qlo 255, qhi 0
 // Decoding uses round-down (lo) and round-up (hi) FMAs, so every decoded box
 // contains its exact fp32 child box; a ray therefore never misses a child the
 // binary traversal would enter, and intersection is the same FP32 watertight
@@ -194,9 +195,10 @@ __global__ void __launch_bounds__(128) k_wide_level(const Bvh2Node *bvh2, const 
     int ri = 0, rl = 0;
     for (int c = 0; c < 8; ++c) {
       if (c >= cnt) {
+        // absent child: an inverted box (lo 255, hi 0) that fails the slab test
         w.meta[c] = 0xFF;
         for (int k = 0; k < 3; ++k) {
-          w.qlo[k][c] = 0;
+          w.qlo[k][c] = 255;
           w.qhi[k][c] = 0;
         }
         continue;
@@ -251,6 +253,47 @@ constexpr int kWideRefill = 8;
 
 __device__ __forceinline__ float scale_of(int8_t e) { return __int_as_float(((int)e + 127) << 23); }
 
+// Packed pairs of fp32 (sm_100 f32x2 arithmetic; each half rounds as the
+// scalar instruction would) and three-input min / max.
+__device__ __forceinline__ unsigned long long pk2(float a, float b) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void up2(unsigned long long v, float &a, float &b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long fma2_rd(unsigned long long a, unsigned long long b, unsigned long long c) {
+  unsigned long long r;
+  asm("fma.rm.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+__device__ __forceinline__ unsigned long long fma2_ru(unsigned long long a, unsigned long long b, unsigned long long c) {
+  unsigned long long r;
+  asm("fma.rp.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+__device__ __forceinline__ unsigned long long add2_rn(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long mul2_rn(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+
 __device__ __forceinline__ void wide_leaf_test(const float4 *leaf, uint32_t i, const Ray &R, uint32_t &best,
                                                uint32_t &best_leaf, float &bt) {
   const float4 a = __ldg(leaf + 3 * (size_t)i), b = __ldg(leaf + 3 * (size_t)i + 1), c = __ldg(leaf + 3 * (size_t)i + 2);
@@ -265,19 +308,27 @@ __device__ __forceinline__ void wide_leaf_test(const float4 *leaf, uint32_t i, c
 }
 
 // One lane per ray.  Per node: the ray is moved into the node's quantised
-// frame once, the eight child boxes are tested, and only then are the hit
-// leaf children's triangles tested (the lanes with leaf hits run those tests
+// frame once, the eight child boxes are tested two at a time with packed
+// f32x2 arithmetic (byte decode, directed-rounding slab FMAs, the 2^-18
+// widening) and three-input min/max, and only then are the hit leaf
+// children's triangles tested (the lanes with leaf hits run those tests
 // together, whatever slots they are in; testing them inside the child loop
-// ran each slot's test separately with few lanes active).  The nearest hit
-// inner child is entered and the others are pushed as one entry {child_base,
-// mask of inner-child ranks}.  Lanes are refilled as their rays finish: when
-// at least kWideRefill lanes of a warp are idle, the warp takes that many
-// new rays from the global counter (waiting for the whole warp to finish left
-// most lanes idle behind the longest ray).  On 16.7M rays of one 16.7M-
-// triangle mesh and on 134M rays over 16,384 meshes, thresholds of 4, 8, 16
-// and 32 (no refill) idle lanes measured 33.6 / 34.7 / 38.5 / 63.7 ms and
-// 71.3 / 69.0 / 74.8 / 155.5 ms; testing leaf triangles inside the child loop
-// instead measured 174.7 ms on the second.
+// ran each slot's test separately with few lanes active).  Absent children
+// are inverted boxes and need no test of their own.  The nearest hit inner
+// child is found inside the box loop and entered; the other hit inner
+// children are pushed as one entry {child_base, slot mask | inner mask << 8}
+// and a popped slot's node is child_base + the inner children below it.
+// Lanes are refilled as their rays finish: when at least kWideRefill lanes of
+// a warp are idle, the warp takes that many new rays from the global counter
+// (waiting for the whole warp to finish left most lanes idle behind the
+// longest ray).  On 16.7M rays of one 16.7M-triangle mesh and on 134M rays
+// over 16,384 meshes, thresholds of 4, 8, 16 and 32 (no refill) idle lanes
+// measured 33.6 / 34.7 / 38.5 / 63.7 ms and 71.3 / 69.0 / 74.8 / 155.5 ms;
+// testing leaf triangles inside the child loop instead measured 174.7 ms on
+// the second.  The packed box loop took the second from 68.7 to 59.2 ms.
+// Keeping a lane's leaf tests pending across nodes until enough lanes had
+// some measured 76.4 ms: lanes finishing with tests pending forced most
+// flushes, and the extra state spilled.
 template <bool ANY, bool BATCHED>
 __global__ void __launch_bounds__(kWideThreads, 8)
     k_trace_wide(const WideNode *nodes, const float4 *leaf, const uint32_t *roots, const uint32_t *ray_off,
@@ -359,74 +410,100 @@ __global__ void __launch_bounds__(kWideThreads, 8)
       }
     }
     float ctn[8];
-    uint32_t inner_hit = 0, leaf_hit = 0;  // slot bits
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      const uint32_t meta = ((c < 4 ? meta_lo : meta_hi) >> (8 * (c & 3))) & 0xFF;
-      ctn[c] = 0.0f;
-      if (meta == 0xFF) continue;
-      const int h = c >> 2;
-      const uint32_t sel = 0x7540u | (uint32_t)(c & 3);
-      float tn = R.tmin, tf = bt;
+    uint32_t hm = 0;  // slots whose box is hit
+    float nt = __int_as_float(0x7f800000);
+    int ns = -1;  // nearest hit inner slot
+    {
+      const unsigned long long bias = pk2(-8388608.0f, -8388608.0f);
+      const unsigned long long lo2 = pk2(kBoxLo, kBoxLo), hi2 = pk2(kBoxHi, kBoxHi);
+      unsigned long long B2[3], N2[3], F2[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        const float fn = __fsub_rn(__uint_as_float(__byte_perm(qn[a][h], 0x4B000000u, sel)), 8388608.0f);
-        const float ff = __fsub_rn(__uint_as_float(__byte_perm(qf[a][h], 0x4B000000u, sel)), 8388608.0f);
-        tn = fmaxf(tn, __fmaf_rd(fn, Bq[a], An[a]));
-        tf = fminf(tf, __fmaf_ru(ff, Bq[a], Af[a]));
+        B2[a] = pk2(Bq[a], Bq[a]);
+        N2[a] = pk2(An[a], An[a]);
+        F2[a] = pk2(Af[a], Af[a]);
       }
-      tn = __fmul_rn(tn, kBoxLo);
-      tf = __fmul_rn(tf, kBoxHi);
-      if (tn <= tf && tn <= bt) {
-        if ((imask >> c) & 1u) {
-          inner_hit |= 1u << c;
-          ctn[c] = tn;
-        } else {
-          leaf_hit |= 1u << c;
+#pragma unroll
+      for (int cp = 0; cp < 4; ++cp) {
+        const int h = cp >> 1;
+        const uint32_t s0 = 0x7540u | (uint32_t)((2 * cp) & 3), s1 = 0x7540u | (uint32_t)((2 * cp + 1) & 3);
+        float n[2][3], f[2][3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const unsigned long long qn2 = pk2(__uint_as_float(__byte_perm(qn[a][h], 0x4B000000u, s0)),
+                                             __uint_as_float(__byte_perm(qn[a][h], 0x4B000000u, s1)));
+          const unsigned long long qf2 = pk2(__uint_as_float(__byte_perm(qf[a][h], 0x4B000000u, s0)),
+                                             __uint_as_float(__byte_perm(qf[a][h], 0x4B000000u, s1)));
+          up2(fma2_rd(add2_rn(qn2, bias), B2[a], N2[a]), n[0][a], n[1][a]);
+          up2(fma2_ru(add2_rn(qf2, bias), B2[a], F2[a]), f[0][a], f[1][a]);
+        }
+        float tn[2], tf[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          tn[k] = fmaxf(max3f(n[k][0], n[k][1], n[k][2]), R.tmin);
+          tf[k] = fminf(min3f(f[k][0], f[k][1], f[k][2]), bt);
+        }
+        up2(mul2_rn(pk2(tn[0], tn[1]), lo2), tn[0], tn[1]);
+        up2(mul2_rn(pk2(tf[0], tf[1]), hi2), tf[0], tf[1]);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const int c = 2 * cp + k;
+          ctn[c] = tn[k];
+          const bool hit = tn[k] <= tf[k] && tn[k] <= bt;
+          hm |= (uint32_t)hit << c;
+          if (hit && ((imask >> c) & 1u) && tn[k] < nt) {
+            nt = tn[k];
+            ns = c;
+          }
         }
       }
     }
+    const uint32_t inner_hit = hm & imask;
+    uint32_t leaf_hit = hm & ~imask;
+    const float bt_before = bt;
     // deferred triangle tests: lanes with leaf hits run them together
     while (leaf_hit) {
       const int c = __ffs(leaf_hit) - 1;
       leaf_hit &= leaf_hit - 1u;
       const uint32_t meta = ((c < 4 ? meta_lo : meta_hi) >> (8 * (c & 3))) & 0xFF;
-      wide_leaf_test(leaf, leaf_base + meta, R, best, best_leaf, bt);
+      if (meta != 0xFF) wide_leaf_test(leaf, leaf_base + meta, R, best, best_leaf, bt);
     }
     bool finished = false;
     if (ANY && best != kMiss) {
       finished = true;
     } else {
-      int nearest = -1;
-      float nt = 0.0f;
-      uint32_t rest = 0;  // inner-child ranks
+      uint32_t rest = inner_hit;  // inner slots still to visit
+      if (bt < bt_before) {
+        // a triangle of this node moved the best distance: drop the inner
+        // children now behind it and pick the nearest again
+        ns = -1;
 #pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        if (!((inner_hit >> c) & 1u) || ctn[c] > bt) continue;
-        const uint32_t rank = ((c < 4 ? meta_lo : meta_hi) >> (8 * (c & 3))) & 0xFF;
-        rest |= 1u << rank;
-        if (nearest < 0 || ctn[c] < nt) {
-          nearest = (int)rank;
-          nt = ctn[c];
-        }
+        for (int c = 0; c < 8; ++c)
+          if (((rest >> c) & 1u) && ctn[c] > bt) rest &= ~(1u << c);
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (((rest >> c) & 1u) && (ns < 0 || ctn[c] < nt)) {
+            ns = c;
+            nt = ctn[c];
+          }
       }
-      if (nearest >= 0) {
-        rest &= ~(1u << nearest);
+      if (ns >= 0) {
+        rest &= ~(1u << ns);
         if (rest) {
           if (sp < kWideStack) {
-            stack[sp++] = make_uint2(child_base, rest);
+            stack[sp++] = make_uint2(child_base, rest | (imask << 8));
           } else {
             atomicCAS(err, 0u, 5u);  // traversal stack overflow
             finished = true;
           }
         }
-        node = child_base + (uint32_t)nearest;
+        node = child_base + (uint32_t)__popc(imask & ((1u << ns) - 1u));
       } else if (sp > 0) {
         uint2 &top = stack[sp - 1];
-        const uint32_t rr = __ffs(top.y) - 1;
-        top.y &= top.y - 1;
-        node = top.x + rr;
-        if (top.y == 0) --sp;
+        const uint32_t c = __ffs(top.y & 0xFFu) - 1;
+        top.y &= ~(1u << c);
+        node = top.x + (uint32_t)__popc((top.y >> 8) & ((1u << c) - 1u));
+        if ((top.y & 0xFFu) == 0) --sp;
       } else {
         finished = true;
       }

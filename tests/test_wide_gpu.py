@@ -118,3 +118,54 @@ def test_wide_batched_equals_batched_binary(cuda):
             hit = gw["prim"] != 0xFFFFFFFF
             assert hit.sum() > 1000
             assert np.array_equal(_bits(gw["t"][hit]), _bits(gb["t"][hit]))
+
+
+def _axis_rays(pos, m, seed):
+    """Rays with one or two zero direction components: along +-x/y/z from
+    outside the unit cube, some with origin coordinates equal to vertex
+    coordinates (rays in vertex / edge planes), and diagonal rays in the
+    coordinate planes."""
+    rng = np.random.default_rng(seed)
+    r = np.zeros((m, 8), np.float32)
+    r[:, 7] = np.inf
+    for i in range(m):
+        kind = i % 4
+        a = rng.integers(0, 3)
+        o = rng.random(3).astype(np.float32)
+        if kind == 1:  # origin on a vertex's coordinates
+            v = pos[rng.integers(0, len(pos))]
+            o = v.copy()
+        d = np.zeros(3, np.float32)
+        if kind < 3:
+            sgn = 1.0 if rng.random() < 0.5 else -1.0
+            d[a] = sgn
+            o[a] = -1.0 if sgn > 0 else 2.0
+        else:
+            b = (a + 1) % 3
+            d[a], d[b] = 0.70710677, -0.70710677 if rng.random() < 0.5 else 0.70710677
+            o[a] = -1.0
+            o[b] = 2.0 if d[b] < 0 else -1.0
+        r[i, :3], r[i, 4:7] = o, d
+    return r
+
+
+@pytest.mark.parametrize("anyhit", [False, True])
+def test_wide_trace_axis_parallel_rays(cuda, anyhit):
+    import torch
+    from gprt_b200 import api
+    pos, tri = scenes.soup(3000, seed=81, sigma=0.05)
+    rays = _axis_rays(pos, 8000, 82)
+    rt = torch.from_numpy(rays).cuda()
+    b = api.lbvh_build_triangles(torch.from_numpy(pos).cuda(), torch.from_numpy(tri.view(np.int32)).cuda())
+    w = api.wide_build(b)
+    gb = api.hits_numpy(api.trace(b, rt, anyhit=anyhit))
+    gw = api.hits_numpy(api.wide_trace(w, rt, anyhit=anyhit))
+    if anyhit:
+        assert np.array_equal(gw["prim"] != 0xFFFFFFFF, gb["prim"] != 0xFFFFFFFF)
+    else:
+        exp = oracle.trace_brute(pos, tri, rays)
+        assert np.array_equal(gw["prim"], exp["prim"])
+        assert np.array_equal(gw["prim"], gb["prim"])
+        hit = gw["prim"] != 0xFFFFFFFF
+        assert hit.sum() > 500
+        assert np.array_equal(_bits(gw["t"][hit]), _bits(gb["t"][hit]))
