@@ -67,7 +67,7 @@ WORKLOAD = ("large combined, batched + quantised: {tris:,} fp32 triangles in {me
 # DRAM bytes (read + write) of one k_trace_wide launch on the default large
 # workload, from the one-pass ncu capture summarised in
 # profiles/k_trace_wide_large.md; reported only for that workload.
-TRACE_WIDE_DRAM_BYTES = 9_045_743_000 + 1_101_867_000
+TRACE_WIDE_DRAM_BYTES = 9_071_616_000 + 1_104_399_000
 
 
 def measured_peaks():
