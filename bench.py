@@ -39,7 +39,9 @@ The JSON line's value is whole-job Mrays/s of that step.  It also carries:
                 16,777,216 rays
   sort, scan    268,435,456 Zipf(1.1) uint32 key/payload pairs and a
                 1,073,741,824-element uint32 exclusive sum, GB/s of
-                algorithmic traffic against the measured HBM bandwidth
+                algorithmic traffic against the measured HBM bandwidth; beside
+                each, the CPU oracle (std::stable_sort, serial exclusive sum,
+                one thread) on a bounded sample of the same data
   clocks        SM clock samples taken during the timed region
 Multi-GPU (torchrun): every rank builds and traces its own scene (weak
 scaling, no data-path collective); time = max over ranks.
@@ -147,7 +149,10 @@ def zipf_keys(n, seed, s=1.1):
     return (r - 1).to(torch.int64).to(torch.int32)  # wraps to the uint32 bit pattern
 
 
-def sortscan(args, dev, peak, rank):
+def sortscan(args, dev, peak, rank, cpu=False):
+    """Sort and scan extras; with cpu, the oracle's single-thread C++ sort
+    (std::stable_sort on (key, payload), the reference test's own oracle) and
+    serial exclusive sum timed beside them on bounded samples of the same data."""
     import torch
 
     from gprt_b200 import api
@@ -178,6 +183,17 @@ def sortscan(args, dev, peak, rank):
                    "mkeys_s": SORT_N / (t * 1e-3) / 1e6, "gbs": alg * SORT_N / (t * 1e-3) / 1e9,
                    "frac_of_hbm": alg * SORT_N / (t * 1e-3) / 1e9 / peak, "sorted": ok,
                    "gpu_launches_per_call": 6}
+    if cpu:
+        import oracle
+        m = 1 << 24
+        kh = k0[:m].cpu().numpy().view(np.uint32).copy()
+        vh = np.arange(m, dtype=np.uint32)
+        t0 = time.perf_counter()
+        oracle.lib().orc_sort(kh.ctypes.data, 4, vh.ctypes.data, 4, m)
+        dt = time.perf_counter() - t0
+        out["sort"]["cpu_baseline"] = {"value": m / dt / 1e6, "unit": "Mkeys/s", "cores": 1, "kind": "port",
+                                       "sample": "first %d of the same Zipf pairs: std::stable_sort of (key, payload)"
+                                                 % m, "ms": dt * 1e3}
     del k0, v0, k, v, scr
     torch.cuda.empty_cache()
     x = torch.randint(0, 256, (SCAN_N,), dtype=torch.int32, device=dev)
@@ -198,6 +214,18 @@ def sortscan(args, dev, peak, rank):
     out["scan"] = {"n": SCAN_N, "values": "uniform [0,255] uint32", "ms": t, "gbs": 8 * SCAN_N / (t * 1e-3) / 1e9,
                    "frac_of_hbm": 8 * SCAN_N / (t * 1e-3) / 1e9 / peak,
                    "total_ok": int(tot.item()) & 0xFFFFFFFF == int(x.sum().item()) & 0xFFFFFFFF}
+    if cpu:
+        import oracle
+        m = 1 << 28
+        xh = x[:m].cpu().numpy().view(np.uint32).copy()
+        oh = np.empty_like(xh)
+        t0 = time.perf_counter()
+        oracle.lib().orc_scan_u32(xh.ctypes.data, oh.ctypes.data, m, 0)
+        dt = time.perf_counter() - t0
+        out["scan"]["cpu_baseline"] = {"value": 8 * m / dt / 1e9, "unit": "GB/s", "cores": 1, "kind": "port",
+                                       "sample": "first %d of the same values: serial exclusive sum" % m,
+                                       "ms": dt * 1e3}
+        del xh, oh
     del x, o, scr, flush
     torch.cuda.empty_cache()
     return out
@@ -425,7 +453,7 @@ def run_b200(args, world, rank, local):
         torch.cuda.empty_cache()
         del flush
         torch.cuda.empty_cache()
-        extra.update(sortscan(args, dev, peak, rank))
+        extra.update(sortscan(args, dev, peak, rank, cpu=rank == 0 and world == 1 and not args.skip_cpu))
     barrier()
 
     if rank == 0:
