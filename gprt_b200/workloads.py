@@ -214,10 +214,73 @@ class LargeScene:
         torch.cuda.synchronize()
         return self.graph
 
+    # ---- end to end from pinned host buffers, pipelined over mesh chunks
+    def e2e_setup(self, host, hits_host, chunks=8):
+        """Split the meshes into `chunks` runs of about equal triangle count.
+        Each run is its own batch (its triangles' vertex indices still point
+        into the whole position array), collapsed and traced on its own, so
+        the run's host-to-device copies, its build + trace and its hits' copy
+        back overlap those of the other runs on three streams.  host: dict of
+        pinned tensors "pos", "tri", "rays" (the scene's shapes)."""
+        self.e2e_host, self.e2e_hits_host = host, hits_host
+        cum = self.off[1:]
+        cuts = [0] + [int(np.searchsorted(cum, self.n * k / chunks, side="left")) + 1 for k in range(1, chunks)]
+        cuts = sorted(set(min(max(c, 1), self.meshes) for c in cuts[1:]) | {0, self.meshes})
+        self.e2e_runs = []
+        for m0, m1 in zip(cuts[:-1], cuts[1:]):
+            t0, t1 = int(self.off[m0]), int(self.off[m1])
+            r0, r1 = int(self.roff[m0]), int(self.roff[m1])
+            off = self.off[m0:m1 + 1] - t0
+            roff = self.roff[m0:m1 + 1] - r0
+            b = api.BatchLbvh(off, self.dev, with_aabbs=False)
+            w = api.WideBvh(t1 - t0, m1 - m0, self.dev)
+            ro = torch.from_numpy(roff.astype(np.uint32).view(np.int32)).to(self.dev)
+            # the run's mesh and ray offsets are inputs too: copied every step
+            ho = (torch.from_numpy(off.astype(np.uint32).view(np.int32)).pin_memory(),
+                  torch.from_numpy(roff.astype(np.uint32).view(np.int32)).pin_memory())
+            self.e2e_runs.append((t0, t1, r0, r1, b, w, ro, ho))
+        self.e2e_hits = torch.empty_like(self.h_q)
+        self.s_in, self.s_run, self.s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+
+    def e2e_step(self):
+        """One pipelined end-to-end step; the caller's stream waits for all of it."""
+        h = self.e2e_host
+        start = torch.cuda.Event()
+        start.record()
+        for s in (self.s_in, self.s_run, self.s_out):
+            s.wait_event(start)
+        ev_in, ev_run = [], []
+        with torch.cuda.stream(self.s_in):
+            for t0, t1, r0, r1, b, _, ro, ho in self.e2e_runs:
+                b.tri_off.copy_(ho[0], non_blocking=True)
+                ro.copy_(ho[1], non_blocking=True)
+                self.pos[3 * t0:3 * t1].copy_(h["pos"][3 * t0:3 * t1], non_blocking=True)
+                self.tri[t0:t1].copy_(h["tri"][t0:t1], non_blocking=True)
+                self.rays[r0:r1].copy_(h["rays"][r0:r1], non_blocking=True)
+                e = torch.cuda.Event()
+                e.record()
+                ev_in.append(e)
+        with torch.cuda.stream(self.s_run):
+            for (t0, t1, r0, r1, b, w, ro, _), e in zip(self.e2e_runs, ev_in):
+                self.s_run.wait_event(e)
+                api.batch_build_triangles(self.pos, self.tri[t0:t1], b)
+                api.wide_build(b, wide=w)
+                api.wide_trace(w, self.rays[r0:r1], ro, hits=self.e2e_hits[r0:r1], scr=self.tscr)
+                e2 = torch.cuda.Event()
+                e2.record()
+                ev_run.append(e2)
+        with torch.cuda.stream(self.s_out):
+            for (t0, t1, r0, r1, _, _, _, _), e in zip(self.e2e_runs, ev_run):
+                self.s_out.wait_event(e)
+                self.e2e_hits_host[r0:r1].copy_(self.e2e_hits[r0:r1], non_blocking=True)
+            done = torch.cuda.Event()
+            done.record()
+        torch.cuda.current_stream().wait_event(done)
+
     def release(self):
         self.graph = None
         for k in ("pos", "tri", "batch", "rays", "wide", "h_plain", "h_bat", "h_q", "pscr", "local_tri", "descs",
-                  "tscr", "ray_off"):
+                  "tscr", "ray_off", "e2e_runs", "e2e_hits", "e2e_host", "e2e_hits_host"):
             if hasattr(self, k):
                 delattr(self, k)
         torch.cuda.empty_cache()
