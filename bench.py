@@ -37,6 +37,10 @@ The JSON line's value is whole-job Mrays/s of that step.  It also carries:
                 rays, closest and any hit
   spheres, lss  4,194,304 spheres / swept-sphere segments (hair strands):
                 bounds + box LBVH build and closest-hit trace of 4,194,304 rays
+  batched_build 4,096 meshes of log-uniform size in [64, 65,536] (~40M
+                triangles, each mesh in its own unit cube): batched build,
+                collapse, and the wide trace of 64 rays per triangle (~2.5G
+                rays, generated on the device in chunks of meshes)
   instances     two-level scene: 16,384 instances of 64 meshes (4,194,304
                 triangles), top-level rebuild and closest-hit trace of
                 16,777,216 rays
@@ -461,6 +465,11 @@ def run_b200(args, world, rank, local):
         isc = workloads.InstanceScene(device=dev)
         extra["instances"] = isc.run(steps=3, warmup=1, flush=flush)
         del isc
+        torch.cuda.empty_cache()
+        bsc = workloads.BatchedScene(device=dev)
+        extra["batched_build"] = bsc.run(steps=2, warmup=1, flush=flush)
+        del bsc
+        torch.cuda.empty_cache()
         torch.cuda.empty_cache()
         del flush
         torch.cuda.empty_cache()

@@ -417,3 +417,70 @@ class InstanceScene:
                 "blas_build_ms": self.blas_ms, "tlas_build_ms": tb, "trace_ms": tt,
                 "trace_mrays_s": self.nrays / tt / 1e3, "step_mrays_s": self.nrays / (tb + tt) / 1e3,
                 "hit_fraction": float((self.hits[:, 0] != -1).float().mean().item())}
+
+
+class BatchedScene:
+    """Batched build configuration: 4,096 meshes of log-uniform size in [64,
+    65,536] (about 40M triangles), each mesh of the small-LBVH distribution
+    in its own unit cube; 64 rays per triangle aimed at the mesh's box (about
+    2.5G rays), generated on the device and traced in chunks of meshes so
+    that no more than `chunk_rays` rays are resident at once.  Timed: the
+    batched build, the collapse, and the wide trace of every chunk (ray
+    generation is outside the timed events)."""
+
+    def __init__(self, meshes=4096, rays_per_tri=64, chunk_rays=1 << 27, seed=2024, device="cuda"):
+        dev = torch.device(device)
+        rng = np.random.default_rng(seed)
+        self.sizes = np.floor(np.exp(rng.uniform(np.log(64), np.log(65536), size=meshes))).astype(np.int64)
+        self.meshes = meshes
+        self.off = np.zeros(meshes + 1, np.int64)
+        self.off[1:] = np.cumsum(self.sizes)
+        self.n = int(self.off[-1])
+        self.roff = self.off * rays_per_tri
+        self.nrays = int(self.roff[-1])
+        toff = torch.from_numpy(self.off.astype(np.uint32).view(np.int32)).to(dev)
+        self.pos, self.tri = api.gen_soup(self.n, seed=seed + 1, sigma=0.002, tri_off=toff, meshes=meshes,
+                                          spacing=2.0, device=dev)
+        self.batch = api.BatchLbvh(self.off, dev, with_aabbs=False)
+        self.wide = api.WideBvh(self.n, meshes, dev)
+        # chunks of whole meshes, each at most chunk_rays rays (a mesh alone may exceed it)
+        self.chunks = []
+        m0 = 0
+        while m0 < meshes:
+            m1 = int(np.searchsorted(self.roff, self.roff[m0] + chunk_rays, side="right")) - 1
+            m1 = max(m1, m0 + 1)
+            self.chunks.append((m0, min(m1, meshes)))
+            m0 = min(m1, meshes)
+        biggest = max(int(self.roff[b] - self.roff[a]) for a, b in self.chunks)
+        self.hits = torch.empty((biggest, 2), dtype=torch.int32, device=dev)
+        self.tscr = api.scratch(lib().gprtcuTraceScratchSize(), dev)
+        self.seed = seed
+
+    def _chunk_offsets(self, a, b):
+        """Ray offsets over all meshes for chunk [a, b): meshes outside it get no rays."""
+        r0, r1 = self.roff[a], self.roff[b]
+        ro = np.clip(self.roff - r0, 0, r1 - r0)
+        return torch.from_numpy(ro.astype(np.uint32).view(np.int32)).to(self.hits.device), int(r1 - r0)
+
+    def run(self, steps=2, warmup=1, flush=None):
+        tb = float(np.mean(time_steps(lambda: api.batch_build_triangles(self.pos, self.tri, self.batch), steps, warmup,
+                                      flush)))
+        tc = float(np.mean(time_steps(lambda: api.wide_build(self.batch, wide=self.wide), steps, warmup, flush)))
+        tt, hits, same = 0.0, 0, None
+        for k, (a, b) in enumerate(self.chunks):
+            ro, nr = self._chunk_offsets(a, b)
+            rays = api.gen_rays(nr, seed=self.seed + 7 + k, ray_off=ro, meshes=self.meshes, boxes=self.batch.scene,
+                                device=self.hits.device)
+            h = self.hits[:nr]
+            tt += float(np.mean(time_steps(lambda: api.wide_trace(self.wide, rays, ro, hits=h, scr=self.tscr), 1,
+                                           1 if k == 0 else 0, flush)))
+            hits += int((h[:, 0] != -1).sum().item())
+            if k == 0:
+                hb = api.batch_trace(self.batch, rays, ro, scr=self.tscr)
+                same = bool(torch.equal(hb, h))
+                del hb
+            del rays
+        return {"meshes": self.meshes, "triangles": self.n, "rays": self.nrays, "ray_chunks": len(self.chunks),
+                "build_ms": tb, "collapse_ms": tc, "build_mprims_s": self.n / (tb + tc) / 1e3,
+                "trace_ms": tt, "trace_mrays_s": self.nrays / tt / 1e3,
+                "hit_fraction": hits / self.nrays, "hits_identical_binary_first_chunk": same}
