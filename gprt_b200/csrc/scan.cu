@@ -389,16 +389,28 @@ __global__ void __launch_bounds__(WARPS * 32) k_scan_tma(const uint32_t *in, uin
 constexpr int RR_SCAN_WARPS = 8;
 constexpr int RR_THREADS = (4 + RR_SCAN_WARPS) * 32;
 constexpr int RR_RS = 3, RR_SS = 4, RR_PQ = 8;
-constexpr size_t RR_SMEM = (size_t)(RR_RS + RR_SS) * SCAN_TILE * 4;
+// A scan stage has 64 bytes of slack past its tile: a partition stages its
+// two runs shifted so that each run's shared-memory and global addresses
+// agree modulo 16 bytes.
+constexpr uint32_t RR_STAGE_BYTES = SCAN_TILE * 4 + 64;
+constexpr size_t RR_SMEM = (size_t)RR_RS * SCAN_TILE * 4 + (size_t)RR_SS * RR_STAGE_BYTES;
 constexpr uint32_t RR_END = 0xFFFFFFFFu;
 struct RrPending {
   uint32_t tile, prefix, part[RR_SCAN_WARPS];
 };
 
+// MODE: 0 exclusive sum, 1 inclusive sum, 2 partition, 3 select (by the
+// sign bit: want_neg selects negatives).  For 2 and 3 the tile aggregates
+// are selected counts, d_total receives the total selected count, and the
+// scanner warps stage each tile's selected items in order at the bottom of
+// its scan stage and, for a partition, its unselected items in reverse order
+// at the top, then write both groups out as coalesced runs (plain stores:
+// the output offsets have any alignment).
 template <int MODE>
 __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *in, uint32_t *out, uint64_t n,
                                                                uint64_t ntiles, ScratchHeader *hdr, uint64_t *status,
-                                                               uint32_t *d_total, uint32_t budget, int64_t skip_tile) {
+                                                               uint32_t *d_total, uint32_t budget, int64_t skip_tile,
+                                                               uint32_t want_neg) {
   constexpr int RS = RR_RS, SS = RR_SS, PQ = RR_PQ, SW = RR_SCAN_WARPS;
   constexpr uint32_t TILE = SCAN_TILE, TB = SCAN_TILE * 4;
   static_assert(PQ % 2 == 0, "pending slot q always belongs to look-back warp q % 2");
@@ -477,13 +489,18 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
       }
       const uint4 *b = reinterpret_cast<const uint4 *>(rbuf + (size_t)s * TB);
       uint32_t part[SW];
+      // elements of the tile (a partial last tile is zero-filled past them)
+      const uint32_t tc = n - (uint64_t)t * TILE < (uint64_t)TILE ? (uint32_t)(n - (uint64_t)t * TILE) : TILE;
 #pragma unroll
       for (int w = 0; w < SW; ++w) {
         uint32_t p = 0;
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
           const uint4 v = b[(w * 8 + r) * 32 + lane];
-          p += (v.x + v.y) + (v.z + v.w);
+          if (MODE < 2)
+            p += (v.x + v.y) + (v.z + v.w);
+          else  // negatives; the zero fill past a partial tile counts as none
+            p += ((v.x >> 31) + (v.y >> 31)) + ((v.z >> 31) + (v.w >> 31));
         }
         part[w] = p;
       }
@@ -491,6 +508,13 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
       for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
         for (int w = 0; w < SW; ++w) part[w] += __shfl_xor_sync(FULL_MASK, part[w], o);
+      if (MODE >= 2 && !want_neg) {  // non-negatives among each scanner's valid items
+#pragma unroll
+        for (int w = 0; w < SW; ++w) {
+          const uint32_t lo = (uint32_t)w * 1024u;
+          part[w] = (tc > lo ? (tc - lo < 1024u ? tc - lo : 1024u) : 0u) - part[w];
+        }
+      }
       __syncwarp();
       uint32_t agg = 0;
 #pragma unroll
@@ -540,7 +564,7 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
         mbar_arrive(&s_full[ss]);
         return;
       }
-      load_tile(reinterpret_cast<uint32_t *>(sbuf + (size_t)ss * TB), t, &s_full[ss], pol);
+      load_tile(reinterpret_cast<uint32_t *>(sbuf + (size_t)ss * RR_STAGE_BYTES), t, &s_full[ss], pol);
     }
   } else {
     const int w = warp - 4;
@@ -555,9 +579,97 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
       }
       const uint32_t t = s_tile[ss];
       if (t == RR_END) break;
+      if constexpr (MODE >= 2) {
+        const uint32_t excl = pend[q].prefix;
+        uint32_t tsel = 0, rowbase = 0;
+#pragma unroll
+        for (int k = 0; k < SW; ++k) {
+          const uint32_t pc = pend[q].part[k];
+          rowbase += k < w ? pc : 0u;
+          tsel += pc;
+        }
+        const uint64_t base = (uint64_t)t * TILE;
+        const uint32_t tc = n - base < (uint64_t)TILE ? (uint32_t)(n - base) : TILE;
+        uint32_t *sb = reinterpret_cast<uint32_t *>(sbuf + (size_t)ss * RR_STAGE_BYTES);
+        const uint4 *wb = reinterpret_cast<const uint4 *>(sb) + w * 8 * 32;
+        uint4 v[8];
+        uint32_t fl[8], pk[2] = {0u, 0u};
+        const uint32_t flip = want_neg ? 0u : 15u;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          v[r] = wb[r * 32 + lane];
+          const uint32_t l0 = (uint32_t)((w * 8 + r) * 128 + lane * 4);
+          const uint32_t rem = tc > l0 ? tc - l0 : 0u;
+          const uint32_t valid = rem >= 4 ? 15u : (1u << rem) - 1u;
+          fl[r] = (((v[r].x >> 31) | ((v[r].y >> 31) << 1) | ((v[r].z >> 31) << 2) | ((v[r].w >> 31) << 3)) ^ flip) & valid;
+          pk[r >> 2] |= (uint32_t)__popc(fl[r]) << (8 * (r & 3));
+        }
+        // Inclusive warp scan of the rows' counts, four rows to a word (a
+        // row's total is at most 128, so a byte holds it).
+        const uint32_t own[2] = {pk[0], pk[1]};
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const uint32_t y = __shfl_up_sync(FULL_MASK, pk[h], o);
+            if (lane >= o) pk[h] += y;
+          }
+        const uint32_t rowtot[2] = {__shfl_sync(FULL_MASK, pk[0], 31), __shfl_sync(FULL_MASK, pk[1], 31)};
+        // Selected rank ls goes to out[excl + ls], unselected rank lu to
+        // out[top - lu].  Staged at sb[s1 + ls] and sb[u_top - lu], with the
+        // shifts chosen so that shared and global indices agree modulo 4:
+        // both runs then leave as 16-byte stores between ragged ends.
+        const uint32_t tunsel = tc - tsel;
+        const uint64_t top = (n - 1) - (base - excl);
+        const uint32_t s1 = (uint32_t)(excl & 3);
+        const uint32_t u_top = TILE + 7 + (uint32_t)((top - (TILE + 7)) & 3);  // <= TILE + 10; u_top == top mod 4
+        named_bar_sync(1, SW * 32);  // every scanner holds its rows: the stage can be overwritten
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const uint32_t sh = 8 * (r & 3);
+          // selected items of the tile before this lane's first in row r
+          uint32_t ls = rowbase + ((pk[r >> 2] - own[r >> 2]) >> sh & 0xFFu);
+          const uint32_t l0 = (uint32_t)((w * 8 + r) * 128 + lane * 4);
+          const uint32_t vals[4] = {v[r].x, v[r].y, v[r].z, v[r].w};
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            const uint32_t sel = (fl[r] >> c) & 1u;
+            if (MODE == 2) {
+              // unselected rank is (l0 + c) - ls
+              const uint32_t at = sel ? s1 + ls : u_top - (l0 + c) + ls;
+              if (l0 + c < tc) sb[at] = vals[c];
+            } else if (sel) {
+              sb[s1 + ls] = vals[c];
+            }
+            ls += sel;
+          }
+          rowbase += rowtot[r >> 2] >> sh & 0xFFu;
+        }
+        named_bar_sync(1, SW * 32);
+        const uint32_t ct = (uint32_t)(tid - 4 * 32);
+        // one run: `cnt` words from sb[sidx] to out[gidx], sidx == gidx mod 4
+        auto write_run = [&](uint32_t sidx, uint64_t gidx, uint32_t cnt) {
+          const uint32_t head = (uint32_t)((4 - (gidx & 3)) & 3) < cnt ? (uint32_t)((4 - (gidx & 3)) & 3) : cnt;
+          const uint32_t mid = (cnt - head) & ~3u;
+          if (ct < head) out[gidx + ct] = sb[sidx + ct];
+          const uint4 *s4 = reinterpret_cast<const uint4 *>(sb + sidx + head);
+          uint4 *g4 = reinterpret_cast<uint4 *>(out + gidx + head);
+          for (uint32_t k = ct; k < mid / 4; k += SW * 32) g4[k] = s4[k];
+          const uint32_t tail = cnt - head - mid;
+          if (ct < tail) out[gidx + head + mid + ct] = sb[sidx + head + mid + ct];
+        };
+        write_run(s1, excl, tsel);
+        if (MODE == 2 && tunsel) write_run(u_top - (tunsel - 1), top - (tunsel - 1), tunsel);
+        named_bar_sync(1, SW * 32);  // the stage has been read
+        if (leader) {
+          mbar_arrive(&p_empty[q]);
+          mbar_arrive(&s_empty[ss]);
+        }
+        continue;
+      }
       uint32_t carry = pend[q].prefix;
       for (int k = 0; k < w; ++k) carry += pend[q].part[k];
-      uint4 *wb = reinterpret_cast<uint4 *>(sbuf + (size_t)ss * TB) + w * 8 * 32;
+      uint4 *wb = reinterpret_cast<uint4 *>(sbuf + (size_t)ss * RR_STAGE_BYTES) + w * 8 * 32;
       uint4 v[8];
       uint32_t sum[8], inc[8];
 #pragma unroll
@@ -596,7 +708,7 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
       const uint64_t base = (uint64_t)t * TILE;
       const uint64_t r = n - base < (uint64_t)TILE ? n - base : (uint64_t)TILE;
       const uint32_t a = (uint32_t)(r & ~3ull);
-      const uint32_t *sb = reinterpret_cast<const uint32_t *>(sbuf + (size_t)ss * TB);
+      const uint32_t *sb = reinterpret_cast<const uint32_t *>(sbuf + (size_t)ss * RR_STAGE_BYTES);
       if (r < (uint64_t)TILE) {
         for (uint32_t k = a + (tid - 4 * 32); k < r; k += SW * 32) out[base + k] = sb[k];
         named_bar_sync(1, SW * 32);
@@ -784,6 +896,10 @@ static int reread_ctas() {
             cudaSuccess &&
         cudaFuncSetAttribute(k_scan_reread<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RR_SMEM) ==
             cudaSuccess &&
+        cudaFuncSetAttribute(k_scan_reread<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RR_SMEM) ==
+            cudaSuccess &&
+        cudaFuncSetAttribute(k_scan_reread<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RR_SMEM) ==
+            cudaSuccess &&
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_scan_reread<0>, RR_THREADS, RR_SMEM) == cudaSuccess)
       cached[dev] = occ * gprtcu_num_sms();
     else
@@ -842,10 +958,10 @@ static gprtcuStatus scan_launch(const uint32_t *in, uint32_t *out, uint64_t n, i
     const unsigned grid = (unsigned)(tiles < (uint64_t)rr_ctas ? tiles : (uint64_t)rr_ctas);
     if (inclusive)
       k_scan_reread<1><<<grid, RR_THREADS, RR_SMEM, stream>>>(in, out, n, tiles, hdr, status, d_total, g_spin_budget,
-                                                             g_skip_tile);
+                                                             g_skip_tile, 0u);
     else
       k_scan_reread<0><<<grid, RR_THREADS, RR_SMEM, stream>>>(in, out, n, tiles, hdr, status, d_total, g_spin_budget,
-                                                             g_skip_tile);
+                                                             g_skip_tile, 0u);
   } else if (impl == 2) {
     // TMA-staged tile-per-CTA kernel (32 KB dynamic shared memory per CTA).
     if (inclusive)
@@ -889,6 +1005,24 @@ static gprtcuStatus partition_launch(const int32_t *in, int32_t *out, uint64_t n
     return GPRTCU_OK;
   }
   const bool vec = ((uintptr_t)in & 15) == 0;
+  // Large buffers with 16-byte aligned input and output: the persistent
+  // re-read kernel (as for the sums); the scan-kernel override of the test
+  // hook applies here too.
+  const bool rr_ok = vec && ((uintptr_t)out & 15) == 0;
+  const int impl = rr_ok ? (g_scan_impl == 0 ? (n >= kRereadMinN ? 3 : 1) : g_scan_impl) : 1;
+  const int rr_ctas = impl == 3 ? reread_ctas() : 0;
+  if (impl == 3 && rr_ctas > 0) {
+    const unsigned g = (unsigned)(tiles < (uint64_t)rr_ctas ? tiles : (uint64_t)rr_ctas);
+    const uint32_t want_neg = select_positive ? 0u : 1u;
+    if (partition)
+      k_scan_reread<2><<<g, RR_THREADS, RR_SMEM, stream>>>((const uint32_t *)in, (uint32_t *)out, n, tiles, hdr, status,
+                                                          d_count, g_spin_budget, -1, want_neg);
+    else
+      k_scan_reread<3><<<g, RR_THREADS, RR_SMEM, stream>>>((const uint32_t *)in, (uint32_t *)out, n, tiles, hdr, status,
+                                                          d_count, g_spin_budget, -1, want_neg);
+    GPRTCU_TRY(cudaGetLastError());
+    return GPRTCU_OK;
+  }
   dim3 grid((unsigned)tiles), block(SCAN_THREADS);
   if (partition) {
     if (vec) k_partition_i32<true, true><<<grid, block, 0, stream>>>(in, out, n, tiles, select_positive, hdr, status, d_count, g_spin_budget);

@@ -101,7 +101,7 @@ def test_scan_empty(cuda):
 
 
 @pytest.mark.parametrize("select_only", [False, True])
-def test_partition_select_t03(cuda, select_only):
+def test_partition_select_t03(cuda, select_only, scan_impl):
     # tests/t03-bufferScans/hostCode.cpp:91-241 on the t03 schedule.
     import torch
     from gprt_b200 import api
@@ -120,16 +120,20 @@ def test_partition_select_t03(cuda, select_only):
             assert np.array_equal(got, exp)
 
 
-def test_partition_negative_select_and_random(cuda):
+def test_partition_negative_select_and_random(cuda, scan_impl):
     import torch
     from gprt_b200 import api
     rng = np.random.default_rng(4)
-    for n in (1, 5, 8191, 8193, 100000):
+    for n in (1, 5, 8191, 8193, 100000, (1 << 20) + 3, 3000017):
         x = rng.integers(-2 ** 31, 2 ** 31, size=n, dtype=np.int64).astype(np.int32)
+        d = torch.from_numpy(x).cuda()
         for sp in (True, False):
-            out, cnt = api.partition(torch.from_numpy(x).cuda(), sp)
+            out, cnt = api.partition(d, sp)
             exp, etot = oracle.partition(x, sp, True)
-            assert int(cnt.item()) == etot and np.array_equal(out.cpu().numpy(), exp)
+            assert int(cnt.item()) == etot and np.array_equal(out.cpu().numpy(), exp), (n, sp)
+            out, cnt = api.partition(d, sp, select_only=True)
+            exp, etot = oracle.partition(x, sp, False)
+            assert int(cnt.item()) == etot and np.array_equal(out.cpu().numpy()[:etot], exp[:etot]), (n, sp)
 
 
 def test_scan_lookback_timeout_is_reported_not_hung(cuda, scan_impl):
