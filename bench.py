@@ -49,6 +49,11 @@ The JSON line's value is whole-job Mrays/s of that step.  It also carries:
                 algorithmic traffic against the measured HBM bandwidth; beside
                 each, the CPU oracle (std::stable_sort, serial exclusive sum,
                 one thread) on a bounded sample of the same data
+  partition, select
+                stable split of 1,073,741,824 uniform int32 by sign (items
+                >= 0 first, the rest reversed behind them) and the selection of
+                the items >= 0 alone; GB/s of algorithmic traffic, with the
+                serial CPU oracle beside each
   clocks        SM clock samples taken during the timed region
 Multi-GPU (torchrun): every rank builds and traces its own scene (weak
 scaling, no data-path collective); time = max over ranks.
@@ -233,6 +238,45 @@ def sortscan(args, dev, peak, rank, cpu=False):
                                        "sample": "first %d of the same values: serial exclusive sum" % m,
                                        "ms": dt * 1e3}
         del xh, oh
+    del x, o
+    torch.cuda.empty_cache()
+    # partition / select by sign: uniform int32, items >= 0 selected
+    g = torch.Generator(device=dev).manual_seed(11 + rank)
+    x = torch.randint(-(1 << 31), (1 << 31) - 1, (SCAN_N,), dtype=torch.int32, device=dev, generator=g)
+    o = torch.empty_like(x)
+    cnt = torch.empty(1, dtype=torch.int32, device=dev)
+    want = int((x >= 0).sum().item())
+    xsum = int(x.sum(dtype=torch.int64).item())
+    for name, sel in (("partition", False), ("select", True)):
+        ts = []
+        for i in range(args.warmup + args.steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            api.partition(x, True, o, cnt, scr, select_only=sel)
+            b.record()
+            b.synchronize()
+            if i >= args.warmup:
+                ts.append(a.elapsed_time(b))
+        t = sum(ts) / len(ts)
+        c = int(cnt.item())
+        ok = c == want and bool((o[:c] >= 0).all().item())
+        if not sel:
+            ok = ok and bool((o[c:] < 0).all().item()) and int(o.sum(dtype=torch.int64).item()) == xsum
+        alg = 4 * SCAN_N + 4 * (c if sel else SCAN_N)
+        out[name] = {"n": SCAN_N, "values": "uniform int32, items >= 0 selected", "ms": t,
+                     "gbs": alg / (t * 1e-3) / 1e9, "frac_of_hbm": alg / (t * 1e-3) / 1e9 / peak, "ok": ok}
+        if cpu:
+            import oracle
+            m = 1 << 28
+            xh = x[:m].cpu().numpy()
+            t0 = time.perf_counter()
+            _, hc = oracle.partition(xh, True, partition=not sel)
+            dt = time.perf_counter() - t0
+            out[name]["cpu_baseline"] = {"value": (4 * m + 4 * (hc if sel else m)) / dt / 1e9, "unit": "GB/s", "cores": 1, "kind": "port",
+                                         "sample": "first %d of the same values: serial stable %s" % (m, name),
+                                         "ms": dt * 1e3}
+            del xh
     del x, o, scr, flush
     torch.cuda.empty_cache()
     return out
