@@ -1,6 +1,7 @@
 """Benchmark of the B200 acceleration-structure path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+    python bench.py --only sortscan [--steps K] [--warmup W]   (those extras alone)
 
 One step = the large combined workload's batched + quantised pass, replayed
 from one CUDA graph: a batched LBVH build over 67,108,864 fp32 triangles in
@@ -412,6 +413,18 @@ def run_b200(args, world, rank, local):
     def slowest(x):
         return max_over_ranks(x, dev, world)
 
+    if args.only == "sortscan":
+        # the sort, scan, partition and select extras alone (their own JSON
+        # object, no headline line): a short command to profile those kernels
+        out = sortscan(args, dev, peak, rank, cpu=rank == 0 and world == 1 and not args.skip_cpu)
+        barrier()
+        if rank == 0:
+            print(json.dumps({"only": "sortscan", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                              "peak_gbs": peak, "peak_kind": peak_kind, **out}))
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     sc = workloads.LargeScene(meshes=args.meshes, n=args.triangles, seed_offset=rank, device=dev)
     g = sc.capture()
@@ -586,6 +599,8 @@ def main():
     ap.add_argument("--ref-tris", type=int, default=1 << 20, help="triangles per step of the reference arm")
     ap.add_argument("--skip-extra", action="store_true", help="only the headline workload")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--only", choices=["sortscan"],
+                    help="run only the named extras and print them as one JSON object (no headline line)")
     args = ap.parse_args()
     world, rank, local = dist_env()
     if args.impl == "reference":

@@ -136,6 +136,36 @@ def test_partition_negative_select_and_random(cuda, scan_impl):
             assert int(cnt.item()) == etot and np.array_equal(out.cpu().numpy()[:etot], exp[:etot]), (n, sp)
 
 
+def test_partition_edges_and_alignment(cuda):
+    # One-sided inputs (every item selected: the unselected run is empty, and
+    # the reverse), the int32 extremes and zeros, and buffers starting 4 bytes
+    # past a 16-byte boundary (input or output), which take the tile-per-CTA
+    # kernel instead of the persistent one.
+    import torch
+    from gprt_b200 import api
+    rng = np.random.default_rng(5)
+    n = (1 << 21) + 5
+    cases = {
+        "nonneg": rng.integers(0, 2 ** 31, size=n, dtype=np.int64).astype(np.int32),
+        "neg": rng.integers(-2 ** 31, 0, size=n, dtype=np.int64).astype(np.int32),
+        "extremes": rng.choice(np.array([-2 ** 31, -1, 0, 1, 2 ** 31 - 1], dtype=np.int32), size=n),
+    }
+    for name, x in cases.items():
+        for shift_in, shift_out in ((0, 0), (1, 0), (0, 1)):
+            buf = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+            buf[shift_in:shift_in + n] = torch.from_numpy(x).cuda()
+            d = buf[shift_in:shift_in + n]
+            for sp in (True, False):
+                for sel in (False, True):
+                    obuf = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+                    out = obuf[shift_out:shift_out + n]
+                    _, cnt = api.partition(d, sp, out=out, select_only=sel)
+                    exp, etot = oracle.partition(x, sp, not sel)
+                    got = out.cpu().numpy()
+                    k = etot if sel else n
+                    assert int(cnt.item()) == etot and np.array_equal(got[:k], exp[:k]), (name, shift_in, shift_out, sp, sel)
+
+
 def test_scan_lookback_timeout_is_reported_not_hung(cuda, scan_impl):
     # Fault injection without a GPU fault: one tile never publishes; its
     # successors exhaust a small wait budget, record TIMEOUT and return.
