@@ -404,8 +404,8 @@ struct RrPending {
 // are selected counts, d_total receives the total selected count, and the
 // scanner warps stage each tile's selected items in order at the bottom of
 // its scan stage and, for a partition, its unselected items in reverse order
-// at the top, then write both groups out as coalesced runs (plain stores:
-// the output offsets have any alignment).
+// at the top, then write both groups out as coalesced runs: 16-byte stores
+// between scalar ends (the dispatch requires a 16-byte aligned output).
 template <int MODE>
 __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *in, uint32_t *out, uint64_t n,
                                                                uint64_t ntiles, ScratchHeader *hdr, uint64_t *status,
