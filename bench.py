@@ -1,7 +1,8 @@
 """Benchmark of the B200 acceleration-structure path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-    python bench.py --only sortscan [--steps K] [--warmup W]   (those extras alone)
+    python bench.py --only sortscan [--steps K] [--warmup W] [--sort-n N] [--scan-n N]
+                    (those extras alone; the sizes default to the full workload)
 
 One step = the large combined workload's batched + quantised pass, replayed
 from one CUDA graph: a batched LBVH build over 67,108,864 fp32 triangles in
@@ -169,14 +170,15 @@ def sortscan(args, dev, peak, rank, cpu=False):
     import torch
 
     from gprt_b200 import api
+    sort_n, scan_n = args.sort_n, args.scan_n
     out = {}
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     # sort: Zipf(1.1) uint32 keys, payload = index
-    k0 = zipf_keys(SORT_N, 7 + rank)
-    v0 = torch.arange(SORT_N, dtype=torch.int32, device=dev)
+    k0 = zipf_keys(sort_n, 7 + rank)
+    v0 = torch.arange(sort_n, dtype=torch.int32, device=dev)
     k = torch.empty_like(k0)
     v = torch.empty_like(v0)
-    scr = api.scratch(api.sort_scratch_size(SORT_N, 4, 4), dev)
+    scr = api.scratch(api.sort_scratch_size(sort_n, 4, 4), dev)
     ts = []
     for i in range(args.warmup + args.steps):
         k.copy_(k0)
@@ -192,13 +194,13 @@ def sortscan(args, dev, peak, rank, cpu=False):
     ok = bool(torch.all(k[1:].to(torch.int64) & 0xFFFFFFFF >= k[:-1].to(torch.int64) & 0xFFFFFFFF).item())
     t = sum(ts) / len(ts)
     alg = 4 + 4 * 2 * 8  # 68 B per pair at 8-bit digits
-    out["sort"] = {"n": SORT_N, "keys": "Zipf(1.1) uint32 + uint32 payload", "ms": t,
-                   "mkeys_s": SORT_N / (t * 1e-3) / 1e6, "gbs": alg * SORT_N / (t * 1e-3) / 1e9,
-                   "frac_of_hbm": alg * SORT_N / (t * 1e-3) / 1e9 / peak, "sorted": ok,
+    out["sort"] = {"n": sort_n, "keys": "Zipf(1.1) uint32 + uint32 payload", "ms": t,
+                   "mkeys_s": sort_n / (t * 1e-3) / 1e6, "gbs": alg * sort_n / (t * 1e-3) / 1e9,
+                   "frac_of_hbm": alg * sort_n / (t * 1e-3) / 1e9 / peak, "sorted": ok,
                    "gpu_launches_per_call": 6}
     if cpu:
         import oracle
-        m = 1 << 24
+        m = min(1 << 24, sort_n)
         kh = k0[:m].cpu().numpy().view(np.uint32).copy()
         vh = np.arange(m, dtype=np.uint32)
         t0 = time.perf_counter()
@@ -209,10 +211,10 @@ def sortscan(args, dev, peak, rank, cpu=False):
                                                  % m, "ms": dt * 1e3}
     del k0, v0, k, v, scr
     torch.cuda.empty_cache()
-    x = torch.randint(0, 256, (SCAN_N,), dtype=torch.int32, device=dev)
+    x = torch.randint(0, 256, (scan_n,), dtype=torch.int32, device=dev)
     o = torch.empty_like(x)
     tot = torch.empty(1, dtype=torch.int32, device=dev)
-    scr = api.scratch(api.scan_scratch_size(SCAN_N), dev)
+    scr = api.scratch(api.scan_scratch_size(scan_n), dev)
     ts = []
     for i in range(args.warmup + args.steps):
         flush.zero_()
@@ -224,12 +226,12 @@ def sortscan(args, dev, peak, rank, cpu=False):
         if i >= args.warmup:
             ts.append(a.elapsed_time(b))
     t = sum(ts) / len(ts)
-    out["scan"] = {"n": SCAN_N, "values": "uniform [0,255] uint32", "ms": t, "gbs": 8 * SCAN_N / (t * 1e-3) / 1e9,
-                   "frac_of_hbm": 8 * SCAN_N / (t * 1e-3) / 1e9 / peak,
+    out["scan"] = {"n": scan_n, "values": "uniform [0,255] uint32", "ms": t, "gbs": 8 * scan_n / (t * 1e-3) / 1e9,
+                   "frac_of_hbm": 8 * scan_n / (t * 1e-3) / 1e9 / peak,
                    "total_ok": int(tot.item()) & 0xFFFFFFFF == int(x.sum().item()) & 0xFFFFFFFF}
     if cpu:
         import oracle
-        m = 1 << 28
+        m = min(1 << 28, scan_n)
         xh = x[:m].cpu().numpy().view(np.uint32).copy()
         oh = np.empty_like(xh)
         t0 = time.perf_counter()
@@ -243,7 +245,7 @@ def sortscan(args, dev, peak, rank, cpu=False):
     torch.cuda.empty_cache()
     # partition / select by sign: uniform int32, items >= 0 selected
     g = torch.Generator(device=dev).manual_seed(11 + rank)
-    x = torch.randint(-(1 << 31), (1 << 31) - 1, (SCAN_N,), dtype=torch.int32, device=dev, generator=g)
+    x = torch.randint(-(1 << 31), (1 << 31) - 1, (scan_n,), dtype=torch.int32, device=dev, generator=g)
     o = torch.empty_like(x)
     cnt = torch.empty(1, dtype=torch.int32, device=dev)
     want = int((x >= 0).sum().item())
@@ -264,12 +266,12 @@ def sortscan(args, dev, peak, rank, cpu=False):
         ok = c == want and bool((o[:c] >= 0).all().item())
         if not sel:
             ok = ok and bool((o[c:] < 0).all().item()) and int(o.sum(dtype=torch.int64).item()) == xsum
-        alg = 4 * SCAN_N + 4 * (c if sel else SCAN_N)
-        out[name] = {"n": SCAN_N, "values": "uniform int32, items >= 0 selected", "ms": t,
+        alg = 4 * scan_n + 4 * (c if sel else scan_n)
+        out[name] = {"n": scan_n, "values": "uniform int32, items >= 0 selected", "ms": t,
                      "gbs": alg / (t * 1e-3) / 1e9, "frac_of_hbm": alg / (t * 1e-3) / 1e9 / peak, "ok": ok}
         if cpu:
             import oracle
-            m = 1 << 28
+            m = min(1 << 28, scan_n)
             xh = x[:m].cpu().numpy()
             t0 = time.perf_counter()
             _, hc = oracle.partition(xh, True, partition=not sel)
@@ -599,6 +601,8 @@ def main():
     ap.add_argument("--ref-tris", type=int, default=1 << 20, help="triangles per step of the reference arm")
     ap.add_argument("--skip-extra", action="store_true", help="only the headline workload")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--sort-n", type=int, default=SORT_N, help="pairs of the sort extra")
+    ap.add_argument("--scan-n", type=int, default=SCAN_N, help="elements of the scan, partition and select extras")
     ap.add_argument("--only", choices=["sortscan"],
                     help="run only the named extras and print them as one JSON object (no headline line)")
     args = ap.parse_args()
