@@ -420,9 +420,11 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
   __shared__ uint64_t r_full[RS], r_empty[RS], p_full[PQ], p_empty[PQ], s_full[SS], s_empty[SS];
   __shared__ RrPending pend[PQ];
   __shared__ uint32_t r_tile[RS], s_tile[SS];
+  __shared__ volatile uint32_t s_scan_stop;  // a scanner's wait gave up: all scanners leave together
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   unsigned char *rbuf = smem, *sbuf = smem + (size_t)RS * TB;
   if (tid == 0) {
+    s_scan_stop = 0;
     for (int i = 0; i < RS; ++i) {
       mbar_init(&r_full[i], 32);
       mbar_init(&r_empty[i], 1);
@@ -573,7 +575,12 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
     int prev = -1;
     for (uint32_t i = 0;; ++i) {
       const int ss = i % SS, q = i % PQ;
-      if (!mbar_wait(&s_full[ss], (i / SS) & 1, MBAR_WAIT_BUDGET)) {
+      // The scanners meet at named barriers, so none may leave on its own:
+      // a warp whose wait gave up raises the flag, and after this barrier
+      // all of them see the same flag and the same stage.
+      if (!mbar_wait(&s_full[ss], (i / SS) & 1, MBAR_WAIT_BUDGET)) s_scan_stop = 1;
+      named_bar_sync(1, SW * 32);
+      if (s_scan_stop) {
         if (leader) record_error(hdr, GPRTCU_ERR_TIMEOUT);
         break;
       }
