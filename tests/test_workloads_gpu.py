@@ -72,3 +72,21 @@ def test_host_generator_restatement_tracks_device(cuda):
     hr = scenes.device_rays_range(6, 0, 4096, box_lo, box_hi)
     fin = np.isfinite(hr)
     assert np.abs(hr[fin] - r[fin]).max() < 1e-4 and np.array_equal(np.isinf(hr), np.isinf(r))
+
+
+def test_bench_sortscan_extras_small(cuda):
+    # The bench's sort / scan / partition / select section on small sizes, as
+    # a user runs it: one JSON object whose own checks all hold.
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--only", "sortscan", "--sort-n", "1048583",
+                          "--scan-n", "4194311", "--steps", "1", "--warmup", "1", "--skip-cpu"],
+                         cwd=root, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = [l for l in out.stdout.splitlines() if l.startswith("{")][-1]
+    d = json.loads(line)
+    assert d["only"] == "sortscan" and d["sort"]["n"] == 1048583 and d["scan"]["n"] == 4194311
+    assert d["sort"]["sorted"] and d["scan"]["total_ok"] and d["partition"]["ok"] and d["select"]["ok"]
