@@ -25,7 +25,10 @@ The JSON line's value is whole-job Mrays/s of that step.  It also carries:
   t_check       hit distances of a seeded 1% subsample of the hits against an
                 FP64 plane-equation distance
   cpu_baseline  the CPU oracle on this host's cores, on the first meshes of
-                the same workload (regenerated on the host)
+                the same workload (their triangles and rays copied from the
+                device); oracle_match: the oracle's hits for those meshes
+                against the batched + quantised step's, ids and t bits, every
+                ray (a mismatch fails the run after the line is printed)
   e2e           the same work from pinned host buffers: triangles, indices,
                 offsets and rays copied in and the hits copied out inside the
                 timed region, pipelined over 16 runs of meshes on three streams
@@ -46,6 +49,10 @@ The JSON line's value is whole-job Mrays/s of that step.  It also carries:
   instances     two-level scene: 16,384 instances of 64 meshes (4,194,304
                 triangles), top-level rebuild and closest-hit trace of
                 16,777,216 rays
+  c0            the small plain case: 1,048,576 uniform uint32 keys (seed 0)
+                with payload = index, and inclusive and exclusive sums of
+                1,048,576 uint32 values uniform in [0, 255]; bit-exact against
+                std::stable_sort and the serial sum beside them
   sort, scan    268,435,456 Zipf(1.1) uint32 key/payload pairs and a
                 1,073,741,824-element uint32 exclusive sum, GB/s of
                 algorithmic traffic against the measured HBM bandwidth; beside
@@ -80,10 +87,6 @@ SORT_N = 268_435_456
 SCAN_N = 1_073_741_824
 WORKLOAD = ("large combined, batched + quantised: {tris:,} fp32 triangles in {meshes:,} meshes, {rays:,} "
             "closest-hit rays; batched LBVH build + 8-wide uint8-quantised collapse + wide trace in one CUDA graph")
-# DRAM bytes (read + write) of one k_trace_wide launch on the default large
-# workload, from the one-pass ncu capture summarised in
-# profiles/k_trace_wide_large.md; reported only for that workload.
-TRACE_WIDE_DRAM_BYTES = 9_071_616_000 + 1_104_399_000
 
 
 def measured_peaks():
@@ -163,6 +166,81 @@ def zipf_keys(n, seed, s=1.1):
     return (r - 1).to(torch.int64).to(torch.int32)  # wraps to the uint32 bit pattern
 
 
+def c0_small(args, dev, peak, cpu=False):
+    """The small plain case: 2^20 uniform uint32 keys from seed 0 with payload
+    = index, and inclusive / exclusive sums of 2^20 uint32 values uniform in
+    [0, 255].  Device-resident, L2 flushed between calls; with cpu, the
+    oracle's std::stable_sort and serial sums (the reference tests' own host
+    oracles) are timed beside them and the GPU results compared bit for bit."""
+    import torch
+
+    from gprt_b200 import api
+    n = 1 << 20
+    rng = np.random.default_rng(0)
+    kh = rng.integers(0, 2 ** 32, size=n, dtype=np.uint64).astype(np.uint32)
+    vh = np.arange(n, dtype=np.uint32)
+    xh = rng.integers(0, 256, size=n, dtype=np.uint64).astype(np.uint32)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    k0 = torch.from_numpy(kh.view(np.int32)).to(dev)
+    v0 = torch.from_numpy(vh.view(np.int32)).to(dev)
+    k, v = torch.empty_like(k0), torch.empty_like(v0)
+    sscr = api.scratch(api.sort_scratch_size(n, 4, 4), dev)
+    x = torch.from_numpy(xh.view(np.int32)).to(dev)
+    oe, oi = torch.empty_like(x), torch.empty_like(x)
+    tot = torch.empty(1, dtype=torch.int32, device=dev)
+    cscr = api.scratch(api.scan_scratch_size(n), dev)
+
+    def timed(fn, prep=None):
+        ts = []
+        for i in range(args.warmup + args.steps):
+            if prep:
+                prep()
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            b.synchronize()
+            if i >= args.warmup:
+                ts.append(a.elapsed_time(b))
+        return float(np.mean(ts))
+
+    sort_ms = timed(lambda: api.sort(k, v, 0, 32, sscr), lambda: (k.copy_(k0), v.copy_(v0)))
+    excl_ms = timed(lambda: api.exclusive_sum(x, oe, tot, cscr))
+    incl_ms = timed(lambda: api.inclusive_sum(x, oi, tot, cscr))
+    out = {"n": n, "note": "L2-resident sizes: fractions reported, not graded",
+           "sort": {"ms": sort_ms, "mkeys_s": n / sort_ms / 1e3, "gbs": 68 * n / sort_ms / 1e6,
+                    "frac_of_hbm": 68 * n / sort_ms / 1e6 / peak},
+           "exclusive_sum": {"ms": excl_ms, "gbs": 8 * n / excl_ms / 1e6, "frac_of_hbm": 8 * n / excl_ms / 1e6 / peak},
+           "inclusive_sum": {"ms": incl_ms, "gbs": 8 * n / incl_ms / 1e6, "frac_of_hbm": 8 * n / incl_ms / 1e6 / peak}}
+    if cpu:
+        import oracle
+        ck, cv = kh.copy(), vh.copy()
+        t0 = time.perf_counter()
+        oracle.lib().orc_sort(ck.ctypes.data, 4, cv.ctypes.data, 4, n)
+        t_sort = time.perf_counter() - t0
+        ce, ci = np.empty_like(xh), np.empty_like(xh)
+        t0 = time.perf_counter()
+        oracle.lib().orc_scan_u32(xh.ctypes.data, ce.ctypes.data, n, 0)
+        t_excl = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        oracle.lib().orc_scan_u32(xh.ctypes.data, ci.ctypes.data, n, 1)
+        t_incl = time.perf_counter() - t0
+        out["bit_exact"] = {
+            "sort": bool(np.array_equal(k.cpu().numpy().view(np.uint32), ck)
+                         and np.array_equal(v.cpu().numpy().view(np.uint32), cv)),
+            "exclusive_sum": bool(np.array_equal(oe.cpu().numpy().view(np.uint32), ce)),
+            "inclusive_sum": bool(np.array_equal(oi.cpu().numpy().view(np.uint32), ci))}
+        out["cpu_baseline"] = {
+            "kind": "port", "cores": 1,
+            "sample": "the same 2^20 keys and values: std::stable_sort of (key, payload) and the serial "
+                      "exclusive / inclusive sum loops, one thread",
+            "sort_mkeys_s": n / t_sort / 1e6, "exclusive_sum_gbs": 8 * n / t_excl / 1e9,
+            "inclusive_sum_gbs": 8 * n / t_incl / 1e9}
+    del flush
+    return out
+
+
 def sortscan(args, dev, peak, rank, cpu=False):
     """Sort and scan extras; with cpu, the oracle's single-thread C++ sort
     (std::stable_sort on (key, payload), the reference test's own oracle) and
@@ -171,7 +249,7 @@ def sortscan(args, dev, peak, rank, cpu=False):
 
     from gprt_b200 import api
     sort_n, scan_n = args.sort_n, args.scan_n
-    out = {}
+    out = {"c0": c0_small(args, dev, peak, cpu)}
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     # sort: Zipf(1.1) uint32 keys, payload = index
     k0 = zipf_keys(sort_n, 7 + rank)
@@ -304,38 +382,58 @@ def whole_job_rate(units_per_rank, ms_per_step, world):
     return world * units_per_rank / (ms_per_step * 1e-3) / 1e6
 
 
-def cpu_sample_run(sample):
-    """The CPU oracle (test infrastructure) over a list of (pos, tri, rays)
-    meshes: a full build and a closest-hit trace of every mesh.  Returns
-    (seconds building, seconds tracing, triangles, rays)."""
+def cpu_sample_run(sample, match=None):
+    """The CPU oracle (test infrastructure) over a list of (pos, tri, rays[,
+    gpu_hits]) meshes: a full build and a closest-hit trace of every mesh.
+    Returns (seconds building, seconds tracing, triangles, rays).  With a
+    `match` dict and GPU hits in the sample, the oracle's hits are compared
+    with them (ids on every ray, t bits on every hit) and the counts added to
+    `match`; the comparison is outside the timed parts."""
     import oracle
     tb = tt = 0.0
     ntri = nray = 0
-    for pos, tri, rays in sample:
+    for item in sample:
+        pos, tri, rays = item[:3]
         t0 = time.perf_counter()
         e = oracle.lbvh_build_tri(pos, tri)
         t1 = time.perf_counter()
-        oracle.trace_lbvh(pos, tri, e, rays)
+        exp = oracle.trace_lbvh(pos, tri, e, rays)
         t2 = time.perf_counter()
         tb += t1 - t0
         tt += t2 - t1
         ntri += tri.shape[0]
         nray += rays.shape[0]
+        if match is not None and len(item) > 3:
+            got = item[3]
+            gp = np.ascontiguousarray(got[:, 0]).view(np.uint32)
+            hit = exp["prim"] != 0xFFFFFFFF
+            bad_id = int((gp != exp["prim"]).sum())
+            bad_t = int((np.ascontiguousarray(got[hit, 1]).view(np.uint32)
+                         != np.ascontiguousarray(exp["t"][hit]).view(np.uint32)).sum())
+            match["meshes"] += 1
+            match["rays"] += int(rays.shape[0])
+            match["hits"] += int(hit.sum())
+            match["id_mismatches"] += bad_id
+            match["t_mismatches"] += bad_t
     return tb, tt, ntri, nray
 
 
-def cpu_baseline(min_tris, meshes, triangles):
+def cpu_baseline(sample, meshes):
+    """The oracle timed on the first meshes of the headline workload (copied
+    from the device), and its hits compared with the GPU's for those meshes."""
     import oracle
-    from gprt_b200 import workloads
     oracle.lib()
-    sample = workloads.large_cpu_sample(min_tris, meshes=meshes, n=triangles)
     cpu_sample_run(sample[:1])  # warm-up
-    tb, tt, ntri, nray = cpu_sample_run(sample)
+    match = {"meshes": 0, "rays": 0, "hits": 0, "id_mismatches": 0, "t_mismatches": 0}
+    tb, tt, ntri, nray = cpu_sample_run(sample, match)
+    match["match"] = match["id_mismatches"] == 0 and match["t_mismatches"] == 0 and match["rays"] > 0
+    match["compared"] = ("the oracle's FP32 LBVH build + closest-hit traversal of each mesh against the "
+                         "batched + quantised step's hits: primitive id of every ray, t bits of every hit")
     return {"value": nray / (tb + tt) / 1e6, "unit": "Mrays/s", "cores": oracle.num_threads(), "kind": "port",
-            "sample": "first %d of %d meshes of the same workload (%d triangles, %d rays), regenerated on the "
-                      "host; per mesh a full LBVH build and a closest-hit trace of its rays"
+            "sample": "first %d of %d meshes of the same workload (%d triangles, %d rays), copied from the "
+                      "device; per mesh a full LBVH build and a closest-hit trace of its rays"
                       % (len(sample), meshes, ntri, nray),
-            "build_mprims_s": ntri / tb / 1e6, "trace_mrays_s": nray / tt / 1e6}
+            "build_mprims_s": ntri / tb / 1e6, "trace_mrays_s": nray / tt / 1e6}, match
 
 
 def run_reference(args, world, rank):
@@ -466,6 +564,9 @@ def run_b200(args, world, rank, local):
     same_q = bool(torch.equal(sc.h_plain, sc.h_q)) if plain_ms is not None else bool(torch.equal(sc.h_bat, sc.h_q))
     hit_fraction = float((sc.h_q[:, 0] != -1).float().mean().item())
     tchk = t_check(sc)
+    # the first meshes exactly as built and traced, for the CPU oracle (its
+    # timing and its hit comparison) once the GPU work is done
+    cpu_sample = sc.host_sample(args.cpu_tris) if rank == 0 and world == 1 and not args.skip_cpu else None
     plain_launches = None
     if plain_ms is not None:
         plain_launches, _ = launches.count_kernels(lambda: sc.plain_mesh(0, torch.cuda.current_stream().cuda_stream))
@@ -536,9 +637,10 @@ def run_b200(args, world, rank, local):
     barrier()
 
     if rank == 0:
-        cb = None
-        if world == 1 and not args.skip_cpu:
-            cb = cpu_baseline(args.cpu_tris, args.meshes, args.triangles)
+        cb = om = None
+        if cpu_sample is not None:
+            cb, om = cpu_baseline(cpu_sample, meshes)
+            del cpu_sample
         achieved = TRACE_BYTES_PER_RAY * nrays / (trace_ms * 1e-3) / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
@@ -548,12 +650,14 @@ def run_b200(args, world, rank, local):
                        "triangles_per_gpu": ntri, "meshes_per_gpu": meshes,
                        "rays_per_gpu": nrays, "l2": "flushed (256 MB write) between timed steps",
                        "parallelism": "independent scene per GPU" if world > 1 else "single GPU"},
-            "roofline": {"kernel": "k_trace_wide (closest hit, batched)", "bound": "hbm", "achieved": achieved,
-                         "peak": peak, "peak_kind": peak_kind + " hbm_gbs (copy)", "unit": "GB/s",
-                         "frac": achieved / peak,
-                         "traffic": TRACE_WIDE_DRAM_BYTES if (ntri, meshes) == (67_108_864, 16_384) else None,
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one full-size "
-                                           "launch (profiles/k_trace_wide_large.md)",
+            "roofline": {"kernel": "k_trace_wide (closest hit, batched)", "bound": "hbm",
+                         "limiter": "instruction issue (divergent per-ray traversal), not DRAM bandwidth: the HBM "
+                                    "roofline is the denominator of frac, not what limits the kernel",
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind + " hbm_gbs (copy)",
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None,
+                         "traffic_source": "not measured by this run (CUDA events give time, not DRAM bytes); "
+                                           "taken from ncu captures of this kernel",
                          "algorithmic_bytes": "40 B/ray (32 B ray in + 8 B hit out) x %d rays per launch" % nrays,
                          "launch_ms": trace_ms},
             "build": {"value": ntri / (build_ms * 1e-3) / 1e6, "unit": "Mprims/s", "ms": build_ms,
@@ -579,9 +683,13 @@ def run_b200(args, world, rank, local):
                                     "source": "kernel nodes of the replayed CUDA graph"},
             "clocks": clocks,
             "cpu_baseline": cb,
+            "oracle_match": om,
         }
         line.update(extra)
         print(json.dumps(line), flush=True)
+        if om is not None and not om["match"]:
+            sys.stderr.write("bench: the GPU hits differ from the oracle's on the CPU sample: %s\n" % json.dumps(om))
+            sys.exit(3)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

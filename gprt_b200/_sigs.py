@@ -57,6 +57,9 @@ SIGNATURES = {
     "gprtcuGenRays": ([u64, u64, vp, u32, vp, vp, vp], st),
     "gprtcuDebugSetSpinBudget": ([u32], None),
     "gprtcuDebugScanSkipTile": ([i64], None),
+    "gprtcuDebugScanSkipStage": ([i64], None),
+    "gprtcuDebugSortSkipTile": ([i64], None),
+    "gprtcuDebugRefitSkipLeaf": ([i64], st),
     "gprtcuDebugScanImpl": ([i32], None),
 }
 

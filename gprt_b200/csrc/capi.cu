@@ -19,12 +19,32 @@ extern "C" GPRTCU_API const char *gprtcuStatusString(int status) {
 
 extern "C" GPRTCU_API int gprtcuVersion(void) { return 100; }
 
+void *gprtcu_noalloc_state(void);  // scan.cu
+
+// A null scratch reads the header of the fixed array that
+// gprtcuExclusiveSumU32NoAlloc uses on the current device.
 extern "C" GPRTCU_API gprtcuStatus gprtcuScratchStatus(const void *scratch, gprtcuStream stream, int *deviceStatus) {
-  if (!scratch || !deviceStatus) return GPRTCU_ERR_INVALID_ARG;
+  if (!deviceStatus) return GPRTCU_ERR_INVALID_ARG;
+  if (!scratch) scratch = gprtcu_noalloc_state();
+  if (!scratch) return GPRTCU_ERR_CUDA;
   uint32_t v = 0;
   GPRTCU_TRY(cudaMemcpyAsync(&v, scratch, sizeof(v), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
   GPRTCU_TRY(cudaStreamSynchronize((cudaStream_t)stream));
   *deviceStatus = (int)v;
+  return GPRTCU_OK;
+}
+
+// Folds a scratch buffer's status word into *acc (first error wins), on the
+// stream, without synchronising: the compat layer's asynchronous calls read
+// *acc at their next synchronisation point.  acc may be mapped host memory.
+__global__ void k_fold_status(const uint32_t *status, uint32_t *acc) {
+  const uint32_t v = *(volatile const uint32_t *)status;
+  if (v && *(volatile uint32_t *)acc == 0u) *(volatile uint32_t *)acc = v;
+}
+
+gprtcuStatus gprtcu_fold_status(const void *scratch, uint32_t *acc, cudaStream_t stream) {
+  k_fold_status<<<1, 1, 0, stream>>>((const uint32_t *)scratch, acc);
+  GPRTCU_TRY(cudaGetLastError());
   return GPRTCU_OK;
 }
 

@@ -198,7 +198,13 @@ __device__ __forceinline__ void named_bar_sync(int id, int threads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
 }
 
-constexpr uint32_t MBAR_WAIT_BUDGET = 1u << 26;
+// Polls an mbarrier wait makes before it gives up: 16 for every poll of the
+// look-back budget the call was given (2^26 at the default 2^22), so a test
+// that shortens the look-back budget shortens these waits too.  A try_wait
+// poll itself suspends the thread for a while, so 2^26 polls are seconds.
+__device__ __forceinline__ uint32_t mbar_budget_of(uint32_t lookback_budget) {
+  return lookback_budget >= (1u << 28) ? 0xFFFFFFFFu : lookback_budget << 4;
+}
 
 }  // namespace gprtcu
 

@@ -20,8 +20,11 @@ struct GPRTContext_T {
   int device;
   cudaStream_t stream;
   uint32_t *d_word;  // device word for totals
-  uint32_t *h_word;  // pinned host word
+  uint32_t *h_word;  // pinned host words: [0] totals, [1] pending device status of asynchronous sorts
+  uint32_t *h_word_dev;  // device view of h_word
 };
+
+gprtcuStatus gprtcu_fold_status(const void *scratch, uint32_t *acc, cudaStream_t stream);  // capi.cu
 
 struct GPRTBuffer_T {
   GPRTContext ctx;
@@ -59,21 +62,35 @@ extern "C" GPRTCU_API GPRTContext gprtContextCreate(int32_t *requestedDeviceIDs,
     compat_error(GPRTCU_ERR_CUDA, "gprtContextCreate: cudaSetDevice");
     return nullptr;
   }
-  GPRTContext c = new (std::nothrow) GPRTContext_T{dev, nullptr, nullptr, nullptr};
+  GPRTContext c = new (std::nothrow) GPRTContext_T{dev, nullptr, nullptr, nullptr, nullptr};
   if (!c) return nullptr;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMalloc(&c->d_word, 256) != cudaSuccess || cudaMallocHost(&c->h_word, 256) != cudaSuccess) {
+      cudaMalloc(&c->d_word, 256) != cudaSuccess ||
+      cudaHostAlloc((void **)&c->h_word, 256, cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer((void **)&c->h_word_dev, c->h_word, 0) != cudaSuccess) {
     compat_error(GPRTCU_ERR_CUDA, "gprtContextCreate: stream / work words");
     delete c;
     return nullptr;
   }
+  std::memset(c->h_word, 0, 256);
   return c;
+}
+
+// After a synchronisation of the context's stream: reports a device-side
+// error that an earlier asynchronous sort (caller scratch) recorded.
+static void report_pending(GPRTContext c) {
+  const uint32_t st = ((volatile uint32_t *)c->h_word)[1];
+  if (st) {
+    ((volatile uint32_t *)c->h_word)[1] = 0;
+    compat_error((int)st, "gprtBufferSort / gprtBufferSortPayload (an earlier call on this context)");
+  }
 }
 
 extern "C" GPRTCU_API void gprtContextDestroy(GPRTContext c) {
   if (!c) return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  report_pending(c);
   cudaFree(c->d_word);
   cudaFreeHost(c->h_word);
   cudaStreamDestroy(c->stream);
@@ -172,6 +189,7 @@ extern "C" GPRTCU_API void gprtBufferMap(GPRTBuffer b, int d) {
   if (!b) return;
   cudaSetDevice(b->ctx->device);
   cudaStreamSynchronize(b->ctx->stream);
+  report_pending(b->ctx);
   if (b->kind != 0) return;
   void *h = gprtBufferGetHostPointer(b, d);
   if (h && b->bytes) cudaMemcpy(h, b->dptr, b->bytes, cudaMemcpyDeviceToHost);
@@ -283,6 +301,7 @@ static uint32_t scan_family(GPRTContext c, GPRTBuffer in, GPRTBuffer out, GPRTBu
     cudaStreamSynchronize(c->stream);
     total = *c->h_word;
   }
+  report_pending(c);
   put_work(c, w);
   return total;
 }
@@ -332,6 +351,11 @@ extern "C" GPRTCU_API void gprtcuCompatSort(GPRTContext c, GPRTBuffer keys, int 
   // asynchronous, like the reference's compute submission; temporary work
   // space is freed after the stream drains, so its status is read then
   else if (w.temp) device_status_ok(c, w.ptr, what);
+  // with the caller's scratch the call stays asynchronous: the status word is
+  // folded into a host word on the stream and reported at the next
+  // synchronisation (gprtBufferMap, a sum / partition / select, destroy)
+  else if (gprtcu_fold_status(w.ptr, c->h_word_dev + 1, c->stream) != GPRTCU_OK)
+    compat_error(GPRTCU_ERR_CUDA, what);
   put_work(c, w);
 }
 

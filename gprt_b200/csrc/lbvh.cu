@@ -290,9 +290,9 @@ __device__ __forceinline__ uint32_t code_at(const uint32_t *codes, const uint64_
 }
 template <bool BATCHED>
 __device__ __forceinline__ int kdelta(const uint32_t *codes, const uint64_t *keys, uint64_t base, int64_t n, int64_t i,
-                                      uint32_t ci, int64_t j) {
+                                      uint32_t ci, int64_t j, uint32_t cmask) {
   if (j < 0 || j >= n) return -1;
-  const uint32_t x = ci ^ code_at<BATCHED>(codes, keys, base + j);
+  const uint32_t x = (ci ^ code_at<BATCHED>(codes, keys, base + j)) & cmask;
   if (x == 0) return __clz((uint32_t)i ^ (uint32_t)j) + 32;
   return __clz(x);
 }
@@ -301,9 +301,14 @@ __device__ __forceinline__ int kdelta(const uint32_t *codes, const uint64_t *key
 // 287-338), one thread per inner node, mesh-local indices.  Writes {left,
 // right, -, -1} of the node, the parent field of both children, and the child
 // references of the traversal node (inner child c -> c, leaf k -> ~k).
+// If the sort before it gave up on a wait (sort_status non-zero), the codes
+// are not sorted and could give overlapping ranges; every code then counts as
+// equal, so the index tie-break alone shapes a valid tree and nothing after it
+// reads out of bounds (the build reports the sort's error).
 template <bool BATCHED>
 __global__ void __launch_bounds__(256) k_karras(const uint32_t *codes, const uint64_t *keys, MeshMap mm, int4 *nodes,
-                                                Bvh2Node *bvh) {
+                                                Bvh2Node *bvh, const uint32_t *sort_status) {
+  const uint32_t cmask = sort_status && ld_relaxed_u32(sort_status) != 0 ? 0u : 0xFFFFFFFFu;
   const uint64_t total_inner = (uint64_t)mm.n - mm.meshes;
   for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total_inner;
        g += (uint64_t)gridDim.x * blockDim.x) {
@@ -313,7 +318,7 @@ __global__ void __launch_bounds__(256) k_karras(const uint32_t *codes, const uin
     const uint64_t inner_base = b - m, node_base = 2 * b - m;
     const int64_t i = (int64_t)(g - inner_base);
     const uint32_t ci = code_at<BATCHED>(codes, keys, b + i);
-#define KD(j) kdelta<BATCHED>(codes, keys, b, N, i, ci, (j))
+#define KD(j) kdelta<BATCHED>(codes, keys, b, N, i, ci, (j), cmask)
     const int d = KD(i + 1) >= KD(i - 1) ? 1 : -1;
     const int dmin = KD(i - d);
     int64_t lmax = 2;
@@ -383,16 +388,32 @@ __device__ __forceinline__ bool refit_read_box(const float2 *o2, float *sb) {
   }
   return ready;
 }
+// Test hooks (set on the current device by gprtcuDebugRefitSkipLeaf and
+// gprtcuDebugSetSpinBudget): the leaf in sorted slot c_refit_skip never
+// stores its box, and the polls a second arrival makes before it gives up.
+__constant__ int64_t c_refit_skip = -1;
+__constant__ uint32_t c_refit_budget = DEFAULT_SPIN_BUDGET;
+
 template <int KIND, bool BATCHED>
 __global__ void __launch_bounds__(256) k_refit(const float *pos, const uint32_t *tri, const uint32_t *ids,
                                                const uint64_t *keys, MeshMap mm, int4 *nodes, float *aabbs,
                                                Bvh2Node *bvh, float4 *leaf_tris, uint32_t *codes_out,
-                                               uint32_t *arrivals, float *root_box) {
+                                               uint32_t *arrivals, float *root_box, const uint32_t *sort_status) {
   const uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (s >= mm.n) return;
+  // The scratch header sits a fixed distance before the arrival counters.
+  auto lbvh_header = [&]() {
+    const size_t slots = ((size_t)mm.meshes * 24 + 255) & ~(size_t)255;
+    return reinterpret_cast<ScratchHeader *>(reinterpret_cast<char *>(arrivals) - slots - sizeof(ScratchHeader));
+  };
+  // A sort that gave up on a wait leaves ids (and keys) that are not a
+  // permutation: each leaf then takes its own slot's primitive, so every read
+  // stays in bounds, and the build reports the sort's error.
+  const uint32_t sort_err = sort_status ? ld_relaxed_u32(sort_status) : 0u;
+  if (sort_err && s == 0) record_error(lbvh_header(), sort_err);
   uint32_t m = 0;
   if (BATCHED) {
-    if (keys) {
+    if (keys && !sort_err) {
       const uint64_t key = keys[s];  // (mesh << 32 | code), sorted
       m = (uint32_t)(key >> 32);
       if (codes_out) codes_out[s] = (uint32_t)key;
@@ -404,7 +425,8 @@ __global__ void __launch_bounds__(256) k_refit(const float *pos, const uint32_t 
   const int64_t N = BATCHED ? mm.count(m) : mm.n;
   const uint64_t inner_base = b - m, node_base = 2 * b - m;
   const int64_t i = (int64_t)(s - b);
-  const uint32_t id = ids[s];
+  const uint32_t id = sort_err ? (uint32_t)i : ids[s];
+  const bool hooked = (int64_t)s == c_refit_skip;
   float v[9], bx[6];
   prim_box<KIND>(pos, tri, b + id, v, bx);
   if (leaf_tris) {
@@ -428,7 +450,9 @@ __global__ void __launch_bounds__(256) k_refit(const float *pos, const uint32_t 
     // This child's box goes into its slot of the parent's traversal node (or
     // is already in the reference-layout array); the release half of the
     // arrival count publishes it.
-    if (bvh) {
+    // (a hooked leaf, at its first step, leaves its slot unwritten)
+    const bool skip_store = hooked && child == leaf;
+    if (bvh && !skip_store) {
       float2 *cb = reinterpret_cast<float2 *>(bvh[inner_base + p].box + 6 * side);
       cb[0] = make_float2(bx[0], bx[1]);
       cb[1] = make_float2(bx[2], bx[3]);
@@ -442,19 +466,18 @@ __global__ void __launch_bounds__(256) k_refit(const float *pos, const uint32_t 
     }
     // Second arrival: read the sibling's box from L2 and form the union,
     // starting from +-1e38 exactly as MakeNodes initialises inner boxes.
+    // (A hooked leaf arriving second waits on its own unwritten slot, so the
+    // wait below runs out whichever child arrives first.)
     const int64_t sib = side == 0 ? pn.y : pn.x;
-    const float *ob = bvh ? bvh[inner_base + p].box + 6 * (1 - side) : aabbs + 6 * (node_base + sib);
+    const int rd = skip_store ? side : 1 - side;
+    const float *ob = bvh ? bvh[inner_base + p].box + 6 * rd : aabbs + 6 * (node_base + sib);
     float sb[6];
     if (bvh) {
       // bounded wait for the sibling's stores; a wait that runs out records
-      // GPRTCU_ERR_TIMEOUT in the scratch header, which sits a fixed distance
-      // before the arrival counters
+      // GPRTCU_ERR_TIMEOUT in the scratch header
       for (uint32_t spin = 0; !refit_read_box(reinterpret_cast<const float2 *>(ob), sb); ++spin)
-        if (spin == DEFAULT_SPIN_BUDGET) {
-          const size_t slots = ((size_t)mm.meshes * 24 + 255) & ~(size_t)255;
-          record_error(reinterpret_cast<ScratchHeader *>(reinterpret_cast<char *>(arrivals) - slots -
-                                                         sizeof(ScratchHeader)),
-                       GPRTCU_ERR_TIMEOUT);
+        if (spin == c_refit_budget) {
+          record_error(lbvh_header(), GPRTCU_ERR_TIMEOUT);
           break;
         }
     } else {
@@ -516,7 +539,7 @@ int ceil_log2(uint32_t v) {
 
 template <int KIND, bool BATCHED>
 void launch_build(const float *pos, const uint32_t *tri, MeshMap mm, int codeKind, gprtcuLbvh *out, uint32_t *slots,
-                  uint64_t *keys, uint32_t *arrivals, cudaStream_t stream, int stage) {
+                  uint64_t *keys, uint32_t *arrivals, const uint32_t *sort_status, cudaStream_t stream, int stage) {
   const int g = grid_for(mm.n, 256, 8);
   int4 *nodes = (int4 *)out->nodes;
   if (stage == 0) {
@@ -526,12 +549,13 @@ void launch_build(const float *pos, const uint32_t *tri, MeshMap mm, int codeKin
   } else {
     if (mm.n > mm.meshes)
       k_karras<BATCHED><<<(unsigned)((mm.n - mm.meshes + 255) / 256), 256, 0, stream>>>(out->codes, keys, mm, nodes,
-                                                                                         (Bvh2Node *)out->bvh2);
+                                                                                         (Bvh2Node *)out->bvh2,
+                                                                                         sort_status);
     // traversal nodes for triangles and user-primitive boxes; leaf-order
     // triangles for triangles only
     k_refit<KIND, BATCHED><<<(unsigned)((mm.n + 255) / 256), 256, 0, stream>>>(
         pos, tri, out->ids, keys, mm, nodes, out->aabbs, (KIND == 0 || KIND == 3) ? (Bvh2Node *)out->bvh2 : nullptr,
-        KIND == 0 ? (float4 *)out->leafTris : nullptr, out->codes, arrivals, out->rootBox);
+        KIND == 0 ? (float4 *)out->leafTris : nullptr, out->codes, arrivals, out->rootBox, sort_status);
   }
 }
 
@@ -559,6 +583,7 @@ gprtcuStatus lbvh_build(int kind, const float *pos, const uint32_t *tri, const u
   uint64_t *keys = meshes > 1 ? (uint64_t *)(s + L.keys) : nullptr;
   const MeshMap mm{meshes > 1 ? prim_off : nullptr, meshes, n};
   const bool batched = meshes > 1;
+  const uint32_t *sort_status = (const uint32_t *)(s + L.sort);  // the sort's own header: its error status first
   for (int stage = 0; stage < 2; ++stage) {
     if (stage == 1) {
       gprtcuStatus st = batched ? gprtcuSortPairsU64(keys, out->ids, n, 0, 32 + (ceil_log2(meshes) > 0 ? ceil_log2(meshes) : 1),
@@ -567,12 +592,12 @@ gprtcuStatus lbvh_build(int kind, const float *pos, const uint32_t *tri, const u
                                                      (gprtcuStream)stream);
       if (st != GPRTCU_OK) return st;
     }
-    if (kind == 0 && batched) launch_build<0, true>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
-    else if (kind == 0) launch_build<0, false>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
-    else if (kind == 2) launch_build<2, false>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
-    else if (kind == 3) launch_build<3, false>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
-    else if (batched) launch_build<1, true>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
-    else launch_build<1, false>(pos, tri, mm, codeKind, out, slots, keys, arrivals, stream, stage);
+    if (kind == 0 && batched) launch_build<0, true>(pos, tri, mm, codeKind, out, slots, keys, arrivals, sort_status, stream, stage);
+    else if (kind == 0) launch_build<0, false>(pos, tri, mm, codeKind, out, slots, keys, arrivals, sort_status, stream, stage);
+    else if (kind == 2) launch_build<2, false>(pos, tri, mm, codeKind, out, slots, keys, arrivals, sort_status, stream, stage);
+    else if (kind == 3) launch_build<3, false>(pos, tri, mm, codeKind, out, slots, keys, arrivals, sort_status, stream, stage);
+    else if (batched) launch_build<1, true>(pos, tri, mm, codeKind, out, slots, keys, arrivals, sort_status, stream, stage);
+    else launch_build<1, false>(pos, tri, mm, codeKind, out, slots, keys, arrivals, sort_status, stream, stage);
     GPRTCU_TRY(cudaGetLastError());
   }
   return GPRTCU_OK;
@@ -637,11 +662,11 @@ extern "C" GPRTCU_API gprtcuStatus gprtcuLbvhRefitTriangles(const float *positio
   if (numMeshes > 1)
     k_refit<0, true><<<grid, 256, 0, stream>>>(positions, triangles, bvh->ids, nullptr, mm, (int4 *)bvh->nodes,
                                                bvh->aabbs, (Bvh2Node *)bvh->bvh2, (float4 *)bvh->leafTris, nullptr,
-                                               arrivals, bvh->rootBox);
+                                               arrivals, bvh->rootBox, nullptr);
   else
     k_refit<0, false><<<grid, 256, 0, stream>>>(positions, triangles, bvh->ids, nullptr, mm, (int4 *)bvh->nodes,
                                                 bvh->aabbs, (Bvh2Node *)bvh->bvh2, (float4 *)bvh->leafTris, nullptr,
-                                                arrivals, bvh->rootBox);
+                                                arrivals, bvh->rootBox, nullptr);
   GPRTCU_TRY(cudaGetLastError());
   return GPRTCU_OK;
 }
@@ -656,4 +681,15 @@ extern "C" GPRTCU_API gprtcuStatus gprtcuBatchBuildTriangles(const float *positi
                                                              void *scratch, size_t scratchBytes, gprtcuStream stream) {
   return lbvh_build(0, positions, triangles, triOffsets, numMeshes, totalTriangles, codeKind, bvh, scratch,
                     scratchBytes, (cudaStream_t)stream);
+}
+
+extern "C" GPRTCU_API gprtcuStatus gprtcuDebugRefitSkipLeaf(int64_t slot) {
+  GPRTCU_TRY(cudaMemcpyToSymbol(c_refit_skip, &slot, sizeof(slot)));
+  return GPRTCU_OK;
+}
+
+// Called by gprtcuDebugSetSpinBudget (scan.cu): the refit's waits follow it.
+gprtcuStatus gprtcu_refit_set_budget(uint32_t polls) {
+  GPRTCU_TRY(cudaMemcpyToSymbol(c_refit_budget, &polls, sizeof(polls)));
+  return GPRTCU_OK;
 }

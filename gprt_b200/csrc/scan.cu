@@ -271,14 +271,18 @@ __global__ void __launch_bounds__(WARPS * 32) k_scan_tma(const uint32_t *in, uin
       mbar_arrive_expect_tx(&bar, TILE_BYTES);
       bulk_g2s(buf, in + tile_start, TILE_BYTES, &bar);
     }
-    if (!mbar_wait(&bar, 0, MBAR_WAIT_BUDGET)) s_abort = 1;
+    if (!mbar_wait(&bar, 0, mbar_budget_of(budget))) s_abort = 1;
   } else {
     uint32_t *sb = reinterpret_cast<uint32_t *>(buf);
     for (int i = tid; i < TILE; i += THREADS) sb[i] = tile_start + i < n ? in[tile_start + i] : 0u;
   }
   __syncthreads();
   if (s_abort) {
-    if (tid == 0) record_error(hdr, GPRTCU_ERR_TIMEOUT);
+    if (tid == 0) {
+      record_error(hdr, GPRTCU_ERR_TIMEOUT);
+      // the copy must land before this CTA's shared memory is released
+      mbar_wait(&bar, 0, mbar_budget_of(budget));
+    }
     return;
   }
   // Warp w owns rows [w*TS_ROWS, (w+1)*TS_ROWS); row r is 32 lanes x uint4.
@@ -410,7 +414,7 @@ template <int MODE>
 __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *in, uint32_t *out, uint64_t n,
                                                                uint64_t ntiles, ScratchHeader *hdr, uint64_t *status,
                                                                uint32_t *d_total, uint32_t budget, int64_t skip_tile,
-                                                               uint32_t want_neg) {
+                                                               uint32_t want_neg, int64_t skip_stage) {
   constexpr int RS = RR_RS, SS = RR_SS, PQ = RR_PQ, SW = RR_SCAN_WARPS;
   constexpr uint32_t TILE = SCAN_TILE, TB = SCAN_TILE * 4;
   static_assert(PQ % 2 == 0, "pending slot q always belongs to look-back warp q % 2");
@@ -422,6 +426,7 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
   __shared__ uint32_t r_tile[RS], s_tile[SS];
   __shared__ volatile uint32_t s_scan_stop;  // a scanner's wait gave up: all scanners leave together
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t mb = mbar_budget_of(budget);
   unsigned char *rbuf = smem, *sbuf = smem + (size_t)RS * TB;
   if (tid == 0) {
     s_scan_stop = 0;
@@ -457,9 +462,10 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
   };
   if (warp == 0) {
     const uint64_t pol = l2_policy_evict_last();
-    for (uint32_t i = 0;; ++i) {
+    uint32_t i = 0;
+    for (;; ++i) {
       const int s = i % RS;
-      if (i >= RS && !mbar_wait(&r_empty[s], ((i / RS) - 1) & 1, MBAR_WAIT_BUDGET)) break;
+      if (i >= RS && !mbar_wait(&r_empty[s], ((i / RS) - 1) & 1, mb)) break;
       uint32_t t = 0;
       if (lane == 0) t = atomicAdd(&hdr->ticket[0], 1u);
       t = __shfl_sync(FULL_MASK, t, 0);
@@ -470,15 +476,20 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
       }
       load_tile(reinterpret_cast<uint32_t *>(rbuf + (size_t)s * TB), t, &r_full[s], pol);
     }
+    // A wait gave up: the copies of the last RS iterations may still be in
+    // flight and must land before the CTA's shared memory is released.  Only
+    // this warp's own copies advance r_full, so each wait ends as soon as its
+    // copy has landed (or at once, if the stage was consumed already).
+    for (uint32_t j = i > (uint32_t)RS ? i - RS : 0u; j < i; ++j) mbar_wait(&r_full[j % RS], (j / RS) & 1, mb);
   } else if (warp == 1) {
     for (uint32_t i = 0;; ++i) {
       const int s = i % RS, q = i % PQ;
-      if (!mbar_wait(&r_full[s], (i / RS) & 1, MBAR_WAIT_BUDGET)) break;
+      if (!mbar_wait(&r_full[s], (i / RS) & 1, mb)) break;
       const uint32_t t = r_tile[s];
       if (t == RR_END) {
         for (uint32_t j = i; j < i + 2; ++j) {  // one end marker for each look-back warp
           const int qj = j % PQ;
-          if (j >= PQ && !mbar_wait(&p_empty[qj], ((j / PQ) - 1) & 1, MBAR_WAIT_BUDGET)) {
+          if (j >= PQ && !mbar_wait(&p_empty[qj], ((j / PQ) - 1) & 1, mb)) {
             if (lane == 0) record_error(hdr, GPRTCU_ERR_TIMEOUT);
             return;
           }
@@ -525,7 +536,7 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
         mbar_arrive(&r_empty[s]);
         if ((int64_t)t != skip_tile) st_relaxed_u64(&status[t], (t == 0 ? ST_INC : ST_AGG) | agg);
       }
-      if (i >= PQ && !mbar_wait(&p_empty[q], ((i / PQ) - 1) & 1, MBAR_WAIT_BUDGET)) break;
+      if (i >= PQ && !mbar_wait(&p_empty[q], ((i / PQ) - 1) & 1, mb)) break;
       if (lane == 0) {
         pend[q].tile = t;
 #pragma unroll
@@ -535,9 +546,11 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
     }
   } else if (warp < 4) {
     const uint64_t pol = l2_policy_evict_first();
-    for (uint32_t i = warp - 2;; i += 2) {
+    uint32_t i = warp - 2;
+    bool hooked = false;
+    for (;; i += 2) {
       const int q = i % PQ, ss = i % SS;
-      if (!mbar_wait(&p_full[q], (i / PQ) & 1, MBAR_WAIT_BUDGET)) break;
+      if (!mbar_wait(&p_full[q], (i / PQ) & 1, mb)) break;
       const uint32_t t = pend[q].tile;
       uint32_t excl = 0;
       if (t != RR_END) {
@@ -557,7 +570,13 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
           if (d_total) *d_total = excl + agg;
         }
       }
-      if (i >= SS && !mbar_wait(&s_empty[ss], ((i / SS) - 1) & 1, MBAR_WAIT_BUDGET)) break;
+      if (t != RR_END && (int64_t)t == skip_stage) {
+        // Fault injection for tests: the tile's prefix is published, but its
+        // scan stage is never filled, so the scanners' wait on it runs out.
+        hooked = true;
+        break;
+      }
+      if (i >= SS && !mbar_wait(&s_empty[ss], ((i / SS) - 1) & 1, mb)) break;
       if (lane == 0) {
         s_tile[ss] = t;
         if (t != RR_END) pend[q].prefix = excl;
@@ -568,6 +587,11 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
       }
       load_tile(reinterpret_cast<uint32_t *>(sbuf + (size_t)ss * RR_STAGE_BYTES), t, &s_full[ss], pol);
     }
+    // As for the producer: this warp's own copies into its scan stages (its
+    // iterations i-2 and i-4) land before the warp leaves.
+    for (uint32_t back = 2; back <= 4; back += 2)
+      if (i >= back) mbar_wait(&s_full[(i - back) % SS], ((i - back) / SS) & 1, mb);
+    if (hooked) return;
   } else {
     const int w = warp - 4;
     const bool leader = tid == 4 * 32;
@@ -578,7 +602,7 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
       // The scanners meet at named barriers, so none may leave on its own:
       // a warp whose wait gave up raises the flag, and after this barrier
       // all of them see the same flag and the same stage.
-      if (!mbar_wait(&s_full[ss], (i / SS) & 1, MBAR_WAIT_BUDGET)) s_scan_stop = 1;
+      if (!mbar_wait(&s_full[ss], (i / SS) & 1, mb)) s_scan_stop = 1;
       named_bar_sync(1, SW * 32);
       if (s_scan_stop) {
         if (leader) record_error(hdr, GPRTCU_ERR_TIMEOUT);
@@ -868,6 +892,7 @@ using namespace gprtcu;
 
 static uint32_t g_spin_budget = DEFAULT_SPIN_BUDGET;
 static int64_t g_skip_tile = -1;
+static int64_t g_skip_stage = -1;
 // 0: automatic; 1: register tile per CTA; 2: TMA-staged tile per CTA;
 // 3: persistent re-read kernel.  1-3 are test overrides (2 and 3 need
 // 16-byte aligned in/out, else 1 runs).
@@ -879,8 +904,14 @@ static const uint64_t kRereadMinN = 1ull << 20;
 extern "C" GPRTCU_API void gprtcuDebugScanImpl(int impl) { g_scan_impl = impl; }
 
 
-extern "C" GPRTCU_API void gprtcuDebugSetSpinBudget(uint32_t polls) { g_spin_budget = polls ? polls : DEFAULT_SPIN_BUDGET; }
+gprtcuStatus gprtcu_refit_set_budget(uint32_t polls);  // lbvh.cu
+
+extern "C" GPRTCU_API void gprtcuDebugSetSpinBudget(uint32_t polls) {
+  g_spin_budget = polls ? polls : DEFAULT_SPIN_BUDGET;
+  gprtcu_refit_set_budget(g_spin_budget);
+}
 extern "C" GPRTCU_API void gprtcuDebugScanSkipTile(int64_t tile) { g_skip_tile = tile; }
+extern "C" GPRTCU_API void gprtcuDebugScanSkipStage(int64_t tile) { g_skip_stage = tile; }
 uint32_t gprtcu_spin_budget(void) { return g_spin_budget; }
 
 static const uint64_t kScanMaxN = 1ull << 40;
@@ -965,10 +996,10 @@ static gprtcuStatus scan_launch(const uint32_t *in, uint32_t *out, uint64_t n, i
     const unsigned grid = (unsigned)(tiles < (uint64_t)rr_ctas ? tiles : (uint64_t)rr_ctas);
     if (inclusive)
       k_scan_reread<1><<<grid, RR_THREADS, RR_SMEM, stream>>>(in, out, n, tiles, hdr, status, d_total, g_spin_budget,
-                                                             g_skip_tile, 0u);
+                                                             g_skip_tile, 0u, g_skip_stage);
     else
       k_scan_reread<0><<<grid, RR_THREADS, RR_SMEM, stream>>>(in, out, n, tiles, hdr, status, d_total, g_spin_budget,
-                                                             g_skip_tile, 0u);
+                                                             g_skip_tile, 0u, g_skip_stage);
   } else if (impl == 2) {
     // TMA-staged tile-per-CTA kernel (32 KB dynamic shared memory per CTA).
     if (inclusive)
@@ -1023,10 +1054,10 @@ static gprtcuStatus partition_launch(const int32_t *in, int32_t *out, uint64_t n
     const uint32_t want_neg = select_positive ? 0u : 1u;
     if (partition)
       k_scan_reread<2><<<g, RR_THREADS, RR_SMEM, stream>>>((const uint32_t *)in, (uint32_t *)out, n, tiles, hdr, status,
-                                                          d_count, g_spin_budget, -1, want_neg);
+                                                          d_count, g_spin_budget, -1, want_neg, g_skip_stage);
     else
       k_scan_reread<3><<<g, RR_THREADS, RR_SMEM, stream>>>((const uint32_t *)in, (uint32_t *)out, n, tiles, hdr, status,
-                                                          d_count, g_spin_budget, -1, want_neg);
+                                                          d_count, g_spin_budget, -1, want_neg, g_skip_stage);
     GPRTCU_TRY(cudaGetLastError());
     return GPRTCU_OK;
   }
@@ -1078,6 +1109,14 @@ extern "C" GPRTCU_API gprtcuStatus gprtcuSelectI32(const int32_t *in, int32_t *o
 //   so calls ordered on one stream are safe; calls whose work overlaps on the
 //   GPU (different streams, no ordering between them) race on the array and
 //   give wrong results.
+// * Device-side errors: a look-back wait that runs out of its budget records
+//   GPRTCU_ERR_TIMEOUT in the array's header, as it would in a scratch
+//   buffer's.  The caller reads it with gprtcuScratchStatus(NULL, stream,
+//   &status) once the call's work is done on `stream`; the next call clears it.
+// * Device reset: the cached address belongs to the device's current
+//   context.  It is dropped whenever a CUDA call of this entry point fails, so
+//   the call after a failure resolves it again; after cudaDeviceReset, make
+//   one call and ignore its result before relying on the next.
 // * No cudaMalloc, cudaFree or allocating library routine is called.
 // ---------------------------------------------------------------------------
 static const uint64_t kNoAllocMaxN = 1ull << 28;
@@ -1086,15 +1125,24 @@ static __device__ __align__(256) unsigned char g_scan_noalloc_state[kNoAllocByte
 
 #include <mutex>
 
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_ptrs[64] = {nullptr};
+
+static void noalloc_forget(void) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  g_noalloc_ptrs[dev] = nullptr;
+}
+
 static void *noalloc_state_ptr(gprtcuStatus &st) {
-  static std::mutex mu;
-  static void *ptrs[64] = {nullptr};
+  void **ptrs = g_noalloc_ptrs;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
     st = GPRTCU_ERR_CUDA;
     return nullptr;
   }
-  std::lock_guard<std::mutex> lock(mu);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
   if (!ptrs[dev]) {
     void *p = nullptr;
     if (cudaGetSymbolAddress(&p, g_scan_noalloc_state) != cudaSuccess || !p) {
@@ -1113,5 +1161,14 @@ extern "C" GPRTCU_API gprtcuStatus gprtcuExclusiveSumU32NoAlloc(const uint32_t *
   gprtcuStatus st;
   void *state = noalloc_state_ptr(st);
   if (!state) return st;
-  return scan_launch(in, out, n, 0, d_total, state, kNoAllocBytes, (cudaStream_t)stream);
+  st = scan_launch(in, out, n, 0, d_total, state, kNoAllocBytes, (cudaStream_t)stream);
+  if (st == GPRTCU_ERR_CUDA) noalloc_forget();
+  return st;
+}
+
+// Device address of the fixed array on the current device (resolving it on
+// first use), for gprtcuScratchStatus(NULL, ...); NULL if that fails.
+void *gprtcu_noalloc_state(void) {
+  gprtcuStatus st;
+  return noalloc_state_ptr(st);
 }

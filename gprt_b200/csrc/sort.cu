@@ -11,6 +11,9 @@ using namespace gprtcu;
 
 uint32_t gprtcu_spin_budget(void);
 
+static int64_t g_sort_skip_tile = -1;
+extern "C" GPRTCU_API void gprtcuDebugSortSkipTile(int64_t tile) { g_sort_skip_tile = tile; }
+
 namespace {
 
 // Type pairs: 0 u32, 1 u32/u32, 2 u64, 3 u64/u32, 4 u64/u64.
@@ -119,6 +122,7 @@ gprtcuStatus sort_dispatch(int slot, int index, void *keys, void *vals, uint64_t
   a.hdr = (SortHeader *)s;
   a.status = (uint32_t *)(s + L.status);
   a.budget = gprtcu_spin_budget();
+  a.skip_tile = g_sort_skip_tile;
   a.use_bulk = ((((uintptr_t)keys) | ((uintptr_t)a.keys_alt)) & 15) == 0;
   a.sms = gprtcu_num_sms();
   // Zero: header, histograms, trivial flags, both look-back regions.

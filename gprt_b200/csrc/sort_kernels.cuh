@@ -89,6 +89,7 @@ struct SortArgs {
   uint32_t budget;
   int use_bulk;
   int sms;
+  int64_t skip_tile;  // test hook: this tile of every pass never publishes (-1: none)
 };
 
 using SortRunFn = gprtcuStatus (*)(const SortArgs &, cudaStream_t);
@@ -253,6 +254,9 @@ __global__ void __launch_bounds__(WARPS * 32, (PassCfg<K, V, RB, WARPS, ITEMS>::
   constexpr int RADIX = C::RADIX, THREADS = C::THREADS, TILE = C::TILE, WK = C::WARP_KEYS;
   const uint32_t flags = ld_relaxed_u32(&a.trivial[pass]);
   if (flags & SORT_FLAG_TRIVIAL) return;  // every key has the same digit: nothing moves
+  // An earlier pass gave up on a wait: its output is not a permutation of the
+  // keys, so the global digit offsets no longer bound this pass's writes.
+  if (ld_relaxed_u32(&a.hdr->h.status) != 0) return;
 
   extern __shared__ __align__(128) unsigned char smem[];
   K *s_keys = reinterpret_cast<K *>(smem);
@@ -305,12 +309,23 @@ __global__ void __launch_bounds__(WARPS * 32, (PassCfg<K, V, RB, WARPS, ITEMS>::
     // keys fill tile-sorted slots [0, tile_n) and no loop needs a bounds test
     // before the scatter; the top digit's count leaves the padding out.
     for (int i = tid; i < TILE; i += THREADS) s_keys[i] = (uint32_t)i < tile_n ? src_k[tile_start + i] : ~(K)0;
-  } else if (!mbar_wait(&bars[0], 0, MBAR_WAIT_BUDGET)) {
+  } else if (!mbar_wait(&bars[0], 0, mbar_budget_of(a.budget))) {
     s_abort = 1;
   }
+  // On every early return, thread 0 first lets the tile's copies land, so no
+  // copy writes shared memory after the CTA has released it.
+  auto leave = [&]() {
+    if (tid == 0) {
+      record_error(&hdr->h, GPRTCU_ERR_TIMEOUT);
+      if (bulk) {
+        mbar_wait(&bars[0], 0, mbar_budget_of(a.budget));
+        if constexpr (C::HAS_V) mbar_wait(&bars[1], 0, mbar_budget_of(a.budget));
+      }
+    }
+  };
   __syncthreads();
   if (s_abort) {
-    if (tid == 0) record_error(&hdr->h, GPRTCU_ERR_TIMEOUT);
+    leave();
     return;
   }
 
@@ -337,17 +352,21 @@ __global__ void __launch_bounds__(WARPS * 32, (PassCfg<K, V, RB, WARPS, ITEMS>::
   // ---- per digit: tile count, publish, tile-exclusive start, look-back;
   // then each warp's first slot of the digit in the tile-sorted order.
   uint32_t tcount = 0;
+  // Fault injection for tests: the hooked tile never publishes its counts.
+  const bool hooked = (int64_t)tile == a.skip_tile;
   if (tid < RADIX) {
 #pragma unroll 4
     for (int w = 0; w < WARPS; ++w) tcount += s_hist[w * RADIX + tid];
     if ((uint32_t)tid == mask) tcount -= TILE - tile_n;  // padding of the last tile
-    st_relaxed_u32(status + (uint64_t)tile * RADIX + tid, (tile == 0 ? LB_INC : LB_AGG) | tcount);
+    if (!hooked) st_relaxed_u32(status + (uint64_t)tile * RADIX + tid, (tile == 0 ? LB_INC : LB_AGG) | tcount);
   }
   const uint32_t tstart = block_excl_scan_digits<RADIX>(tcount, s_tmp);
   if (tid < RADIX) {
     uint32_t excl = 0;
     bool ok = true;
-    if (tile > 0) {
+    if (hooked) {
+      s_abort = 1;
+    } else if (tile > 0) {
       // Eight predecessors per probe (loads issued together), nearest first:
       // the inclusive prefix of a digit can only advance one probe window per
       // L2 round trip.
@@ -397,7 +416,7 @@ __global__ void __launch_bounds__(WARPS * 32, (PassCfg<K, V, RB, WARPS, ITEMS>::
   }
   __syncthreads();
   if (s_abort) {
-    if (tid == 0) record_error(&hdr->h, GPRTCU_ERR_TIMEOUT);
+    leave();
     return;
   }
 
@@ -420,14 +439,14 @@ __global__ void __launch_bounds__(WARPS * 32, (PassCfg<K, V, RB, WARPS, ITEMS>::
   if constexpr (C::HAS_V) {
     V v[ITEMS];
     if (bulk) {
-      if (!mbar_wait(&bars[1], 0, MBAR_WAIT_BUDGET)) s_abort = 1;
+      if (!mbar_wait(&bars[1], 0, mbar_budget_of(a.budget))) s_abort = 1;
     } else {
       for (int i = tid; i < TILE; i += THREADS)
         if ((uint32_t)i < tile_n) s_vals[i] = src_v[tile_start + i];
     }
     __syncthreads();
     if (s_abort) {
-      if (tid == 0) record_error(&hdr->h, GPRTCU_ERR_TIMEOUT);
+      leave();
       return;
     }
 #pragma unroll

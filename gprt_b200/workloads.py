@@ -277,6 +277,26 @@ class LargeScene:
             done.record()
         torch.cuda.current_stream().wait_event(done)
 
+    def host_sample(self, min_tris, hits=None):
+        """The first meshes up to `min_tris` triangles, copied from the device
+        exactly as they were built and traced: a list of (pos, tri, rays,
+        hits) per mesh, with each mesh's triangles local ([k, 3] indices into
+        its own [3k, 3] positions) and its hits mesh-local (by default those
+        of the batched + quantised step, `h_q`)."""
+        m_end = min(max(int(np.searchsorted(self.off, min_tris)) + 1, 1), self.meshes)
+        t1, r1 = int(self.off[m_end]), int(self.roff[m_end])
+        tri = self.tri[:t1].to(torch.int64).reshape(-1)
+        pos = self.pos.view(-1, 3)[tri].cpu().numpy()
+        rays = self.rays[:r1].cpu().numpy()
+        h = (self.h_q if hits is None else hits)[:r1].cpu().numpy()
+        out = []
+        for m in range(m_end):
+            lo, hi = int(self.off[m]), int(self.off[m + 1])
+            rlo, rhi = int(self.roff[m]), int(self.roff[m + 1])
+            lt = np.arange(3 * (hi - lo), dtype=np.uint32).reshape(-1, 3)
+            out.append((np.ascontiguousarray(pos[3 * lo:3 * hi]), lt, rays[rlo:rhi], h[rlo:rhi]))
+        return out
+
     def release(self):
         self.graph = None
         for k in ("pos", "tri", "batch", "rays", "wide", "h_plain", "h_bat", "h_q", "pscr", "local_tri", "descs",

@@ -48,7 +48,9 @@ GPRTCU_API const char *gprtcuStatusString(int status);
 GPRTCU_API int gprtcuVersion(void);
 
 /* Reads the device-side status word of a scratch buffer after the work that
- * used it has completed on `stream` (synchronises `stream`). */
+ * used it has completed on `stream` (synchronises `stream`).  A NULL scratch
+ * reads the status of the last gprtcuExclusiveSumU32NoAlloc call on the
+ * current device (its fixed array's header). */
 GPRTCU_API gprtcuStatus gprtcuScratchStatus(const void *scratch, gprtcuStream stream, int *deviceStatus);
 
 /* ------------------------------------------------------------------------
@@ -77,7 +79,9 @@ GPRTCU_API gprtcuStatus gprtcuInclusiveSumU32(const uint32_t *in, uint32_t *out,
  * returns GPRTCU_ERR_TOO_LARGE.  The first call on a device resolves the
  * array's device address (make it before any stream capture on that device).
  * All calls share the array: calls ordered on one stream are fine, calls that
- * overlap on the GPU race and give wrong results. */
+ * overlap on the GPU race and give wrong results.  A device-side timeout is
+ * read with gprtcuScratchStatus(NULL, stream, &status) after the call's work
+ * is done; the next call clears it. */
 GPRTCU_API gprtcuStatus gprtcuExclusiveSumU32NoAlloc(const uint32_t *in, uint32_t *out, uint64_t n,
                                                      uint32_t *d_total, gprtcuStream stream);
 
@@ -389,14 +393,31 @@ GPRTCU_API gprtcuStatus gprtcuGenRays(uint64_t numRays, uint64_t seed, const uin
 
 /* ------------------------------------------------------------------------
  * Test hooks (fault injection without a GPU fault).  Process-wide settings
- * read at launch time by the look-back kernels.
- * gprtcuDebugSetSpinBudget: polls a look-back wait makes before it records
- *   GPRTCU_ERR_TIMEOUT (0 restores the default, 2^22).
+ * read at launch time by the kernels that wait.  No counterpart in the
+ * reference, whose waits happen inside the Vulkan driver.
+ * gprtcuDebugSetSpinBudget: polls a look-back wait (scan, sort) or a refit's
+ *   wait for its sibling makes before it records GPRTCU_ERR_TIMEOUT (0
+ *   restores the default, 2^22); the mbarrier waits of the TMA-staged kernels
+ *   get 16 polls for each of these.  The refit's budget is set on the current
+ *   device.
  * gprtcuDebugScanSkipTile: the scan tile with this ticket never publishes its
  *   status (-1 disables), so its successors run out of budget and return.
+ * gprtcuDebugScanSkipStage: in the persistent scan / partition kernel, the
+ *   tile with this ticket publishes its prefix but its scan stage is never
+ *   filled, so the scanner warps' wait runs out and they stop together
+ *   (-1 disables).
+ * gprtcuDebugSortSkipTile: in every pass of a sort, the tile with this ticket
+ *   never publishes its digit counts (-1 disables); later passes see the
+ *   recorded error and do nothing.
+ * gprtcuDebugRefitSkipLeaf: the leaf in this sorted slot never stores its box
+ *   in its parent's traversal node, so the parent's second arrival runs out of
+ *   budget (-1 disables; set on the current device).
  * ------------------------------------------------------------------------ */
 GPRTCU_API void gprtcuDebugSetSpinBudget(uint32_t polls);
 GPRTCU_API void gprtcuDebugScanSkipTile(int64_t tile);
+GPRTCU_API void gprtcuDebugScanSkipStage(int64_t tile);
+GPRTCU_API void gprtcuDebugSortSkipTile(int64_t tile);
+GPRTCU_API gprtcuStatus gprtcuDebugRefitSkipLeaf(int64_t slot);
 /* Scan kernel selection for tests: 0 = automatic (default: the persistent
  * re-read kernel for n >= 2^20 and the TMA-staged tile-per-CTA kernel below,
  * when in/out are 16-byte aligned; else the register-staged kernel),

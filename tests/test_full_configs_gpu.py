@@ -1,7 +1,16 @@
-"""Parity at the full sizes of the batched-build and quantised configurations,
-through properties that do not depend on size (the oracle finishes these
-sizes only on samples):
+"""Parity at the full sizes of the configurations, against the oracle where
+it finishes the size and through size-independent properties and samples
+where it does not:
 
+* plain LBVH, 262,144 triangles (centroids uniform in the unit cube, vertices
+  N(0, 0.002^2) about them) and 1,048,576 rays from a radius-2 sphere: build
+  arrays bit-identical to the oracle's build, every ray's hit id identical to
+  the oracle's FP32 traversal, t within 1e-6 of FP64 on every hit;
+* large combined workload, 67,108,864 triangles of a 256-cluster mixture in
+  16,384 meshes of log-uniform size, 134,217,728 rays: sampled meshes (the
+  smallest, the largest and random ones) built and traced by the oracle from
+  the device's own triangles and rays, build arrays and every hit (ids and t
+  bits) of the batched + quantised step identical;
 * batched build, 4,096 meshes of log-uniform size in [64, 65,536] (about 40M
   triangles), each mesh of the small-LBVH distribution in its own unit cube:
   sampled meshes' arrays bit-identical to the oracle's build of that mesh
@@ -12,7 +21,8 @@ sizes only on samples):
   16,777,216 rays aimed at the unit cube: binary and quantised traversal
   identical on every ray (closest: ids and t bits; any hit: occlusion), ids
   of a seeded sample identical to the oracle's FP32 traversal of the same
-  tree, t within 1e-6 of FP64 on a seeded 1 % of the hits.
+  tree, t within 1e-6 of FP64 on a seeded 1 % of the hits; the whole build
+  bit-identical to the oracle's own build of the 16.7M triangles.
 """
 import numpy as np
 import pytest
@@ -40,6 +50,71 @@ def _t64_check(hits, rays, vert, tri_of_hit, frac=0.01, seed=0):
     t64 = np.einsum("ij,ij->i", v[:, 0] - o, n) / np.einsum("ij,ij->i", d, n)
     t32 = hits[idx, 1].view(np.float32).astype(np.float64)
     return float((np.abs(t32 - t64) / np.abs(t64)).max()), idx.size
+
+
+def _t64_all(hits, rays, v):
+    """Relative error of every hit's t against the FP64 plane distance;
+    v: [k, 3, 3] float64 vertices of the hit triangles."""
+    r = rays.astype(np.float64)
+    o, d = r[:, 0:3], r[:, 4:7]
+    n = np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0])
+    t64 = np.einsum("ij,ij->i", v[:, 0] - o, n) / np.einsum("ij,ij->i", d, n)
+    t32 = np.ascontiguousarray(hits[:, 1]).view(np.float32).astype(np.float64)
+    return np.abs(t32 - t64) / np.abs(t64)
+
+
+def test_plain_lbvh_full_size(cuda):
+    from gprt_b200 import workloads
+    ps = workloads.PlainScene()  # 262,144 triangles, 1,048,576 rays
+    assert (ps.n, ps.nrays) == (262_144, 1_048_576)
+    ps.step()
+    h = ps.bvh.host()
+    e = oracle.lbvh_build_tri(ps.pos_h, ps.tri_h)
+    for k in ("scene", "codes", "ids", "nodes", "aabbs"):
+        assert np.array_equal(_bits(h[k]), _bits(e[k].reshape(h[k].shape))), k
+    got = ps.hits.cpu().numpy()
+    exp = oracle.trace_lbvh(ps.pos_h, ps.tri_h, e, ps.rays_h)
+    assert np.array_equal(np.ascontiguousarray(got[:, 0]).view(np.uint32), exp["prim"])
+    hit = exp["prim"] != 0xFFFFFFFF
+    assert hit.sum() > 100_000
+    assert np.array_equal(np.ascontiguousarray(got[hit, 1]).view(np.uint32), _bits(exp["t"][hit]))
+    v = ps.pos_h[ps.tri_h[exp["prim"][hit]].reshape(-1)].reshape(-1, 3, 3).astype(np.float64)
+    rel = _t64_all(got[hit], ps.rays_h[hit], v)
+    assert rel.max() <= T_REL_TOL, rel.max()
+
+
+def test_large_combined_sampled_meshes_match_oracle(cuda):
+    import torch
+    from gprt_b200 import workloads
+    sc = workloads.LargeScene()  # 67,108,864 triangles, 16,384 meshes, 134,217,728 rays
+    assert (sc.n, sc.meshes, sc.nrays) == (67_108_864, 16_384, 134_217_728)
+    sc.quantised()
+    sc.batched()
+    torch.cuda.synchronize()
+    assert torch.equal(sc.h_q, sc.h_bat)
+    rng = np.random.default_rng(77)
+    sample = sorted({int(np.argmin(sc.sizes)), int(np.argmax(sc.sizes)), 0, sc.meshes - 1}
+                    | set(int(m) for m in rng.choice(sc.meshes, 12, replace=False)))
+    for m in sample:
+        lo, hi = int(sc.off[m]), int(sc.off[m + 1])
+        rlo, rhi = int(sc.roff[m]), int(sc.roff[m + 1])
+        tri = sc.tri[lo:hi].to(torch.int64).reshape(-1)
+        lp = sc.pos.view(-1, 3)[tri].cpu().numpy()
+        lt = np.arange(3 * (hi - lo), dtype=np.uint32).reshape(-1, 3)
+        e = oracle.lbvh_build_tri(lp, lt)
+        h = sc.batch.mesh_host(m)
+        for k in ("scene", "codes", "ids", "nodes"):
+            assert np.array_equal(_bits(h[k]), _bits(e[k].reshape(h[k].shape))), (m, k)
+        rays = sc.rays[rlo:rhi].cpu().numpy()
+        exp = oracle.trace_lbvh(lp, lt, e, rays)
+        got = sc.h_q[rlo:rhi].cpu().numpy()
+        assert np.array_equal(np.ascontiguousarray(got[:, 0]).view(np.uint32), exp["prim"]), m
+        hit = exp["prim"] != 0xFFFFFFFF
+        assert np.array_equal(np.ascontiguousarray(got[hit, 1]).view(np.uint32), _bits(exp["t"][hit])), m
+        if hit.any():
+            v = lp[lt[exp["prim"][hit]].reshape(-1)].reshape(-1, 3, 3).astype(np.float64)
+            assert _t64_all(got[hit], rays[hit], v).max() <= T_REL_TOL, m
+    sc.release()
 
 
 def test_batched_build_full_size(cuda):
@@ -110,3 +185,8 @@ def test_quantised_wide_full_size(cuda):
     worst, k = _t64_check(hb, rays_h, lambda t: pos_h[tri_h[t].reshape(-1)].reshape(-1, 3, 3).astype(np.float64),
                           lambda idx_, prim: prim)
     assert k > 1000 and worst <= T_REL_TOL, worst
+    # the whole 16.7M-triangle build against the oracle's own build
+    h = b.host()
+    e = oracle.lbvh_build_tri(pos_h, tri_h)
+    for k in ("scene", "codes", "ids", "nodes", "aabbs"):
+        assert np.array_equal(_bits(h[k]), _bits(e[k].reshape(h[k].shape))), k

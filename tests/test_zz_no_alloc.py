@@ -46,6 +46,52 @@ def test_no_alloc_matches_scratch_entry_point_on_consecutive_calls(cuda):
         assert int(total.item()) == int(ref_total.item()), n
 
 
+def test_no_alloc_matches_the_oracle(cuda):
+    import torch
+    import oracle
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rng = np.random.default_rng(321)
+    for n in (1, 8191, 8192 * 3 + 1, (1 << 20) + 13):
+        x = rng.integers(0, 256, size=n, dtype=np.uint32)
+        st, out, total = _call_noalloc(torch.from_numpy(x.view(np.int32)).cuda(), stream)
+        assert st == 0
+        torch.cuda.synchronize()
+        exp, etotal = oracle.scan(x)
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), exp), n
+        assert int(total.item()) & 0xFFFFFFFF == etotal, n
+
+
+def _noalloc_status(stream):
+    import gprt_b200
+    v = ctypes.c_int(-1)
+    assert gprt_b200.lib().gprtcuScratchStatus(None, stream, ctypes.byref(v)) == 0
+    return v.value
+
+
+def test_no_alloc_reports_a_device_timeout(cuda):
+    # The fixed array has no address the caller knows, so its status is read
+    # with a NULL scratch.  A tile that never publishes (test hook) makes its
+    # successors' waits run out; the next call clears the status again.
+    import torch
+    import gprt_b200
+    L = gprt_b200.lib()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    x = torch.ones(8192 * 40, dtype=torch.int32, device="cuda")
+    L.gprtcuDebugSetSpinBudget(2000)
+    L.gprtcuDebugScanSkipTile(3)
+    try:
+        st, _, _ = _call_noalloc(x, stream)
+        assert st == 0
+        assert _noalloc_status(stream) == 4
+    finally:
+        L.gprtcuDebugScanSkipTile(-1)
+        L.gprtcuDebugSetSpinBudget(0)
+    st, out, total = _call_noalloc(x, stream)
+    assert st == 0 and _noalloc_status(stream) == 0
+    assert int(total.item()) == x.numel()
+    assert torch.equal(out, torch.arange(x.numel(), dtype=torch.int32, device="cuda"))
+
+
 def test_no_alloc_rejects_sizes_beyond_its_fixed_array(cuda):
     import torch
     import gprt_b200
