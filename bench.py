@@ -42,6 +42,10 @@ The JSON line's value is whole-job Mrays/s of that step.  It also carries:
                 rays, closest and any hit
   spheres, lss  4,194,304 spheres / swept-sphere segments (hair strands):
                 bounds + box LBVH build and closest-hit trace of 4,194,304 rays
+  solids        a volume mesh of 96^3 jittered cubes filled with tetrahedra,
+                pyramids, wedges, hexahedra and tetrahedral pairs (~2.8M
+                cells): cell bounds + box LBVH build, and point location of
+                16,777,216 points; a sample checked against the oracle
   batched_build 4,096 meshes of log-uniform size in [64, 65,536] (~40M
                 triangles, each mesh in its own unit cube): batched build,
                 collapse, and the wide trace of 64 rays per triangle (~2.5G
@@ -622,6 +626,29 @@ def run_b200(args, world, rank, local):
             us = workloads.UserScene(kind, device=dev)
             extra[kind] = us.run(steps=3, warmup=1, flush=flush)
             del us
+        ss = workloads.SolidScene(device=dev)
+        sol = ss.run(steps=3, warmup=1, flush=flush)
+        qms = sol["locate_ms"]
+        sol["roofline"] = {"kernel": "k_locate_solids", "bound": "hbm",
+                           "limiter": "instruction issue (Newton inversion of every candidate cell)",
+                           "achieved": 40 * ss.npts / (qms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                           "frac": 40 * ss.npts / (qms * 1e-3) / 1e9 / peak,
+                           "algorithmic_bytes": "40 B/query (16 B point in, 8 B hit + 16 B rstw out)"}
+        if rank == 0 and world == 1 and not args.skip_cpu:
+            import oracle
+            k = 2000
+            pts, gh, gr = ss.host_sample(k)
+            t0 = time.perf_counter()
+            ec, ek, er = oracle.solid_locate_brute(ss.verts_h, ss.idx_h, ss.types_h, pts)
+            dt = time.perf_counter() - t0
+            sol["oracle_match"] = {"points": k, "cells_equal": bool(np.array_equal(gh[:, 0], ec)),
+                                   "kinds_equal": bool(np.array_equal(gh[:, 1], ek)),
+                                   "rstw_bits_equal": bool(np.array_equal(gr.view(np.uint32), er.view(np.uint32)))}
+            sol["cpu_baseline"] = {"value": k / dt / 1e6, "unit": "Mqueries/s", "cores": oracle.num_threads(),
+                                   "kind": "port", "sample": "%d of the points: every cell's box, then the Newton "
+                                                             "inversion of each cell whose box holds the point" % k}
+        extra["solids"] = sol
+        del ss
         isc = workloads.InstanceScene(device=dev)
         extra["instances"] = isc.run(steps=3, warmup=1, flush=flush)
         del isc

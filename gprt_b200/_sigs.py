@@ -41,6 +41,8 @@ SIGNATURES = {
     "gprtcuLbvhBuildBoxes": ([vp, u32, i32, vp, vp, sz, vp], st),
     "gprtcuTraceSpheres": ([vp, vp, vp, u64, i32, i32, vp, vp, vp, sz, vp], st),
     "gprtcuTraceLss": ([vp, vp, vp, i32, i32, vp, u64, i32, i32, vp, vp, vp, sz, vp], st),
+    "gprtcuSolidBounds": ([vp, vp, vp, vp], st),
+    "gprtcuLocateSolidPoints": ([vp, vp, vp, u64, vp, vp, vp, sz, vp], st),
     "gprtcuInstancesPrepare": ([vp, u32, vp, u32, vp, vp, vp], st),
     "gprtcuTraceInstances": ([vp, vp, vp, vp, vp, u32, vp, u64, u32, i32, vp, vp, vp, sz, vp], st),
     "gprtcuTraceScratchSize": ([], sz),

@@ -351,6 +351,53 @@ def trace_lss(bvh, verts, idx, rays, endcap0=True, endcap1=True, hits=None, u=No
 INSTANCE_DTYPE = [("transform", "<f4", (12,)), ("custom_mask", "<u4"), ("geom_flags", "<u4"), ("blas", "<u8")]
 
 
+# ---------------------------------------------------------------- solid cells
+class SolidsDesc(ctypes.Structure):
+    """gprtcuSolids (include/gprtcu.h)."""
+    _fields_ = [("vertices", ctypes.c_void_p), ("indices", ctypes.c_void_p), ("types", ctypes.c_void_p),
+                ("numCells", ctypes.c_uint32), ("vertexStride", ctypes.c_uint32), ("indexStride", ctypes.c_uint32),
+                ("typeStride", ctypes.c_uint32)]
+
+
+class Solids:
+    """A volume mesh on the device: vertices float32 [V, 4] {x, y, z, density},
+    indices int32/uint32 [C, 8] (unused slots ignored), types uint8 [C]."""
+
+    def __init__(self, vertices, indices, types):
+        _need_cuda(vertices, indices, types)
+        self.vertices, self.indices, self.types = vertices, indices, types
+        self.n = int(types.numel())
+        self.desc = SolidsDesc(_p(vertices), _p(indices), _p(types), self.n, 0, 0, 0)
+
+
+def solid_bounds(solids, aabbs=None, boxes=None):
+    """(aabbs float32 [C, 8] in the reference's layout, boxes float32 [C, 6])."""
+    dev = solids.types.device
+    if aabbs is None:
+        aabbs = torch.empty((solids.n, 8), dtype=torch.float32, device=dev)
+    if boxes is None:
+        boxes = torch.empty((solids.n, 6), dtype=torch.float32, device=dev)
+    _check(lib().gprtcuSolidBounds(ctypes.byref(solids.desc), _ptr(aabbs), _ptr(boxes), _stream()),
+           "gprtcuSolidBounds")
+    return aabbs, boxes
+
+
+def locate_solid_points(bvh, solids, points, hits=None, rstw=None, scr=None):
+    """points float32 [P, 4]; returns (hits int32 [P, 2] {cell, kind}, rstw float32 [P, 4])."""
+    _need_cuda(points)
+    npts = points.shape[0]
+    if hits is None:
+        hits = torch.empty((npts, 2), dtype=torch.int32, device=points.device)
+    if rstw is None:
+        rstw = torch.empty((npts, 4), dtype=torch.float32, device=points.device)
+    if scr is None:
+        scr = scratch(lib().gprtcuTraceScratchSize(), points.device)
+    _check(lib().gprtcuLocateSolidPoints(ctypes.byref(bvh.desc), ctypes.byref(solids.desc), _ptr(points), npts,
+                                         _ptr(hits), _ptr(rstw), _ptr(scr), scr.numel(), _stream()),
+           "gprtcuLocateSolidPoints")
+    return hits, rstw
+
+
 def instances_tensor(records, device="cuda"):
     """Device copy (uint8 [n, 64]) of a numpy array of INSTANCE_DTYPE records."""
     import numpy as np

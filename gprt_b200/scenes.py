@@ -11,6 +11,11 @@ There is no public dataset here: every scene is generated from a seed.
                  centre, directions normalised towards uniform points in the
                  cube; tmin = 0, tmax = +inf.
   * mesh sizes:  log-uniform integer sizes in [lo, hi].
+  * solid_grid(g): a volume mesh of g^3 jittered grid cubes, each cube
+                 filled with one seeded choice of linear cells: a hexahedron,
+                 two wedges, six pyramids on the cube's centre, six
+                 tetrahedra around its main diagonal, or a tetrahedral pair;
+                 per-vertex densities N(0, 1).
 Host-side numpy generation; the arrays are then copied to the device.
 """
 import numpy as np
@@ -155,3 +160,65 @@ def device_rays_range(seed, lo, hi, box_lo, box_hi):
     out[:, 4:7] = d
     out[:, 7] = np.inf
     return out
+
+
+# Corners of a unit cube by (x, y, z) bits, and the cells one cube is split
+# into, as node lists of corner numbers (8 = the cube's centre vertex).  Node
+# orders follow the shape functions of the reference's cells
+# (gprt/gprt_fallbacks.slang:370-406): hexahedron 000 100 110 010 001 101 111
+# 011; wedge = a triangle at t = 0 then the same triangle at t = 1; pyramid =
+# a bilinear base quad, then the apex.
+def _c(x, y, z):
+    return x | (y << 1) | (z << 2)
+
+
+_HEX = [_c(0, 0, 0), _c(1, 0, 0), _c(1, 1, 0), _c(0, 1, 0), _c(0, 0, 1), _c(1, 0, 1), _c(1, 1, 1), _c(0, 1, 1)]
+_WEDGES = [[_c(0, 0, 0), _c(1, 0, 0), _c(0, 1, 0), _c(0, 0, 1), _c(1, 0, 1), _c(0, 1, 1)],
+           [_c(1, 1, 0), _c(0, 1, 0), _c(1, 0, 0), _c(1, 1, 1), _c(0, 1, 1), _c(1, 0, 1)]]
+_FACES = [[_c(0, 0, 0), _c(1, 0, 0), _c(1, 1, 0), _c(0, 1, 0)], [_c(0, 0, 1), _c(0, 1, 1), _c(1, 1, 1), _c(1, 0, 1)],
+          [_c(0, 0, 0), _c(0, 0, 1), _c(1, 0, 1), _c(1, 0, 0)], [_c(0, 1, 0), _c(1, 1, 0), _c(1, 1, 1), _c(0, 1, 1)],
+          [_c(0, 0, 0), _c(0, 1, 0), _c(0, 1, 1), _c(0, 0, 1)], [_c(1, 0, 0), _c(1, 0, 1), _c(1, 1, 1), _c(1, 1, 0)]]
+_PYRAMIDS = [f + [8] for f in _FACES]
+_TETS = []
+for _a, _b in ((0, 1), (0, 2), (1, 0), (1, 2), (2, 0), (2, 1)):
+    _e = [0, 0, 0]
+    _e[_a] = 1
+    _p1 = _c(*_e)
+    _e[_b] = 1
+    _TETS.append([_c(0, 0, 0), _p1, _c(*_e), _c(1, 1, 1)])
+SOLID_FILLS = [(12, [_HEX]), (13, _WEDGES), (14, _PYRAMIDS), (10, _TETS), (23, [_HEX])]
+
+
+def solid_grid(g, seed=0, jitter=0.15, fills=None):
+    """(vertices float32 [V, 4], indices uint32 [C, 8], types uint8 [C]) of a
+    g^3-cube volume mesh over [0, 1]^3: grid vertices jittered by up to
+    `jitter` of the spacing, one extra centre vertex per cube; each cube
+    filled by a seeded choice among SOLID_FILLS (or the given fill indices);
+    unused index slots are 0xFFFFFFFF."""
+    rng = np.random.default_rng(seed)
+    h = 1.0 / g
+    gv = np.stack(np.meshgrid(np.arange(g + 1), np.arange(g + 1), np.arange(g + 1), indexing="ij"), -1)
+    gv = gv.reshape(-1, 3).astype(np.float64) * h + rng.uniform(-jitter, jitter, ((g + 1) ** 3, 3)) * h
+    cc = np.stack(np.meshgrid(np.arange(g), np.arange(g), np.arange(g), indexing="ij"), -1).reshape(-1, 3)
+    centre = (cc + 0.5) * h + rng.uniform(-jitter / 2, jitter / 2, (g ** 3, 3)) * h
+    verts = np.zeros(((g + 1) ** 3 + g ** 3, 4), np.float32)
+    verts[:, :3] = np.concatenate([gv, centre])
+    verts[:, 3] = rng.normal(0.0, 1.0, verts.shape[0])
+    # vertex numbers of each cube's 8 corners and its centre: [g^3, 9]
+    stride = np.array([(g + 1) ** 2, g + 1, 1])
+    corner = np.array([[(k >> 0) & 1, (k >> 1) & 1, (k >> 2) & 1] for k in range(8)])
+    cv = np.concatenate([((cc[:, None, :] + corner[None]) * stride).sum(-1),
+                         ((g + 1) ** 3 + np.arange(g ** 3))[:, None]], axis=1)
+    fill = rng.integers(0, len(SOLID_FILLS), g ** 3) if fills is None else np.resize(np.asarray(fills), g ** 3)
+    idx_parts, type_parts, order = [], [], []
+    for f, (ctype, cells) in enumerate(SOLID_FILLS):
+        cubes = np.nonzero(fill == f)[0]
+        for j, nodes in enumerate(cells):
+            ix = np.full((cubes.size, 8), 0xFFFFFFFF, np.uint32)
+            ix[:, :len(nodes)] = cv[cubes][:, nodes]
+            idx_parts.append(ix)
+            type_parts.append(np.full(cubes.size, ctype, np.uint8))
+            order.append(cubes * 8 + j)
+    # cells numbered cube by cube (a cube's cells consecutive)
+    o = np.argsort(np.concatenate(order), kind="stable")
+    return verts, np.concatenate(idx_parts)[o], np.concatenate(type_parts)[o]

@@ -385,6 +385,55 @@ class UserScene:
                 "hit_fraction": float((self.hits[:, 0] != -1).float().mean().item())}
 
 
+class SolidScene:
+    """A volume mesh of g^3 jittered grid cubes filled with linear cells
+    (hexahedra, wedge pairs, six pyramids, six tetrahedra or a tetrahedral
+    pair per cube; scenes.solid_grid), per-vertex densities N(0, 1); point
+    location of `npts` points uniform in [0, 1]^3: cell bounds + box LBVH
+    build, then the query."""
+
+    def __init__(self, g=96, npts=16_777_216, seed=13, device="cuda"):
+        dev = torch.device(device)
+        self.g, self.npts = g, npts
+        self.verts_h, self.idx_h, self.types_h = scenes.solid_grid(g, seed=seed)
+        self.n = int(self.types_h.size)
+        self.solids = api.Solids(torch.from_numpy(self.verts_h).to(dev),
+                                 torch.from_numpy(self.idx_h.view(np.int32)).to(dev),
+                                 torch.from_numpy(self.types_h).to(dev))
+        gen = torch.Generator(device=dev).manual_seed(seed + 1)
+        self.points = torch.zeros((npts, 4), dtype=torch.float32, device=dev)
+        self.points[:, :3] = torch.rand((npts, 3), generator=gen, device=dev)
+        self.aabbs = torch.empty((self.n, 8), dtype=torch.float32, device=dev)
+        self.boxes = torch.empty((self.n, 6), dtype=torch.float32, device=dev)
+        self.bvh = api.Lbvh(self.n, dev)
+        self.hits = torch.empty((npts, 2), dtype=torch.int32, device=dev)
+        self.rstw = torch.empty((npts, 4), dtype=torch.float32, device=dev)
+        self.tscr = api.scratch(lib().gprtcuTraceScratchSize(), dev)
+
+    def build(self):
+        api.solid_bounds(self.solids, self.aabbs, self.boxes)
+        api.lbvh_build_boxes(self.boxes, self.bvh)
+
+    def locate(self):
+        api.locate_solid_points(self.bvh, self.solids, self.points, self.hits, self.rstw, scr=self.tscr)
+
+    def run(self, steps=3, warmup=1, flush=None):
+        tb = float(np.mean(time_steps(self.build, steps, warmup, flush)))
+        tq = float(np.mean(time_steps(self.locate, steps, warmup, flush)))
+        return {"grid": self.g, "cells": self.n, "vertices": int(self.verts_h.shape[0]),
+                "cell_types": {str(int(t)): int(c) for t, c in zip(*np.unique(self.types_h, return_counts=True))},
+                "points": self.npts, "build_ms": tb, "locate_ms": tq,
+                "build_mcells_s": self.n / tb / 1e3, "locate_mqueries_s": self.npts / tq / 1e3,
+                "found_fraction": float((self.hits[:, 0] != -1).float().mean().item())}
+
+    def host_sample(self, k, seed=0):
+        """k of the query points and the GPU's answers for them (numpy)."""
+        idx = np.sort(np.random.default_rng(seed).choice(self.npts, size=k, replace=False))
+        ti = torch.from_numpy(idx).to(self.points.device)
+        return (self.points[ti].cpu().numpy(), self.hits[ti].cpu().numpy().view(np.uint32),
+                self.rstw[ti].cpu().numpy())
+
+
 class InstanceScene:
     """Two-level scene: a batch of `meshes` bottom-level meshes (Gaussian
     mixture triangles, log-uniform sizes summing to `n`), `instances` placements

@@ -276,6 +276,57 @@ GPRTCU_API gprtcuStatus gprtcuTraceLss(const gprtcuLbvh *bvh, const float *verti
                                        gprtcuStream stream);
 
 /* ------------------------------------------------------------------------
+ * Solid cells (volume-mesh elements) as software-BVH primitives, with point
+ * location.  Replaces gprtSolidsSetVertices / SetIndices / SetTypes +
+ * gprtSolidAccelCreate (gprt/gprt_host.h:552-579,1393) and TracePoint over
+ * that structure (gprt/gprt_builtins.slang:80-90), whose box and point test
+ * are SolidBounds and SolidIntersection (gprt/gprt_fallbacks.slang:467-566).
+ * Cell types are the reference's GPRTSolidTypes (gprt/gprt_host.h:291-298):
+ * 10 tetrahedron (4 vertices), 14 pyramid (5), 13 wedge (6), 12 hexahedron
+ * (8), 23 tetrahedral pair (8 vertices, evaluated as a trilinear cell and
+ * reported with the tetrahedron kind, as the reference does); any other code
+ * is a cell with no vertices that holds no point.  Vertices are float4
+ * {x, y, z, density}; each cell has up to eight uint32 vertex indices (unused
+ * slots are ignored); strides are in bytes (0 selects the reference's
+ * defaults: 16, 32 and 1).  The reference's buffer offsets are applied by
+ * advancing the pointers.
+ *   gprtcuSolidBounds: aabbs (optional) receives two float4 per cell in the
+ *     reference's layout {lo.xyz, hi.x}, {hi.yz, density min, density max};
+ *     boxes (optional) float[6] {lo.xyz, hi.xyz} per cell, the input of
+ *     gprtcuLbvhBuildBoxes.  (The reference's program stores the last
+ *     vertex's density in both density words; these are the minimum and
+ *     maximum its layout documents.)
+ *   gprtcuLocateSolidPoints: for each point (float4, w ignored), the
+ *     lowest-numbered cell whose box holds the point (lo <= p <= hi, as a
+ *     zero-length ray from the point meets it) and whose Newton inversion
+ *     (intersectPointSolid) places it inside the cell; hits {cell, hit kind}
+ *     (0xFFFFFFFF and 0 when none), rstw (optional) float4 (r, s, t,
+ *     interpolated density) per point, zero when none.  The LBVH must be
+ *     built over this set's boxes.  Results are bit-identical to the
+ *     reference's SolidBounds / intersectPointSolid compiled for the host.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+  const float *vertices;    /* float4 {x, y, z, density} per vertex */
+  const uint32_t *indices;  /* up to 8 vertex indices per cell */
+  const uint8_t *types;     /* one cell type per cell */
+  uint32_t numCells;
+  uint32_t vertexStride;    /* bytes between vertices, a multiple of 16 (0: 16) */
+  uint32_t indexStride;     /* bytes between cells' indices, a multiple of 4 (0: 32) */
+  uint32_t typeStride;      /* bytes between types (0: 1) */
+} gprtcuSolids;
+
+typedef struct {
+  uint32_t cell; /* 0xFFFFFFFF: no cell holds the point */
+  uint32_t kind; /* hit kind: 10 tetrahedron, 12 hexahedron, 13 wedge, 14 pyramid */
+} gprtcuSolidHit;
+
+GPRTCU_API gprtcuStatus gprtcuSolidBounds(const gprtcuSolids *solids, float *aabbs, float *boxes,
+                                          gprtcuStream stream);
+GPRTCU_API gprtcuStatus gprtcuLocateSolidPoints(const gprtcuLbvh *bvh, const gprtcuSolids *solids,
+                                                const float *points, uint64_t numPoints, gprtcuSolidHit *hits,
+                                                float *rstw, void *scratch, size_t scratchBytes, gprtcuStream stream);
+
+/* ------------------------------------------------------------------------
  * Two-level instancing.  Replaces gprtInstanceAccelCreate + TraceRay over an
  * instance acceleration structure (gprt/gprt_host.h:1418; instance record
  * gprt::Instance, gprt/gprt_shared.h:92-101) in software: a top-level LBVH

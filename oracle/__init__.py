@@ -77,6 +77,14 @@ def lib():
         L.orc_trace_brute.argtypes = [vp, vp, u32, vp, u64, vp]
         L.orc_trace_lbvh.argtypes = [vp, vp, u32, vp, vp, vp, u64, i32, vp]
         L.orc_num_threads.restype = i32
+        L.orc_solid_vertex_count.argtypes = [u32]
+        L.orc_solid_vertex_count.restype = i32
+        L.orc_solid_hit_kind.argtypes = [u32]
+        L.orc_solid_hit_kind.restype = u32
+        L.orc_solid_intersect.argtypes = [vp, vp, u32, vp]
+        L.orc_solid_intersect.restype = i32
+        L.orc_solid_bounds.argtypes = [vp, vp, vp, u32, vp]
+        L.orc_solid_locate_brute.argtypes = [vp, vp, vp, u32, vp, u64, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -94,6 +102,13 @@ def ref():
         R.ref_lbvh_build.argtypes = [i32, vp, u32, vp, u32, vp, vp, vp, vp, vp]
         R.ref_hilbert3d.argtypes = [u32, u32, u32]
         R.ref_hilbert3d.restype = u32
+        R.ref_solid_intersect.argtypes = [vp, vp, u32, vp]
+        R.ref_solid_intersect.restype = i32
+        R.ref_solid_bounds.argtypes = [vp, vp, vp, u32, vp]
+        R.ref_solid_vertex_count.argtypes = [u32]
+        R.ref_solid_vertex_count.restype = i32
+        R.ref_solid_hit_kind.argtypes = [u32]
+        R.ref_solid_hit_kind.restype = u32
         _ref = R
     return _ref
 
@@ -349,6 +364,63 @@ def isect32(ray, v0, v1, v2):
     t = np.zeros(1, np.float32)
     hit = lib().orc_isect_tri32(*[_p(v) for v in a], _p(t))
     return bool(hit), float(t[0])
+
+
+# ---------------------------------------------------------------- solid cells
+def _qw(verts, n):
+    qw = np.zeros((8, 4), np.float32)
+    qw[:n] = np.asarray(verts, np.float32).reshape(-1, 4)[:n]
+    return qw
+
+
+def solid_intersect(p, verts, n):
+    """intersectPointSolid restated: (hit, rstw[4]) for a point and a cell's
+    n float4 vertices {x, y, z, density}."""
+    r = np.zeros(4, np.float32)
+    p = np.ascontiguousarray(p, dtype=np.float32)
+    h = lib().orc_solid_intersect(_p(p), _p(_qw(verts, n)), n, _p(r))
+    return bool(h), r
+
+
+def ref_solid_intersect(p, verts, n):
+    """The reference's own intersectPointSolid (needs oracle/_ref)."""
+    r = np.zeros(4, np.float32)
+    p = np.ascontiguousarray(p, dtype=np.float32)
+    h = ref().ref_solid_intersect(_p(p), _p(_qw(verts, n)), n, _p(r))
+    return bool(h), r
+
+
+def solid_bounds(verts, idx, types):
+    verts = np.ascontiguousarray(verts, dtype=np.float32)
+    idx = np.ascontiguousarray(idx, dtype=np.uint32)
+    types = np.ascontiguousarray(types, dtype=np.uint8)
+    out = np.zeros((types.size, 8), np.float32)
+    lib().orc_solid_bounds(_p(verts), _p(idx), _p(types), types.size, _p(out))
+    return out
+
+
+def ref_solid_bounds(verts, idx, types):
+    """The reference's own SolidBounds (needs oracle/_ref)."""
+    verts = np.ascontiguousarray(verts, dtype=np.float32)
+    idx = np.ascontiguousarray(idx, dtype=np.uint32)
+    types = np.ascontiguousarray(types, dtype=np.uint8)
+    out = np.zeros((types.size, 8), np.float32)
+    ref().ref_solid_bounds(_p(verts), _p(idx), _p(types), types.size, _p(out))
+    return out
+
+
+def solid_locate_brute(verts, idx, types, points):
+    """(cell u32 [P], kind u32 [P], rstw f32 [P, 4]) by exhaustive search."""
+    verts = np.ascontiguousarray(verts, dtype=np.float32)
+    idx = np.ascontiguousarray(idx, dtype=np.uint32)
+    types = np.ascontiguousarray(types, dtype=np.uint8)
+    pts = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 4)
+    cell = np.zeros(pts.shape[0], np.uint32)
+    kind = np.zeros(pts.shape[0], np.uint32)
+    rstw = np.zeros((pts.shape[0], 4), np.float32)
+    lib().orc_solid_locate_brute(_p(verts), _p(idx), _p(types), types.size, _p(pts), pts.shape[0], _p(cell),
+                                 _p(kind), _p(rstw))
+    return cell, kind, rstw
 
 
 def num_threads():

@@ -10,6 +10,7 @@
 #include "oracle.h"
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -973,5 +974,221 @@ extern "C" void orc_trace_instances_brute(const orc_instance *inst, uint32_t nin
     } else {
       hits[r].t = INFINITY;
     }
+  }
+}
+
+// ============================================================================
+// solid cells: bounds and point location
+// ============================================================================
+// Cell types and vertex counts (gprt/gprt_fallbacks.slang:289-318; the type
+// codes match gprt/gprt_host.h:291-298).  A tetrahedral pair is evaluated as
+// an eight-node (trilinear) cell and reports the tetrahedron hit kind.
+static int solid_nodes(uint32_t type) {
+  switch (type) {
+    case 10: return 4;
+    case 14: return 5;
+    case 13: return 6;
+    case 12: return 8;
+    case 23: return 8;
+    default: return 0;
+  }
+}
+extern "C" uint32_t orc_solid_hit_kind(uint32_t type) {
+  switch (type) {
+    case 10: return 10;
+    case 23: return 10;
+    case 14: return 14;
+    case 13: return 13;
+    case 12: return 12;
+    default: return 0;
+  }
+}
+extern "C" int orc_solid_vertex_count(uint32_t type) { return solid_nodes(type); }
+
+// Forward-mode dual number: the reference differentiates IsoToSupport with
+// Slang's fwd_diff (gprt/gprt_fallbacks.slang:437-439); the derivative of
+// c - a is -da and of a b is da b + a db, every operation rounded once.
+struct Dl {
+  float v, d;
+};
+static inline Dl dl_add(Dl a, Dl b) { return {a.v + b.v, a.d + b.d}; }
+static inline Dl dl_sub(Dl a, Dl b) { return {a.v - b.v, a.d - b.d}; }
+static inline Dl dl_rsub(float c, Dl a) { return {c - a.v, -a.d}; }
+static inline Dl dl_mul(Dl a, Dl b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+
+// IsoToSupport (gprt/gprt_fallbacks.slang:370-406): shape functions of the
+// linear tetrahedron, pyramid, wedge and hexahedron at (r, s, t), in the
+// reference's operation order; with a seed direction the derivatives too.
+static void iso_support(int n, const Dl rst[3], Dl w[8]) {
+  for (int i = 0; i < 8; ++i) w[i] = {0.0f, 0.0f};
+  const Dl r = rst[0], s = rst[1], t = rst[2];
+  const Dl mr = dl_rsub(1.0f, r), ms = dl_rsub(1.0f, s), mt = dl_rsub(1.0f, t);
+  if (n == 4) {
+    w[0] = dl_rsub(1.0f, dl_add(dl_add(r, s), t));
+    w[1] = r;
+    w[2] = s;
+    w[3] = t;
+  }
+  if (n == 5) {
+    w[0] = dl_mul(dl_mul(mr, ms), mt);
+    w[1] = dl_mul(dl_mul(r, ms), mt);
+    w[2] = dl_mul(dl_mul(r, s), mt);
+    w[3] = dl_mul(dl_mul(mr, s), mt);
+    w[4] = t;
+  }
+  if (n == 6) {
+    const Dl rs = dl_sub(dl_rsub(1.0f, r), s);
+    w[0] = dl_mul(rs, dl_rsub(1.0f, t));
+    w[1] = dl_mul(r, dl_rsub(1.0f, t));
+    w[2] = dl_mul(s, dl_rsub(1.0f, t));
+    w[3] = dl_mul(rs, t);
+    w[4] = dl_mul(r, t);
+    w[5] = dl_mul(s, t);
+  }
+  if (n == 8) {
+    w[0] = dl_mul(dl_mul(mr, ms), mt);
+    w[1] = dl_mul(dl_mul(r, ms), mt);
+    w[2] = dl_mul(dl_mul(r, s), mt);
+    w[3] = dl_mul(dl_mul(mr, s), mt);
+    w[4] = dl_mul(dl_mul(mr, ms), t);
+    w[5] = dl_mul(dl_mul(r, ms), t);
+    w[6] = dl_mul(dl_mul(r, s), t);
+    w[7] = dl_mul(dl_mul(mr, s), t);
+  }
+}
+
+// determinant of the 3x3 matrix with rows a, b, c: cofactor expansion along
+// the first row.
+static inline float det3(const float a[3], const float b[3], const float c[3]) {
+  return a[0] * (b[1] * c[2] - b[2] * c[1]) - a[1] * (b[0] * c[2] - b[2] * c[0]) + a[2] * (b[0] * c[1] - b[1] * c[0]);
+}
+
+// intersectPointSolid (gprt/gprt_fallbacks.slang:409-464): Newton inversion of
+// the cell's isoparametric map, at most five steps from the cell's centre
+// (GetInitialRST, :320-325); the step is taken before the convergence test of
+// the residual it used; containment per IsoIsContained (:327-340); the
+// density is the last evaluated shape functions applied to the nodal values.
+// qw: 8 float4 {x, y, z, density}, zero beyond the cell's vertex count.
+extern "C" int orc_solid_intersect(const float *p, const float *qw, uint32_t n, float *rstw) {
+  float rst[3] = {0.5f, 0.5f, 0.5f};
+  if (n == 4) rst[0] = rst[1] = rst[2] = 0.25f;
+  if (n == 5) rst[2] = 0.2f;
+  rstw[0] = rst[0];
+  rstw[1] = rst[1];
+  rstw[2] = rst[2];
+  rstw[3] = 0.0f;
+  float w[8] = {0};
+  bool converged = false;
+  for (int it = 0; it < 5; ++it) {
+    Dl x[3] = {{rst[0], 0.0f}, {rst[1], 0.0f}, {rst[2], 0.0f}}, dw[8];
+    iso_support((int)n, x, dw);
+    for (int i = 0; i < 8; ++i) w[i] = dw[i].v;
+    float f[3] = {-p[0], -p[1], -p[2]};
+    for (int i = 0; i < 8; ++i)
+      for (int k = 0; k < 3; ++k) f[k] = f[k] + qw[4 * i + k] * w[i];
+    float col[3][3];  // world-space derivatives along r, s, t
+    for (int dir = 0; dir < 3; ++dir) {
+      Dl y[3] = {{rst[0], dir == 0 ? 1.0f : 0.0f}, {rst[1], dir == 1 ? 1.0f : 0.0f}, {rst[2], dir == 2 ? 1.0f : 0.0f}};
+      iso_support((int)n, y, dw);
+      float c[3] = {0.0f, 0.0f, 0.0f};
+      for (int i = 0; i < 8; ++i)
+        for (int k = 0; k < 3; ++k) c[k] = c[k] + qw[4 * i + k] * dw[i].d;
+      std::memcpy(col[dir], c, sizeof(c));
+    }
+    const float d = det3(col[0], col[1], col[2]);
+    if (std::fabs(d) < 1e-20f) return 0;
+    const float dinv = 1.0f / d;
+    rst[0] = rst[0] - det3(f, col[1], col[2]) * dinv;
+    rst[1] = rst[1] - det3(col[0], f, col[2]) * dinv;
+    rst[2] = rst[2] - det3(col[0], col[1], f) * dinv;
+    rstw[0] = rst[0];
+    rstw[1] = rst[1];
+    rstw[2] = rst[2];
+    if (std::fabs(f[0]) < 1e-3f && std::fabs(f[1]) < 1e-3f && std::fabs(f[2]) < 1e-3f) {
+      converged = true;
+      break;
+    }
+  }
+  if (!converged) return 0;
+  bool in = rst[0] >= 0.0f && rst[1] >= 0.0f && rst[2] >= 0.0f && rst[0] <= 1.0f && rst[1] <= 1.0f && rst[2] <= 1.0f;
+  if (n == 4) in = in && (rst[0] + rst[1] + rst[2]) <= 1.0f;
+  if (n == 6) in = in && rst[0] + rst[1] <= 1.0f;
+  if (!in) return 0;
+  float dens = 0.0f;
+  for (int i = 0; i < 8; ++i) dens = dens + qw[4 * i + 3] * w[i];
+  rstw[3] = dens;
+  return 1;
+}
+
+// A cell's nodes in index order (SolidIntersection's gather,
+// gprt/gprt_fallbacks.slang:504-522), zero beyond its vertex count.
+static int solid_gather(const float *verts, const uint32_t *idx, const uint8_t *types, uint32_t cell, float qw[32]) {
+  const int n = solid_nodes(types[cell]);
+  std::memset(qw, 0, 32 * sizeof(float));
+  for (int i = 0; i < n; ++i) std::memcpy(qw + 4 * i, verts + 4 * (size_t)idx[8 * (size_t)cell + i], 16);
+  return n;
+}
+
+// SolidBounds (gprt/gprt_fallbacks.slang:467-502): the min / max of the
+// cell's vertices, and of their densities.  aabbs: two float4 per cell,
+// {lo.xyz, hi.x}, {hi.yz, density min, density max}.  The reference's own
+// density update assigns a scalar to its float2 (:488-489), which leaves the
+// last vertex's density in both words; this follows the documented meaning
+// (the minimum and maximum of the densities) instead.
+extern "C" void orc_solid_bounds(const float *verts, const uint32_t *idx, const uint8_t *types, uint32_t ncells,
+                                 float *aabbs) {
+  for (uint32_t c = 0; c < ncells; ++c) {
+    const int n = solid_nodes(types[c]);
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    float dlo = FLT_MAX, dhi = -FLT_MAX;
+    for (int i = 0; i < n; ++i) {
+      const float *v = verts + 4 * (size_t)idx[8 * (size_t)c + i];
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::fmin(lo[k], v[k]);
+        hi[k] = std::fmax(hi[k], v[k]);
+      }
+      dlo = std::fmin(dlo, v[3]);
+      dhi = std::fmax(dhi, v[3]);
+    }
+    float *o = aabbs + 8 * (size_t)c;
+    o[0] = lo[0];
+    o[1] = lo[1];
+    o[2] = lo[2];
+    o[3] = hi[0];
+    o[4] = hi[1];
+    o[5] = hi[2];
+    o[6] = dlo;
+    o[7] = dhi;
+  }
+}
+
+// Point location by brute force: for every point the lowest-numbered cell
+// that contains it (TracePoint, gprt/gprt_builtins.slang:80-90, traces a
+// zero-length ray from the point; every accepted hit is at t = 0, so ties go
+// to the lowest id as for rays), with its hit kind and (r, s, t, density).
+extern "C" void orc_solid_locate_brute(const float *verts, const uint32_t *idx, const uint8_t *types, uint32_t ncells,
+                                       const float *points, uint64_t npts, uint32_t *cell, uint32_t *kind,
+                                       float *rstw) {
+  std::vector<float> box(8 * (size_t)ncells);
+  orc_solid_bounds(verts, idx, types, ncells, box.data());
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t q = 0; q < (int64_t)npts; ++q) {
+    const float *p = points + 4 * q;
+    cell[q] = 0xFFFFFFFFu;
+    kind[q] = 0;
+    float out[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (uint32_t c = 0; c < ncells; ++c) {
+      const float *b = &box[8 * (size_t)c];
+      if (!(b[0] <= p[0] && p[0] <= b[3] && b[1] <= p[1] && p[1] <= b[4] && b[2] <= p[2] && p[2] <= b[5])) continue;
+      float qw[32], r[4];
+      const int n = solid_gather(verts, idx, types, c, qw);
+      if (n && orc_solid_intersect(p, qw, (uint32_t)n, r)) {
+        cell[q] = c;
+        kind[q] = orc_solid_hit_kind(types[c]);
+        std::memcpy(out, r, sizeof(out));
+        break;
+      }
+    }
+    std::memcpy(rstw + 4 * q, out, sizeof(out));
   }
 }

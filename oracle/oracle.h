@@ -116,6 +116,23 @@ void orc_trace_brute(const float *pos, const uint32_t *tri, uint32_t n, const fl
 void orc_trace_lbvh(const float *pos, const uint32_t *tri, uint32_t n, const int32_t *nodes,
                     const float *aabbs, const float *rays, uint64_t nrays, int anyhit, orc_hit *hits);
 
+/* ---------------- solid cells ---------------- */
+/* Vertex count and hit kind of a cell type (gprt/gprt_fallbacks.slang:289-318). */
+int orc_solid_vertex_count(uint32_t type);
+uint32_t orc_solid_hit_kind(uint32_t type);
+/* intersectPointSolid (gprt/gprt_fallbacks.slang:409-464): qw = 8 float4
+ * {x, y, z, density}, zero beyond the vertex count n; rstw = (r, s, t,
+ * density).  Pinned to the reference's own function compiled from its
+ * sources (oracle/_ref). */
+int orc_solid_intersect(const float *p, const float *qw, uint32_t n, float *rstw);
+/* SolidBounds (gprt/gprt_fallbacks.slang:467-502) with the documented
+ * density range; two float4 per cell. */
+void orc_solid_bounds(const float *verts, const uint32_t *idx, const uint8_t *types, uint32_t ncells, float *aabbs);
+/* Point location by exhaustive search: the lowest-numbered cell whose box
+ * and Newton inversion contain the point. */
+void orc_solid_locate_brute(const float *verts, const uint32_t *idx, const uint8_t *types, uint32_t ncells,
+                            const float *points, uint64_t npts, uint32_t *cell, uint32_t *kind, float *rstw);
+
 /* ---------------- misc ---------------- */
 int orc_num_threads(void);
 

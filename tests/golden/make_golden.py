@@ -15,6 +15,12 @@
 * lss_ref.npz    -- intersectRayLSS and computeLssAabb of gprt/gprt_fallbacks.slang
                     compiled from the reference sources, on seeded rays, spheres
                     and swept-sphere segments, every cap / exit-test combination.
+* solid_ref.npz  -- intersectPointSolid and SolidBounds of gprt/gprt_fallbacks.slang
+                    compiled from the reference sources, on seeded distorted
+                    tetrahedra, pyramids, wedges, hexahedra and tetrahedral
+                    pairs (each cell in its own region of space) and points at
+                    their vertices, edge midpoints and around their boxes.
+                    `python make_golden.py solids` regenerates this file alone.
 * sortscan.npz   -- the reference tests' own host oracles restated with numpy:
                     std::sort / std::sort-by-key (tests/t02-bufferSort/hostCode.cpp:59,115),
                     the serial exclusive sum (tests/t03-bufferScans/hostCode.cpp:53-58)
@@ -92,6 +98,64 @@ def lss_cases():
     np.savez_compressed(os.path.join(HERE, "lss_ref.npz"), **out)
 
 
+SOLID_BASE = {
+    4: [[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]],
+    5: [[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0.5, 0.5, 1]],
+    6: [[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [0, 1, 1]],
+    8: [[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]],
+}
+SOLID_TYPES = [(10, 4), (14, 5), (13, 6), (12, 8), (23, 8)]
+
+
+def solid_case_inputs(cells=1000, pts_per_cell=8, seed=4321):
+    """Distorted cells of every type, cell c in its own slab x in [16c, 16c +
+    10), and points per cell: a vertex, an edge midpoint, the rest uniform in
+    the cell's box grown by 10 % on each side."""
+    r = np.random.default_rng(seed)
+    verts = np.zeros((cells * 8, 4), np.float32)
+    idx = np.full((cells, 8), 0xFFFFFFFF, np.uint32)
+    types = np.zeros(cells, np.uint8)
+    pts = np.zeros((cells * pts_per_cell, 4), np.float32)
+    for c in range(cells):
+        t, n = SOLID_TYPES[c % len(SOLID_TYPES)]
+        jit = [0.0, 0.05, 0.2, 0.45][(c // len(SOLID_TYPES)) % 4]
+        base = np.asarray(SOLID_BASE[n], np.float64)
+        v = base * r.uniform(0.3, 3.0) + r.normal(0, jit, (n, 3))
+        v = v + np.array([16.0 * c, r.uniform(-3, 3), r.uniform(-3, 3)])
+        verts[8 * c:8 * c + n, :3] = v
+        verts[8 * c:8 * c + n, 3] = r.uniform(-2, 2, n)
+        idx[c, :n] = np.arange(8 * c, 8 * c + n)
+        types[c] = t
+        vv = verts[8 * c:8 * c + n, :3]
+        lo, hi = vv.min(0), vv.max(0)
+        for k in range(pts_per_cell):
+            if k == 0:
+                p = vv[r.integers(n)]
+            elif k == 1:
+                a, b = r.choice(n, 2, replace=False)
+                p = (vv[a] + vv[b]) * np.float32(0.5)
+            else:
+                p = lo + (hi - lo) * r.uniform(-0.1, 1.1, 3)
+            pts[pts_per_cell * c + k, :3] = p
+    return verts, idx, types, pts
+
+
+def solid_cases():
+    """The reference's own intersectPointSolid and SolidBounds on the cases above."""
+    verts, idx, types, pts = solid_case_inputs()
+    ppc = pts.shape[0] // types.size
+    hit = np.zeros(pts.shape[0], np.uint8)
+    rstw = np.zeros((pts.shape[0], 4), np.float32)
+    for q in range(pts.shape[0]):
+        c = q // ppc
+        n = oracle.lib().orc_solid_vertex_count(int(types[c]))
+        h, r4 = oracle.ref_solid_intersect(pts[q, :3], verts[idx[c, :n]], n)
+        hit[q], rstw[q] = h, r4
+    aabbs = oracle.ref_solid_bounds(verts, idx, types)
+    np.savez_compressed(os.path.join(HERE, "solid_ref.npz"), verts=verts, idx=idx, types=types, points=pts,
+                        hit=hit, rstw=rstw, ref_aabbs=aabbs)
+
+
 def main():
     oracle.build(ref=True)
     rng = np.random.default_rng(20240601)
@@ -133,6 +197,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "lbvh_ref.npz"), **out)
 
     lss_cases()
+    solid_cases()
 
     R = oracle.ref()
     co = rng.integers(0, 1024, size=(4096, 3)).astype(np.uint32)
@@ -175,4 +240,8 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["solids"]:
+        oracle.build(ref=True)
+        solid_cases()
+    else:
+        main()
