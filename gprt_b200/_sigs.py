@@ -24,6 +24,7 @@ SIGNATURES = {
     "gprtcuSortPairsU32": ([vp, vp, u64, i32, i32, vp, sz, vp], st),
     "gprtcuSortKeysU64": ([vp, u64, i32, i32, vp, sz, vp], st),
     "gprtcuSortPairsU64": ([vp, vp, u64, i32, i32, vp, sz, vp], st),
+    "gprtcuSortPairsU32U64": ([vp, vp, u64, i32, i32, vp, sz, vp], st),
     "gprtcuSortPairsU64U64": ([vp, vp, u64, i32, i32, vp, sz, vp], st),
     "gprtcuSortConfigCount": ([], i32),
     "gprtcuSortConfigAt": ([i32, vp], st),
@@ -61,6 +62,7 @@ SIGNATURES = {
     "gprtcuDebugScanSkipTile": ([i64], None),
     "gprtcuDebugScanSkipStage": ([i64], None),
     "gprtcuDebugSortSkipTile": ([i64], None),
+    "gprtcuDebugSortRanking": ([i32], None),
     "gprtcuDebugRefitSkipLeaf": ([i64], st),
     "gprtcuDebugScanImpl": ([i32], None),
 }

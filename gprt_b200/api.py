@@ -93,6 +93,7 @@ def select(inp, select_positive=True, out=None, count=None, scr=None):
 _SORT_FN = {
     (4, 0): "gprtcuSortKeysU32",
     (4, 4): "gprtcuSortPairsU32",
+    (4, 8): "gprtcuSortPairsU32U64",
     (8, 0): "gprtcuSortKeysU64",
     (8, 4): "gprtcuSortPairsU64",
     (8, 8): "gprtcuSortPairsU64U64",

@@ -346,7 +346,7 @@ extern "C" GPRTCU_API void gprtcuCompatSort(GPRTContext c, GPRTBuffer keys, int 
   else if (kw == 8 && vw == 0) st = gprtcuSortKeysU64((uint64_t *)k, n, 0, 64, w.ptr, w.bytes, s);
   else if (kw == 8 && vw == 4) st = gprtcuSortPairsU64((uint64_t *)k, (uint32_t *)v, n, 0, 64, w.ptr, w.bytes, s);
   else if (kw == 8 && vw == 8) st = gprtcuSortPairsU64U64((uint64_t *)k, (uint64_t *)v, n, 0, 64, w.ptr, w.bytes, s);
-  else st = GPRTCU_ERR_INVALID_ARG;  // 32-bit keys with 64-bit payloads: not provided
+  else st = gprtcuSortPairsU32U64((uint32_t *)k, (uint64_t *)v, n, 0, 32, w.ptr, w.bytes, s);
   if (st != GPRTCU_OK) compat_error(st, what);
   // asynchronous, like the reference's compute submission; temporary work
   // space is freed after the stream drains, so its status is read then

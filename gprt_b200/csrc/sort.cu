@@ -13,16 +13,24 @@ uint32_t gprtcu_spin_budget(void);
 
 static int64_t g_sort_skip_tile = -1;
 extern "C" GPRTCU_API void gprtcuDebugSortSkipTile(int64_t tile) { g_sort_skip_tile = tile; }
+static int g_sort_ranking = 0;
+extern "C" GPRTCU_API void gprtcuDebugSortRanking(int mode) { g_sort_ranking = mode; }
+int gprtcu::gprtcu_sort_ranking() { return g_sort_ranking; }
 
 namespace {
 
-// Type pairs: 0 u32, 1 u32/u32, 2 u64, 3 u64/u32, 4 u64/u64.
+// Type pairs: 0 u32, 1 u32/u32, 2 u64, 3 u64/u32, 4 u64/u64, 5 u32/u64.
+constexpr int kTypeSlots = 6;
+// The reference counts keys in a uint32 (gprt/gprt.cpp:8837).
+constexpr uint64_t kSortMaxN = 0xFFFFFFFFull;
+
 int type_slot(int kw, int vw) {
   if (kw == 4 && vw == 0) return 0;
   if (kw == 4 && vw == 4) return 1;
   if (kw == 8 && vw == 0) return 2;
   if (kw == 8 && vw == 4) return 3;
   if (kw == 8 && vw == 8) return 4;
+  if (kw == 4 && vw == 8) return 5;
   return -1;
 }
 
@@ -32,6 +40,7 @@ const std::array<SortRunFn, kSortGridSize> &table_for(int slot) {
     case 1: return kSortTableK32V32;
     case 2: return kSortTableK64;
     case 3: return kSortTableK64V32;
+    case 5: return kSortTableK32V64;
     default: return kSortTableK64V64;
   }
 }
@@ -55,7 +64,7 @@ int default_index(int slot, uint64_t n) {
   return grid_index(8, 4096, 8);
 }
 
-std::atomic<int> g_active[5] = {{-1}, {-1}, {-1}, {-1}, {-1}};
+std::atomic<int> g_active[kTypeSlots] = {{-1}, {-1}, {-1}, {-1}, {-1}, {-1}};
 
 int active_index(int slot, uint64_t n) {
   const int i = g_active[slot].load(std::memory_order_relaxed);
@@ -82,16 +91,23 @@ SortLayout sort_layout(uint64_t n, int kw, int vw, int begin_bit, int end_bit, c
   L.trivial = off;
   off += 256;
   L.status = off;
-  off += gprtcu_align256((size_t)2 * L.tiles * (1u << s.rb) * 4);
+  // look-back words: 32-bit, or 64-bit once n needs more than 30 value bits
+  off += gprtcu_align256((size_t)2 * L.tiles * (1u << s.rb) * (n > (uint64_t)LB_VALUE ? 8 : 4));
   L.total = off;
   return L;
 }
 
-// Scratch that fits every shape of the grid, so a scratch sized once stays
-// valid whatever shape the tuner installs later.
+// Shapes that can sort n keys: all of them below 2^30; beyond, the 8-bit
+// shapes with tiles of 4096 keys or more (their wide look-back words, and a
+// bounded number of them).
+bool shape_usable(const SortShape &s, uint64_t n) { return n <= (uint64_t)LB_VALUE || (s.rb == 8 && s.tile >= 4096); }
+
+// Scratch that fits every usable shape of the grid, so a scratch sized once
+// stays valid whatever shape the tuner installs later.
 size_t scratch_any_shape(uint64_t n, int kw, int vw) {
   size_t m = 0;
-  for (int i = 0; i < kSortGridSize; ++i) m = std::max(m, sort_layout(n, kw, vw, 0, 8 * kw, kSortGrid[i]).total);
+  for (int i = 0; i < kSortGridSize; ++i)
+    if (shape_usable(kSortGrid[i], n)) m = std::max(m, sort_layout(n, kw, vw, 0, 8 * kw, kSortGrid[i]).total);
   return m;
 }
 
@@ -100,13 +116,17 @@ gprtcuStatus sort_dispatch(int slot, int index, void *keys, void *vals, uint64_t
   if (!keys && n) return GPRTCU_ERR_INVALID_ARG;
   if (vw && !vals && n) return GPRTCU_ERR_INVALID_ARG;
   if (begin_bit < 0 || end_bit > 8 * kw || begin_bit >= end_bit) return GPRTCU_ERR_INVALID_ARG;
-  if (n > (uint64_t)LB_VALUE) return GPRTCU_ERR_TOO_LARGE;
+  if (n > kSortMaxN) return GPRTCU_ERR_TOO_LARGE;
   if (!scratch || ((uintptr_t)scratch & 255)) return GPRTCU_ERR_INVALID_ARG;
   const SortShape &shape = kSortGrid[index];
+  if (!shape_usable(shape, n)) return GPRTCU_ERR_TOO_LARGE;
   SortLayout L = sort_layout(n, kw, vw, begin_bit, end_bit, shape);
   if (scratch_bytes < L.total) return GPRTCU_ERR_SCRATCH_TOO_SMALL;
-  if (n <= 1) return GPRTCU_OK;
   char *s = (char *)scratch;
+  // the header (its status word first) is valid after every call, even one
+  // with nothing to sort: callers such as the LBVH build read it
+  GPRTCU_TRY(cudaMemsetAsync(s, 0, sizeof(SortHeader), stream));
+  if (n <= 1) return GPRTCU_OK;
   SortArgs a;
   a.keys = keys;
   a.vals = vals;
@@ -125,8 +145,7 @@ gprtcuStatus sort_dispatch(int slot, int index, void *keys, void *vals, uint64_t
   a.skip_tile = g_sort_skip_tile;
   a.use_bulk = ((((uintptr_t)keys) | ((uintptr_t)a.keys_alt)) & 15) == 0;
   a.sms = gprtcu_num_sms();
-  // Zero: header, histograms, trivial flags, both look-back regions.
-  GPRTCU_TRY(cudaMemsetAsync(s, 0, sizeof(SortHeader), stream));
+  // Zero: histograms, trivial flags, both look-back regions.
   GPRTCU_TRY(cudaMemsetAsync(s + L.hist, 0, L.total - L.hist, stream));
   return table_for(slot)[index](a, stream);
 }
@@ -189,6 +208,11 @@ extern "C" GPRTCU_API gprtcuStatus gprtcuSortPairsU64(uint64_t *keys, uint32_t *
                                                       int endBit, void *scratch, size_t scratchBytes,
                                                       gprtcuStream stream) {
   return sort_entry(keys, values, n, 8, 4, beginBit, endBit, scratch, scratchBytes, stream);
+}
+extern "C" GPRTCU_API gprtcuStatus gprtcuSortPairsU32U64(uint32_t *keys, uint64_t *values, uint64_t n, int beginBit,
+                                                         int endBit, void *scratch, size_t scratchBytes,
+                                                         gprtcuStream stream) {
+  return sort_entry(keys, values, n, 4, 8, beginBit, endBit, scratch, scratchBytes, stream);
 }
 extern "C" GPRTCU_API gprtcuStatus gprtcuSortPairsU64U64(uint64_t *keys, uint64_t *values, uint64_t n, int beginBit,
                                                          int endBit, void *scratch, size_t scratchBytes,

@@ -463,6 +463,298 @@ __global__ void __launch_bounds__(WARPS * 32, (PassCfg<K, V, RB, WARPS, ITEMS>::
   }
 }
 
+// ---------------------------------------------------------------------------
+// 2b. one 8-bit digit pass with fewer instructions per key
+// ---------------------------------------------------------------------------
+// The pass above executes ~130 warp instructions per 32 keys on B200 (2^26
+// pairs; ALU pipe 59 %, issue 59 %), about 40 of them in the eight votes of
+// its ranking.  This one ranks the same way but trims the rest: digits are
+// one byte-permute when they are whole bytes (instead of a shift and a mask,
+// four times per key), every lane of a digit's peers writes the warp's count
+// (no leader election), no key is held in registers (the tile-sorted order
+// is a 16-bit index per slot, and the scatter gathers keys and payloads from
+// their untouched tiles, so payloads need no reorder round), full tiles
+// skip bounds tests, and keys and payloads leave the tile in one loop.
+// RANK 1 finds a key's peers with a 32-bit shared-memory OR of its lane bit
+// into the digit's word instead of votes (measured against the votes; a
+// 64-bit OR word carrying the count as well was 2.5x slower on Zipf keys:
+// same-word atomics serialise).
+template <typename K, typename V, int WARPS, int ITEMS, int RANK> struct Pass8Cfg {
+  static constexpr int RADIX = 256;
+  static constexpr int THREADS = WARPS * 32;
+  static constexpr int TILE = THREADS * ITEMS;
+  static constexpr int WARP_KEYS = 32 * ITEMS;
+  static constexpr bool HAS_V = sizeof(V) > 1;
+  static constexpr size_t KEY_BYTES = (size_t)TILE * sizeof(K);
+  static constexpr size_t VAL_BYTES = HAS_V ? (size_t)TILE * sizeof(V) : 0;
+  static constexpr size_t TBL_BYTES = (size_t)WARPS * RADIX * 4;  // per-warp counts, then first slots
+  static constexpr size_t MSK_BYTES = RANK == 1 ? (size_t)WARPS * RADIX * 4 : 0;  // per-warp lane masks
+  static constexpr size_t PERM_BYTES = (size_t)TILE * 2;
+  static constexpr size_t SMEM =
+      KEY_BYTES + VAL_BYTES + TBL_BYTES + MSK_BYTES + PERM_BYTES + RADIX * 4 /*goff*/ + 16 /*barriers*/;
+  static_assert(TILE <= 65536, "16-bit slot indices");
+  static constexpr int SMEM_CTAS = (int)((228 * 1024) / (SMEM + 1024));
+  static constexpr int THREAD_CTAS = 2048 / THREADS;
+  static constexpr int MIN_CTAS_A = SMEM_CTAS < THREAD_CTAS ? SMEM_CTAS : THREAD_CTAS;
+  static constexpr int REG_CTAS = 65536 / (THREADS * 64);
+  static constexpr int MIN_CTAS_B = MIN_CTAS_A < REG_CTAS ? MIN_CTAS_A : REG_CTAS;
+  static constexpr int MIN_CTAS = MIN_CTAS_B < 1 ? 1 : MIN_CTAS_B;
+  static_assert(THREADS >= RADIX, "one thread per digit");
+};
+
+// Look-back words of the 8-bit pass: {flag : 2 | value : 30} for n below
+// 2^30, or {flag : 2 | value : 62} (WIDE) for the larger n up to 2^32 - 1
+// that the reference's uint32 key count allows.
+template <bool WIDE> struct LbWord {
+  using T = typename std::conditional<WIDE, uint64_t, uint32_t>::type;
+  static constexpr int FB = WIDE ? 62 : 30;
+  static constexpr T AGG = (T)1 << FB, INC = (T)2 << FB, POISON = (T)3 << FB, VALUE = ((T)1 << FB) - 1;
+  __device__ static __forceinline__ T load(const T *p) {
+    if constexpr (WIDE) return ld_relaxed_u64(p);
+    else return ld_relaxed_u32(p);
+  }
+  __device__ static __forceinline__ void store(T *p, T v) {
+    if constexpr (WIDE) st_relaxed_u64(p, v);
+    else st_relaxed_u32(p, v);
+  }
+};
+
+
+// Digit of a key: BYTE = the digit is one whole byte of the key (8 bits at a
+// multiple of 8), taken by one byte-permute of the key's word that holds it.
+template <bool BYTE, typename K>
+__device__ __forceinline__ uint32_t digit8(K key, int shift, uint32_t mask, uint32_t sel) {
+  if constexpr (BYTE) {
+    const uint32_t w = sizeof(K) == 8 ? (uint32_t)((uint64_t)key >> (shift & 32)) : (uint32_t)key;
+    return __byte_perm(w, 0u, sel);
+  } else {
+    return (uint32_t)(key >> shift) & mask;
+  }
+}
+
+template <typename K, typename V, int WARPS, int ITEMS, bool BYTE, bool WIDE, int RANK>
+__global__ void __launch_bounds__(WARPS * 32, (Pass8Cfg<K, V, WARPS, ITEMS, RANK>::MIN_CTAS))
+    k_sort_pass8(const SortArgs a, int pass, int shift, int bits) {
+  using C = Pass8Cfg<K, V, WARPS, ITEMS, RANK>;
+  using LB = LbWord<WIDE>;
+  using SW = typename LB::T;
+  constexpr int RADIX = C::RADIX, THREADS = C::THREADS, TILE = C::TILE, WK = C::WARP_KEYS;
+  const uint32_t flags = ld_relaxed_u32(&a.trivial[pass]);
+  if (flags & SORT_FLAG_TRIVIAL) return;  // every key has the same digit: nothing moves
+  // An earlier pass gave up on a wait: its output is not a permutation of the
+  // keys, so the global digit offsets no longer bound this pass's writes.
+  if (ld_relaxed_u32(&a.hdr->h.status) != 0) return;
+
+  extern __shared__ __align__(128) unsigned char smem[];
+  K *s_keys = reinterpret_cast<K *>(smem);
+  V *s_vals = reinterpret_cast<V *>(smem + C::KEY_BYTES);
+  uint32_t *s_cnt = reinterpret_cast<uint32_t *>(smem + C::KEY_BYTES + C::VAL_BYTES);  // [WARPS][RADIX]
+  uint32_t *s_msk = reinterpret_cast<uint32_t *>(smem + C::KEY_BYTES + C::VAL_BYTES + C::TBL_BYTES);
+  uint16_t *s_perm = reinterpret_cast<uint16_t *>(smem + C::KEY_BYTES + C::VAL_BYTES + C::TBL_BYTES + C::MSK_BYTES);
+  uint32_t *s_goff = reinterpret_cast<uint32_t *>(smem + C::KEY_BYTES + C::VAL_BYTES + C::TBL_BYTES + C::MSK_BYTES +
+                                                  C::PERM_BYTES);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(s_goff + RADIX);
+  __shared__ uint32_t s_tile, s_abort;
+  __shared__ uint32_t s_tmp[32];
+
+  SortHeader *hdr = a.hdr;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t sel = hdr->sel[pass];
+  const K *src_k = static_cast<const K *>(sel ? a.keys_alt : a.keys);
+  K *dst_k = static_cast<K *>(sel ? a.keys : a.keys_alt);
+  const V *src_v = static_cast<const V *>(sel ? a.vals_alt : a.vals);
+  V *dst_v = static_cast<V *>(sel ? a.vals : a.vals_alt);
+  const uint32_t mask = (1u << bits) - 1u;
+  const uint32_t bsel = 0x4440u | (uint32_t)((shift >> 3) & 3);  // byte (shift / 8) % 4 of the word, zero above
+  SW *status = reinterpret_cast<SW *>(a.status) + (sel ? a.tiles * RADIX : 0);
+  SW *status_next = reinterpret_cast<SW *>(a.status) + (sel ? 0 : a.tiles * RADIX);
+
+  if (tid == 0) {
+    s_tile = atomicAdd(&hdr->ticket[1 + pass], 1u);
+    s_abort = 0;
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint64_t tile_start = (uint64_t)tile * TILE;
+  const uint32_t tile_n = (uint32_t)min((uint64_t)TILE, a.n - tile_start);
+  const bool full = tile_n == TILE;
+  const bool bulk = a.use_bulk && full;
+  if (tid == 0 && bulk) {
+    mbar_arrive_expect_tx(&bars[0], (uint32_t)C::KEY_BYTES);
+    bulk_g2s(s_keys, src_k + tile_start, (uint32_t)C::KEY_BYTES, &bars[0]);
+    if constexpr (C::HAS_V) {
+      mbar_arrive_expect_tx(&bars[1], (uint32_t)C::VAL_BYTES);
+      bulk_g2s(s_vals, src_v + tile_start, (uint32_t)C::VAL_BYTES, &bars[1]);
+    }
+  }
+  {
+    uint4 *t4 = reinterpret_cast<uint4 *>(s_cnt);  // counts and (RANK 1) masks are adjacent
+    for (int i = tid; i < (int)((C::TBL_BYTES + C::MSK_BYTES) / 16); i += THREADS) t4[i] = make_uint4(0u, 0u, 0u, 0u);
+  }
+  for (int i = tid; i < RADIX; i += THREADS) status_next[(uint64_t)tile * RADIX + i] = 0;
+  if (!bulk) {
+    // The last tile is padded with all-ones keys: they rank after every real
+    // key within the top digit, so the real keys fill slots [0, tile_n).
+    for (int i = tid; i < TILE; i += THREADS) s_keys[i] = (uint32_t)i < tile_n ? src_k[tile_start + i] : ~(K)0;
+    if constexpr (C::HAS_V)
+      for (int i = tid; i < TILE; i += THREADS)
+        if ((uint32_t)i < tile_n) s_vals[i] = src_v[tile_start + i];
+  } else if (!mbar_wait(&bars[0], 0, mbar_budget_of(a.budget))) {
+    s_abort = 1;
+  }
+  auto leave = [&]() {
+    if (tid == 0) {
+      record_error(&hdr->h, GPRTCU_ERR_TIMEOUT);
+      if (bulk) {
+        mbar_wait(&bars[0], 0, mbar_budget_of(a.budget));
+        if constexpr (C::HAS_V) mbar_wait(&bars[1], 0, mbar_budget_of(a.budget));
+      }
+    }
+  };
+  __syncthreads();
+  if (s_abort) {
+    leave();
+    return;
+  }
+
+  // ---- rank: warp w owns tile positions [w*WK, (w+1)*WK), row-major (row
+  // i = positions w*WK + 32 i .. +31).
+  uint32_t rank[ITEMS];
+  uint32_t *wc = s_cnt + warp * RADIX;
+  uint32_t *wm = s_msk + warp * RADIX;
+  const uint32_t lanebit = 1u << lane, lt = lanebit - 1u;
+#pragma unroll
+  for (int i = 0; i < ITEMS; ++i) {
+    const uint32_t d = digit8<BYTE>(s_keys[warp * WK + i * 32 + lane], shift, mask, bsel);
+    uint32_t peers;
+    const uint32_t base = wc[d];
+    if constexpr (RANK == 1) {
+      atomicOr(wm + d, lanebit);
+      __syncwarp();
+      peers = *reinterpret_cast<volatile uint32_t *>(wm + d);
+      __syncwarp();
+      wm[d] = 0u;
+    } else {
+      peers = warp_peers<8>(d);
+      __syncwarp();
+    }
+    wc[d] = base + __popc(peers);  // every peer stores the same count
+    __syncwarp();
+    rank[i] = base + __popc(peers & lt);
+  }
+  __syncthreads();
+
+  // ---- per digit: tile count, publish, tile-exclusive start, look-back;
+  // then each warp's first slot of the digit in the tile-sorted order (kept
+  // in the low half of the warp's word).
+  uint32_t tcount = 0;
+  const bool hooked = (int64_t)tile == a.skip_tile;  // test hook: this tile never publishes
+  if (tid < RADIX) {
+#pragma unroll 4
+    for (int w = 0; w < WARPS; ++w) tcount += s_cnt[w * RADIX + tid];
+    if ((uint32_t)tid == mask) tcount -= TILE - tile_n;  // padding of the last tile
+    if (!hooked) LB::store(status + (uint64_t)tile * RADIX + tid, (tile == 0 ? LB::INC : LB::AGG) | (SW)tcount);
+  }
+  const uint32_t tstart = block_excl_scan_digits<RADIX>(tcount, s_tmp);
+  if (tid < RADIX) {
+    uint32_t excl = 0;  // below 2^32: the count of keys before this tile's digit run
+    bool ok = true;
+    if (hooked) {
+      s_abort = 1;
+    } else if (tile > 0) {
+      int64_t j = (int64_t)tile - 1;
+      uint32_t spins = 0;
+      bool done = false;
+      while (!done && ok) {
+        SW sw[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          sw[c] = j - c >= 0 ? LB::load(status + (uint64_t)(j - c) * RADIX + tid) : LB::INC;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          if (done || !ok) break;
+          SW x = sw[c];
+          while ((x & ~LB::VALUE) == 0) {
+            if (++spins > a.budget) {
+              ok = false;
+              break;
+            }
+            x = LB::load(status + (uint64_t)(j - c) * RADIX + tid);
+          }
+          if (!ok) break;
+          const SW f = x & ~LB::VALUE;
+          if (f == LB::POISON) {
+            ok = false;
+            break;
+          }
+          excl += (uint32_t)(x & LB::VALUE);
+          if (f == LB::INC) done = true;
+        }
+        j -= 8;
+      }
+      LB::store(status + (uint64_t)tile * RADIX + tid, ok ? (LB::INC | (SW)(excl + tcount)) : LB::POISON);
+      if (!ok) s_abort = 1;
+    }
+    s_goff[tid] = a.hist[pass * RADIX + tid] + excl - tstart;
+    uint32_t run = tstart;
+#pragma unroll 4
+    for (int w = 0; w < WARPS; ++w) {
+      const uint32_t c = s_cnt[w * RADIX + tid];
+      s_cnt[w * RADIX + tid] = run;  // the warp's first slot of the digit
+      run += c;
+    }
+  }
+  __syncthreads();
+  if (s_abort) {
+    leave();
+    return;
+  }
+
+  // ---- tile-sorted order: slot (warp's first slot of the digit + rank)
+  // holds the key at this position.
+#pragma unroll
+  for (int i = 0; i < ITEMS; ++i) {
+    const uint32_t pos = warp * WK + i * 32 + lane;
+    s_perm[wc[digit8<BYTE>(s_keys[pos], shift, mask, bsel)] + rank[i]] = (uint16_t)pos;
+  }
+  if constexpr (C::HAS_V)
+    if (bulk && !mbar_wait(&bars[1], 0, mbar_budget_of(a.budget))) s_abort = 1;
+  __syncthreads();  // order complete; payload tile landed (s_abort visible)
+  if (s_abort) {
+    leave();
+    return;
+  }
+
+  // ---- scatter: slot p of the tile-sorted order goes to s_goff[digit] + p;
+  // a digit's slots are consecutive, so each run leaves as coalesced stores.
+  if (full) {
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+      const uint32_t p = j * THREADS + tid;
+      const uint32_t src = s_perm[p];
+      const K key = s_keys[src];
+      const uint32_t g = s_goff[digit8<BYTE>(key, shift, mask, bsel)] + p;
+      dst_k[g] = key;
+      if constexpr (C::HAS_V) dst_v[g] = s_vals[src];
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+      const uint32_t p = j * THREADS + tid;
+      if (p < tile_n) {
+        const uint32_t src = s_perm[p];
+        const K key = s_keys[src];
+        const uint32_t g = s_goff[digit8<BYTE>(key, shift, mask, bsel)] + p;
+        dst_k[g] = key;
+        if constexpr (C::HAS_V) dst_v[g] = s_vals[src];
+      }
+    }
+  }
+}
+
 // Copies the sorted result back into the caller's buffers when the number of
 // executed passes was odd (the data then ended in the alternate buffers).
 template <typename K, typename V>
@@ -477,6 +769,11 @@ __global__ void k_sort_final_copy(K *keys, const K *keys_alt, V *vals, const V *
 }
 
 // Shared memory a pass kernel of this shape needs.
+// Kernel of the 8-bit passes: 0 = k_sort_pass8 with vote ranking, 1 = the
+// original k_sort_pass, 2 = k_sort_pass8 with shared-memory OR ranking; a
+// test and measurement switch (sort.cu).
+int gprtcu_sort_ranking();
+
 template <typename K, typename V, int RB, int WARPS, int ITEMS>
 gprtcuStatus sort_run(const SortArgs &a, cudaStream_t stream) {
   using C = PassCfg<K, V, RB, WARPS, ITEMS>;
@@ -485,13 +782,51 @@ gprtcuStatus sort_run(const SortArgs &a, cudaStream_t stream) {
   k_sort_hist<K, RB><<<a.sms * 4, 512, 0, stream>>>(keys, a.n, a.begin_bit, a.end_bit, a.passes, a.hist, a.trivial,
                                                     a.hdr);
   GPRTCU_TRY(cudaGetLastError());
-  GPRTCU_TRY(cudaFuncSetAttribute(k_sort_pass<K, V, RB, WARPS, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)C::SMEM));
-  for (int p = 0; p < a.passes; ++p) {
-    const int shift = a.begin_bit + p * RB;
-    const int bits = a.end_bit - shift < RB ? a.end_bit - shift : RB;
-    k_sort_pass<K, V, RB, WARPS, ITEMS><<<(unsigned)a.tiles, C::THREADS, C::SMEM, stream>>>(a, p, shift, bits);
-    GPRTCU_TRY(cudaGetLastError());
+  bool match = false;
+  if constexpr (RB == 8) {
+    using C8 = Pass8Cfg<K, V, WARPS, ITEMS, 0>;
+    static_assert(C8::SMEM <= 227 * 1024, "shared memory per CTA");
+    // more keys than 30-bit look-back values can count need the wide words,
+    // which only the 8-bit kernel has
+    const bool wide = a.n > (uint64_t)LB_VALUE;
+    const int mode = gprtcu_sort_ranking();
+    match = wide || mode != 1;
+    if (match) {
+      for (int p = 0; p < a.passes; ++p) {
+        const int shift = a.begin_bit + p * RB;
+        const int bits = a.end_bit - shift < RB ? a.end_bit - shift : RB;
+        const bool byte = bits == 8 && (shift & 7) == 0;
+        auto launch = [&](auto kernel, size_t smem) -> gprtcuStatus {
+          GPRTCU_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+          kernel<<<(unsigned)a.tiles, C8::THREADS, smem, stream>>>(a, p, shift, bits);
+          GPRTCU_TRY(cudaGetLastError());
+          return GPRTCU_OK;
+        };
+        constexpr size_t S0 = Pass8Cfg<K, V, WARPS, ITEMS, 0>::SMEM, S1 = Pass8Cfg<K, V, WARPS, ITEMS, 1>::SMEM;
+        gprtcuStatus st;
+        if (mode == 2 && !wide)
+          st = byte ? launch(k_sort_pass8<K, V, WARPS, ITEMS, true, false, 1>, S1)
+                    : launch(k_sort_pass8<K, V, WARPS, ITEMS, false, false, 1>, S1);
+        else if (wide)
+          st = byte ? launch(k_sort_pass8<K, V, WARPS, ITEMS, true, true, 0>, S0)
+                    : launch(k_sort_pass8<K, V, WARPS, ITEMS, false, true, 0>, S0);
+        else
+          st = byte ? launch(k_sort_pass8<K, V, WARPS, ITEMS, true, false, 0>, S0)
+                    : launch(k_sort_pass8<K, V, WARPS, ITEMS, false, false, 0>, S0);
+        if (st != GPRTCU_OK) return st;
+      }
+    }
+  }
+  if (!match && a.n > (uint64_t)LB_VALUE) return GPRTCU_ERR_TOO_LARGE;
+  if (!match) {
+    GPRTCU_TRY(cudaFuncSetAttribute(k_sort_pass<K, V, RB, WARPS, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)C::SMEM));
+    for (int p = 0; p < a.passes; ++p) {
+      const int shift = a.begin_bit + p * RB;
+      const int bits = a.end_bit - shift < RB ? a.end_bit - shift : RB;
+      k_sort_pass<K, V, RB, WARPS, ITEMS><<<(unsigned)a.tiles, C::THREADS, C::SMEM, stream>>>(a, p, shift, bits);
+      GPRTCU_TRY(cudaGetLastError());
+    }
   }
   k_sort_final_copy<K, V><<<a.sms * 4, 256, 0, stream>>>(keys, static_cast<const K *>(a.keys_alt),
                                                          static_cast<V *>(a.vals),
@@ -509,6 +844,7 @@ constexpr std::array<SortRunFn, sizeof...(I)> make_sort_table(std::index_sequenc
 // sort_*.cu files.
 extern const std::array<SortRunFn, kSortGridSize> kSortTableK32;
 extern const std::array<SortRunFn, kSortGridSize> kSortTableK32V32;
+extern const std::array<SortRunFn, kSortGridSize> kSortTableK32V64;
 extern const std::array<SortRunFn, kSortGridSize> kSortTableK64;
 extern const std::array<SortRunFn, kSortGridSize> kSortTableK64V32;
 extern const std::array<SortRunFn, kSortGridSize> kSortTableK64V64;

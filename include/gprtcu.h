@@ -107,7 +107,11 @@ GPRTCU_API gprtcuStatus gprtcuSelectI32(const int32_t *in, int32_t *out, uint64_
  * reference.  The reference sorts 64-bit keys with 64-bit payloads over all
  * 64 bits (gprt/gprt.cpp:8837,8966-8969); the 32-bit forms are what its
  * typed shims and tests/t02-bufferSort use.  Key widths 4/8 bytes, payload
- * widths 0/4/8 bytes.  Maximum n: 2^30 - 1.
+ * widths 0/4/8 bytes (a 32-bit key may carry the reference's 64-bit payload,
+ * gprt/gprt_sort.slang:29-36).  Maximum n: 2^32 - 1, the reference's uint32
+ * key count (gprt/gprt.cpp:8837); from 2^30 keys on, the shape must have
+ * 8-bit digits and tiles of at least 4096 keys (the defaults do), else
+ * GPRTCU_ERR_TOO_LARGE.
  * ------------------------------------------------------------------------ */
 GPRTCU_API size_t gprtcuSortScratchSize(uint64_t n, int keyBytes, int valueBytes);
 GPRTCU_API gprtcuStatus gprtcuSortKeysU32(uint32_t *keys, uint64_t n, int beginBit, int endBit, void *scratch,
@@ -118,6 +122,8 @@ GPRTCU_API gprtcuStatus gprtcuSortKeysU64(uint64_t *keys, uint64_t n, int beginB
                                           size_t scratchBytes, gprtcuStream stream);
 GPRTCU_API gprtcuStatus gprtcuSortPairsU64(uint64_t *keys, uint32_t *values, uint64_t n, int beginBit, int endBit,
                                            void *scratch, size_t scratchBytes, gprtcuStream stream);
+GPRTCU_API gprtcuStatus gprtcuSortPairsU32U64(uint32_t *keys, uint64_t *values, uint64_t n, int beginBit, int endBit,
+                                              void *scratch, size_t scratchBytes, gprtcuStream stream);
 GPRTCU_API gprtcuStatus gprtcuSortPairsU64U64(uint64_t *keys, uint64_t *values, uint64_t n, int beginBit, int endBit,
                                               void *scratch, size_t scratchBytes, gprtcuStream stream);
 
@@ -468,6 +474,10 @@ GPRTCU_API void gprtcuDebugSetSpinBudget(uint32_t polls);
 GPRTCU_API void gprtcuDebugScanSkipTile(int64_t tile);
 GPRTCU_API void gprtcuDebugScanSkipStage(int64_t tile);
 GPRTCU_API void gprtcuDebugSortSkipTile(int64_t tile);
+/* Kernel of the 8-bit sort passes, for tests and measurements: 0 (default)
+ * the trimmed pass with vote ranking, 1 the original pass, 2 the trimmed
+ * pass ranking by shared-memory OR words.  All give the same bits. */
+GPRTCU_API void gprtcuDebugSortRanking(int mode);
 GPRTCU_API gprtcuStatus gprtcuDebugRefitSkipLeaf(int64_t slot);
 /* Scan kernel selection for tests: 0 = automatic (default: the persistent
  * re-read kernel for n >= 2^20 and the TMA-staged tile-per-CTA kernel below,

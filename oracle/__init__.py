@@ -22,10 +22,12 @@ HIT_DTYPE = np.dtype([("prim", np.uint32), ("t", np.float32)])
 
 
 def build(ref=None):
-    """Compile the oracle (and the reference checker when the reference sources exist)."""
+    """Compile the oracle, and the reference checker when ref is true or,
+    with ref None, when the recipe finds the reference sources (oracle/Makefile,
+    variable REF)."""
     subprocess.check_call(["make", "-s", "-C", HERE])
     if ref is None:
-        ref = os.path.isdir("/root/reference/gprt")
+        ref = subprocess.call(["make", "-s", "-C", HERE, "has-ref"], stderr=subprocess.DEVNULL) == 0
     if ref:
         subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
 

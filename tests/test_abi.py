@@ -68,7 +68,8 @@ def test_sort_tuning_grid_host_side():
     L = api.lib()
     bad = api.SortConfig(5, 1024, 4)
     assert L.gprtcuSortSetConfig(4, 4, ctypes.byref(bad)) == 1
-    assert L.gprtcuSortSetConfig(4, 8, ctypes.byref(api.SortConfig(*grid[0]))) == 1  # no u32-key/u64-payload
+    assert L.gprtcuSortSetConfig(4, 2, ctypes.byref(api.SortConfig(*grid[0]))) == 1  # no 16-bit payloads
+    assert L.gprtcuSortSetConfig(4, 8, None) == 0  # u32 keys with the reference's u64 payloads
     assert L.gprtcuSortConfigAt(len(grid), ctypes.byref(bad)) == 1
     # scratch covers the largest shape: two look-back regions at 1024-key tiles, 8-bit digits
     n = 1 << 20

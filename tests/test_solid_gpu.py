@@ -76,8 +76,10 @@ def test_solid_grid_location_matches_oracle(cuda, g, npts, seed):
     k = min(500, verts.shape[0])
     pts[:k, :3] = verts[rng.choice(verts.shape[0], k, replace=False), :3]
     cell = _check_against_brute(verts, idx, types, pts)
-    # a lone jittered cube leaves a quarter of the sampled region outside it
-    assert (cell != MISS).mean() > (0.6 if g == 1 else 0.8)
+    # the sampled region reaches past the mesh, and neighbouring cubes of
+    # different fills meet along non-matching faces: about 3/4 of the points
+    # lie in a cell
+    assert (cell != MISS).mean() > 0.6
 
 
 @pytest.mark.parametrize("fill", range(5))
@@ -126,7 +128,7 @@ def test_strides(cuda):
     t2[:, 1] = 99
     dv, di, dt = _dev(vbig), _dev(i4, np.int32), _dev(t2)
     s = api.Solids(dv, di, dt)
-    s.desc.numCells = types.size
+    s.n = s.desc.numCells = types.size
     s.desc.vertexStride, s.desc.indexStride, s.desc.typeStride = 32, 16, 2
     _, boxes = api.solid_bounds(s)
     bvh = api.lbvh_build_boxes(boxes)

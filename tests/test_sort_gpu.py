@@ -150,7 +150,7 @@ def test_sort_host_errors(cuda):
     assert L.gprtcuSortKeysU32(api._ptr(k), 100, 5, 5, api._ptr(big), big.numel(), api._stream()) == 1
 
 
-_TYPES = [(4, 0), (4, 4), (8, 0), (8, 4), (8, 8)]
+_TYPES = [(4, 0), (4, 4), (4, 8), (8, 0), (8, 4), (8, 8)]
 
 
 @pytest.mark.parametrize("kw,vw", _TYPES)
@@ -206,3 +206,65 @@ def test_sort_autotune_installs_a_shape(cuda):
     finally:
         api.sort_set_config(4, 4, None)
         api.sort_set_config(4, 0, None)
+
+
+@pytest.mark.parametrize("kw,vw", [(4, 4), (4, 8), (8, 4)])
+def test_sort_rankings_agree(cuda, kw, vw):
+    # the 8-bit passes have three kernels (test switch): the trimmed pass with
+    # vote ranking (default), the original pass, and the trimmed pass ranking
+    # by shared-memory OR words; all must give the oracle's bits
+    import torch
+    import gprt_b200
+    from gprt_b200 import api
+    L = gprt_b200.lib()
+    rng = np.random.default_rng(kw * 100 + vw)
+    kdt = np.uint32 if kw == 4 else np.uint64
+    try:
+        for n in (8191, 65536 + 3, 1 << 21):
+            for name, k in _dists(rng, n, 32 if kw == 4 else 44):
+                k = k.astype(kdt)
+                if name == "uniform":
+                    k[::5] = k[1]
+                v = rng.integers(0, 2 ** 63, size=n, dtype=np.uint64)
+                v = v.astype(np.uint32) if vw == 4 else v
+                ek, ev = oracle.sort(k, v)
+                for mode in (0, 1, 2):
+                    L.gprtcuDebugSortRanking(mode)
+                    kt = torch.from_numpy(k.view(np.int32 if kw == 4 else np.int64).copy()).cuda()
+                    vt = torch.from_numpy(v.view(np.int32 if vw == 4 else np.int64).copy()).cuda()
+                    api.sort(kt, vt, 0, 32 if kw == 4 else 44)
+                    assert np.array_equal(kt.cpu().numpy().view(kdt), ek), (n, name, mode)
+                    assert np.array_equal(vt.cpu().numpy().view(v.dtype), ev), (n, name, mode)
+    finally:
+        L.gprtcuDebugSortRanking(0)
+
+
+def test_sort_beyond_2_30_keys(cuda):
+    # n past 2^30 - 1 needs the wide look-back words; checked through
+    # size-independent properties: keys ascending, the payload (original
+    # index) a permutation that maps every key back to its input, equal keys
+    # in input order (stability)
+    import torch
+    from gprt_b200 import api
+    n = (1 << 30) + 4097
+    g = torch.Generator(device="cuda").manual_seed(99)
+    k0 = torch.randint(-2 ** 31, 2 ** 31 - 1, (n,), generator=g, dtype=torch.int32, device="cuda")
+    k0[::3] = k0[7]  # many equal keys
+    k = k0.clone()
+    v = torch.arange(n, dtype=torch.int32, device="cuda")
+    scr = api.scratch(api.sort_scratch_size(n, 4, 4))
+    api.sort(k, v, 0, 32, scr)
+    torch.cuda.synchronize()
+    assert api.scratch_status(scr) == 0
+    step = 1 << 27
+    for lo in range(0, n, step):
+        hi = min(n, lo + step + 1)
+        ku = k[lo:hi].to(torch.int64) & 0xFFFFFFFF
+        vi = v[lo:hi].to(torch.int64)
+        assert bool(torch.all(ku[1:] >= ku[:-1]))
+        assert bool(torch.equal(k0[vi], k[lo:hi]))
+        same = ku[1:] == ku[:-1]
+        assert bool(torch.all(vi[1:][same] > vi[:-1][same]))
+    seen = torch.zeros(n, dtype=torch.bool, device="cuda")
+    seen[v.to(torch.int64)] = True
+    assert bool(seen.all())
