@@ -223,17 +223,74 @@ __device__ __forceinline__ bool point_in(float px, float py, float pz, float lx,
 }
 
 // Point location over the box LBVH (gprtcuLbvh.bvh2 over the cells' boxes;
-// leaf slot k holds cell ids[k]).  One lane per point, 32 points per warp
-// taken from a global counter, warp-uniform visit loop; every leaf whose box
-// holds the point and whose cell id is below the best so far runs the Newton
-// inversion.  hits: {cell, kind} per point (cell 0xFFFFFFFF, kind 0 when no
-// cell holds it); rstw (optional): (r, s, t, density), zero on a miss.
+// leaf slot k holds cell ids[k]).  32 points per warp, one lane per point,
+// taken from a global counter.  The traversal only collects candidates: a
+// leaf whose box holds the point appends (cell, lane) to the warp's queue in
+// shared memory.  The Newton inversions then run from the queue with every
+// lane of the warp taking one candidate, whoever's point it is, and a cell
+// that holds the point lowers its owner's best cell with a shared-memory
+// atomicMin.  (Running each lane's inversions where its traversal met them
+// left 3.2 of 32 lanes active: lanes reach leaves at different steps, and an
+// inversion is ~1,000 instructions.)  The queue is drained whenever it could
+// overflow on the next step and at the end; candidates at or above the
+// owner's best so far are dropped.  The winner's (r, s, t, density) is
+// recomputed by its owner once at the end (the same arithmetic, so the same
+// bits).  hits: {cell, kind} per point (cell 0xFFFFFFFF, kind 0 when no cell
+// holds it); rstw (optional): (r, s, t, density), zero on a miss.
+constexpr int kLocateQueue = 256;  // per warp; a step appends at most 64
+
+__device__ __forceinline__ bool locate_cell(const SolidView &sv, uint32_t id, float px, float py, float pz,
+                                            float4 &r) {
+  const int n = solid_nodes(sv.type(id));
+  float4 q[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) q[i] = i < n ? sv.vertex(sv.index(id, i)) : make_float4(0.f, 0.f, 0.f, 0.f);
+  return n && solid_intersect(px, py, pz, q, n, r);
+}
+
 __global__ void __launch_bounds__(kLocateThreads) k_locate_solids(const Bvh2Node *bvh, const uint32_t *ids,
                                                                   uint32_t nleaves, const float *root_box, SolidView sv,
                                                                   const float4 *points, uint64_t npts, uint2 *hits,
                                                                   float4 *rstw_out, unsigned long long *counter,
                                                                   uint32_t *err) {
-  const int lane = threadIdx.x & 31;
+  constexpr int WARPS = kLocateThreads / 32;
+  __shared__ uint32_t s_qcell[WARPS][kLocateQueue];
+  __shared__ uint8_t s_qown[WARPS][kLocateQueue];
+  __shared__ float4 s_pt[WARPS][32];
+  __shared__ uint32_t s_best[WARPS][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  uint32_t *qcell = s_qcell[warp];
+  uint8_t *qown = s_qown[warp];
+  uint32_t *best = s_best[warp];
+  uint32_t qn = 0;  // warp-uniform queue length
+  // every lane takes one queued candidate per round
+  auto drain = [&]() {
+    __syncwarp();
+    for (uint32_t b = 0; b < qn; b += 32) {
+      const uint32_t e = b + lane;
+      if (e < qn) {
+        const uint32_t id = qcell[e], own = qown[e];
+        if (id < *reinterpret_cast<volatile uint32_t *>(best + own)) {
+          const float4 p = s_pt[warp][own];
+          float4 r;
+          if (locate_cell(sv, id, p.x, p.y, p.z, r)) atomicMin(best + own, id);
+        }
+      }
+    }
+    qn = 0;
+    __syncwarp();
+  };
+  // append this lane's candidate (if want) to the warp's queue
+  auto push = [&](bool want, uint32_t id) {
+    const unsigned m = __ballot_sync(FULL_MASK, want);
+    if (want) {
+      const uint32_t at = qn + __popc(m & lt);
+      qcell[at] = id;
+      qown[at] = (uint8_t)lane;
+    }
+    qn += __popc(m);
+  };
   while (true) {
     unsigned long long base = 0;
     if (lane == 0) base = atomicAdd(counter, 32ull);
@@ -242,32 +299,21 @@ __global__ void __launch_bounds__(kLocateThreads) k_locate_solids(const Bvh2Node
     const uint64_t qi = base + lane;
     const bool active = qi < npts;
     const float4 p = active ? __ldg(points + qi) : make_float4(0.f, 0.f, 0.f, 0.f);
-    uint32_t best = kNoCell;
-    float4 brstw = make_float4(0.f, 0.f, 0.f, 0.f);
-    auto leaf = [&](uint32_t slot) {
-      const uint32_t id = __ldg(ids + slot);
-      if (id >= best) return;
-      const int n = solid_nodes(sv.type(id));
-      float4 q[8];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) q[i] = i < n ? sv.vertex(sv.index(id, i)) : make_float4(0.f, 0.f, 0.f, 0.f);
-      float4 r;
-      if (n && solid_intersect(p.x, p.y, p.z, q, n, r)) {
-        best = id;
-        brstw = r;
-      }
-    };
+    s_pt[warp][lane] = p;
+    best[lane] = kNoCell;
+    __syncwarp();
     bool done = !active;
     int stack[kLocateStack];
     int sp = 0;
     int node = 0;
-    if (nleaves == 1 || !active) {
-      if (active && point_in(p.x, p.y, p.z, root_box[0], root_box[1], root_box[2], root_box[3], root_box[4],
-                             root_box[5]))
-        leaf(0);
+    if (nleaves == 1) {
+      push(active && point_in(p.x, p.y, p.z, root_box[0], root_box[1], root_box[2], root_box[3], root_box[4],
+                              root_box[5]),
+           __ldg(ids));
       done = true;
     }
     while (__any_sync(FULL_MASK, !done)) {
+      uint32_t c0 = kNoCell, c1 = kNoCell;  // leaf candidates of this step
       if (!done) {
         const float4 *np = reinterpret_cast<const float4 *>(bvh + node);
         const float4 f0 = __ldg(np), f1 = __ldg(np + 1), f2 = __ldg(np + 2);
@@ -275,11 +321,11 @@ __global__ void __launch_bounds__(kLocateThreads) k_locate_solids(const Bvh2Node
         bool h0 = point_in(p.x, p.y, p.z, f0.x, f0.y, f0.z, f0.w, f1.x, f1.y);
         bool h1 = point_in(p.x, p.y, p.z, f1.z, f1.w, f2.x, f2.y, f2.z, f2.w);
         if (h0 && rf.x < 0) {
-          leaf((uint32_t)~rf.x);
+          c0 = __ldg(ids + (uint32_t)~rf.x);
           h0 = false;
         }
         if (h1 && rf.y < 0) {
-          leaf((uint32_t)~rf.y);
+          c1 = __ldg(ids + (uint32_t)~rf.y);
           h1 = false;
         }
         if (h0 && h1) {
@@ -300,11 +346,20 @@ __global__ void __launch_bounds__(kLocateThreads) k_locate_solids(const Bvh2Node
           done = true;
         }
       }
+      const uint32_t b = best[lane];
+      push(c0 < b, c0);
+      push(c1 < b, c1);
+      if (qn > kLocateQueue - 64) drain();
     }
+    drain();
     if (active) {
-      hits[qi] = make_uint2(best, best == kNoCell ? 0u : solid_kind(sv.type(best)));
-      if (rstw_out) rstw_out[qi] = brstw;
+      const uint32_t id = best[lane];
+      float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (id != kNoCell) locate_cell(sv, id, p.x, p.y, p.z, r);
+      hits[qi] = make_uint2(id, id == kNoCell ? 0u : solid_kind(sv.type(id)));
+      if (rstw_out) rstw_out[qi] = r;
     }
+    __syncwarp();
   }
 }
 

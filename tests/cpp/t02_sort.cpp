@@ -79,6 +79,44 @@ int main(int argc, char **argv) {
     gprtContextDestroy(context);
   }
   {
+    // 32-bit keys with the reference's 64-bit payloads (gprt/gprt_sort.slang:29-36)
+    GPRTContext context = gprtContextCreate(nullptr, 1);
+    const uint32_t m = n < 10000000u ? n : 10000000u;
+    auto keys = gprtDeviceBufferCreate<uint32_t>(context, m);
+    auto values = gprtDeviceBufferCreate<uint64_t>(context, m);
+    auto scratch = gprtDeviceBufferCreate<uint32_t>(context);
+    std::vector<std::pair<uint32_t, uint64_t>> kv(m);
+    std::uniform_int_distribution<uint32_t> kd(0, 1023u);  // many equal keys: stability shows
+    for (uint32_t i = 0; i < m; ++i) kv[i] = {kd(rng), ((uint64_t)i << 32) | (uint64_t)rng()};
+    gprtBufferMap(keys);
+    gprtBufferMap(values);
+    uint32_t *kp = gprtBufferGetHostPointer(keys);
+    uint64_t *vp = gprtBufferGetHostPointer(values);
+    for (uint32_t i = 0; i < m; ++i) {
+      kp[i] = kv[i].first;
+      vp[i] = kv[i].second;
+    }
+    gprtBufferUnmap(keys);
+    gprtBufferUnmap(values);
+    std::stable_sort(kv.begin(), kv.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+    gprtBufferSortPayload(context, keys, values, scratch);
+    gprtBufferMap(keys);
+    gprtBufferMap(values);
+    kp = gprtBufferGetHostPointer(keys);
+    vp = gprtBufferGetHostPointer(values);
+    for (uint32_t i = 0; i < m; ++i) {
+      check(kp[i] == kv[i].first, "u32/u64 pairs: key differs");
+      check(vp[i] == kv[i].second, "u32/u64 pairs: value differs (stability)");
+    }
+    gprtBufferUnmap(keys);
+    gprtBufferUnmap(values);
+    check(gprtcuCompatLastError() == 0, "u32/u64 pairs: error recorded");
+    gprtBufferDestroy(keys);
+    gprtBufferDestroy(values);
+    gprtBufferDestroy(scratch);
+    gprtContextDestroy(context);
+  }
+  {
     // untyped: 64-bit words with 64-bit payloads, stability visible through
     // repeated keys (payload = original index)
     const uint32_t m = n / 8;
