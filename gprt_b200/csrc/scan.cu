@@ -17,8 +17,6 @@
 //     tile lands and reads the tile a second time, from L2, once its prefix
 //     is known, so no tile holds shared memory while it waits.
 // Traffic: 4 B read + 4 B written per element; HBM-bound.
-#include <type_traits>
-
 #include "common.cuh"
 
 namespace gprtcu {
@@ -625,7 +623,29 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
         const uint32_t tc = n - base < (uint64_t)TILE ? (uint32_t)(n - base) : TILE;
         uint32_t *sb = reinterpret_cast<uint32_t *>(sbuf + (size_t)ss * RR_STAGE_BYTES);
         const uint4 *wb = reinterpret_cast<const uint4 *>(sb) + w * 8 * 32;
+        uint4 v[8];
+        uint32_t fl[8], pk[2] = {0u, 0u};
         const uint32_t flip = want_neg ? 0u : 15u;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          v[r] = wb[r * 32 + lane];
+          const uint32_t l0 = (uint32_t)((w * 8 + r) * 128 + lane * 4);
+          const uint32_t rem = tc > l0 ? tc - l0 : 0u;
+          const uint32_t valid = rem >= 4 ? 15u : (1u << rem) - 1u;
+          fl[r] = (((v[r].x >> 31) | ((v[r].y >> 31) << 1) | ((v[r].z >> 31) << 2) | ((v[r].w >> 31) << 3)) ^ flip) & valid;
+          pk[r >> 2] |= (uint32_t)__popc(fl[r]) << (8 * (r & 3));
+        }
+        // Inclusive warp scan of the rows' counts, four rows to a word (a
+        // row's total is at most 128, so a byte holds it).
+        const uint32_t own[2] = {pk[0], pk[1]};
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const uint32_t y = __shfl_up_sync(FULL_MASK, pk[h], o);
+            if (lane >= o) pk[h] += y;
+          }
+        const uint32_t rowtot[2] = {__shfl_sync(FULL_MASK, pk[0], 31), __shfl_sync(FULL_MASK, pk[1], 31)};
         // Selected rank ls goes to out[excl + ls], unselected rank lu to
         // out[top - lu].  Staged at sb[s1 + ls] and sb[u_top - lu], with the
         // shifts chosen so that shared and global indices agree modulo 4:
@@ -634,62 +654,28 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
         const uint64_t top = (n - 1) - (base - excl);
         const uint32_t s1 = (uint32_t)(excl & 3);
         const uint32_t u_top = TILE + 7 + (uint32_t)((top - (TILE + 7)) & 3);  // <= TILE + 10; u_top == top mod 4
-        // FULL: the tile has TILE items, so no row needs its valid-item mask
-        // and no item its bounds test (every tile but the last).
-        auto stage = [&](auto full_tag) {
-          constexpr bool FULL = decltype(full_tag)::value;
-          uint4 v[8];
-          uint32_t fl[8], pk[2] = {0u, 0u};
+        named_bar_sync(1, SW * 32);  // every scanner holds its rows: the stage can be overwritten
 #pragma unroll
-          for (int r = 0; r < 8; ++r) {
-            v[r] = wb[r * 32 + lane];
-            const uint32_t l0 = (uint32_t)((w * 8 + r) * 128 + lane * 4);
-            uint32_t valid = 15u;
-            if (!FULL) {
-              const uint32_t rem = tc > l0 ? tc - l0 : 0u;
-              valid = rem >= 4 ? 15u : (1u << rem) - 1u;
+        for (int r = 0; r < 8; ++r) {
+          const uint32_t sh = 8 * (r & 3);
+          // selected items of the tile before this lane's first in row r
+          uint32_t ls = rowbase + ((pk[r >> 2] - own[r >> 2]) >> sh & 0xFFu);
+          const uint32_t l0 = (uint32_t)((w * 8 + r) * 128 + lane * 4);
+          const uint32_t vals[4] = {v[r].x, v[r].y, v[r].z, v[r].w};
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            const uint32_t sel = (fl[r] >> c) & 1u;
+            if (MODE == 2) {
+              // unselected rank is (l0 + c) - ls
+              const uint32_t at = sel ? s1 + ls : u_top - (l0 + c) + ls;
+              if (l0 + c < tc) sb[at] = vals[c];
+            } else if (sel) {
+              sb[s1 + ls] = vals[c];
             }
-            fl[r] = (((v[r].x >> 31) | ((v[r].y >> 31) << 1) | ((v[r].z >> 31) << 2) | ((v[r].w >> 31) << 3)) ^ flip) &
-                    valid;
-            pk[r >> 2] |= (uint32_t)__popc(fl[r]) << (8 * (r & 3));
+            ls += sel;
           }
-          // Inclusive warp scan of the rows' counts, four rows to a word (a
-          // row's total is at most 128, so a byte holds it).
-          const uint32_t own[2] = {pk[0], pk[1]};
-#pragma unroll
-          for (int o = 1; o < 32; o <<= 1)
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              const uint32_t y = __shfl_up_sync(FULL_MASK, pk[h], o);
-              if (lane >= o) pk[h] += y;
-            }
-          const uint32_t rowtot[2] = {__shfl_sync(FULL_MASK, pk[0], 31), __shfl_sync(FULL_MASK, pk[1], 31)};
-          named_bar_sync(1, SW * 32);  // every scanner holds its rows: the stage can be overwritten
-          uint32_t rb = rowbase;
-#pragma unroll
-          for (int r = 0; r < 8; ++r) {
-            const uint32_t sh = 8 * (r & 3);
-            // selected items of the tile before this lane's first in row r
-            uint32_t ls = rb + ((pk[r >> 2] - own[r >> 2]) >> sh & 0xFFu);
-            const uint32_t l0 = (uint32_t)((w * 8 + r) * 128 + lane * 4);
-            const uint32_t vals[4] = {v[r].x, v[r].y, v[r].z, v[r].w};
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-              const uint32_t sel = (fl[r] >> c) & 1u;
-              if (MODE == 2) {
-                // unselected rank is (l0 + c) - ls
-                const uint32_t at = sel ? s1 + ls : u_top - (l0 + c) + ls;
-                if (FULL || l0 + c < tc) sb[at] = vals[c];
-              } else if (sel) {
-                sb[s1 + ls] = vals[c];
-              }
-              ls += sel;
-            }
-            rb += rowtot[r >> 2] >> sh & 0xFFu;
-          }
-        };
-        if (tc == TILE) stage(std::true_type{});
-        else stage(std::false_type{});
+          rowbase += rowtot[r >> 2] >> sh & 0xFFu;
+        }
         named_bar_sync(1, SW * 32);
         const uint32_t ct = (uint32_t)(tid - 4 * 32);
         // one run: `cnt` words from sb[sidx] to out[gidx], sidx == gidx mod 4

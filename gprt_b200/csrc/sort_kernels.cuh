@@ -113,6 +113,28 @@ template <int BITS> __device__ __forceinline__ unsigned warp_peers(uint32_t d) {
   return m;
 }
 
+// The same peers with four instructions per digit bit: a predicate from one
+// AND, the vote, a select of 0 or ~0 from the predicate, and one
+// three-input logic op m &= votes ^ select (the plain form above compiles to
+// about six per bit).
+template <int BITS> __device__ __forceinline__ unsigned warp_peers_p(uint32_t d) {
+  unsigned m = FULL_MASK;
+#pragma unroll
+  for (int b = 0; b < BITS; ++b) {
+    unsigned bb, t;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "and.b32 %1, %2, %3;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "vote.sync.ballot.b32 %0, p, 0xffffffff;\n\t"
+        "selp.b32 %1, 0, -1, p;\n\t}"
+        : "=r"(bb), "=&r"(t)
+        : "r"(d), "r"(1u << b));
+    m &= bb ^ t;
+  }
+  return m;
+}
+
 __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -637,6 +659,12 @@ __global__ void __launch_bounds__(WARPS * 32, (Pass8Cfg<K, V, WARPS, ITEMS, RANK
       peers = *reinterpret_cast<volatile uint32_t *>(wm + d);
       __syncwarp();
       wm[d] = 0u;
+    } else if constexpr (RANK == 2) {
+      peers = __match_any_sync(FULL_MASK, d);
+      __syncwarp();
+    } else if constexpr (RANK == 3) {
+      peers = warp_peers_p<8>(d);
+      __syncwarp();
     } else {
       peers = warp_peers<8>(d);
       __syncwarp();
@@ -770,8 +798,9 @@ __global__ void k_sort_final_copy(K *keys, const K *keys_alt, V *vals, const V *
 
 // Shared memory a pass kernel of this shape needs.
 // Kernel of the 8-bit passes: 0 = k_sort_pass8 with vote ranking, 1 = the
-// original k_sort_pass, 2 = k_sort_pass8 with shared-memory OR ranking; a
-// test and measurement switch (sort.cu).
+// original k_sort_pass, 2 = k_sort_pass8 with shared-memory OR ranking, 3 =
+// k_sort_pass8 with match.any ranking, 4 = k_sort_pass8 with the predicated
+// vote ranking; a test and measurement switch (sort.cu).
 int gprtcu_sort_ranking();
 
 template <typename K, typename V, int RB, int WARPS, int ITEMS>
@@ -807,6 +836,12 @@ gprtcuStatus sort_run(const SortArgs &a, cudaStream_t stream) {
         if (mode == 2 && !wide)
           st = byte ? launch(k_sort_pass8<K, V, WARPS, ITEMS, true, false, 1>, S1)
                     : launch(k_sort_pass8<K, V, WARPS, ITEMS, false, false, 1>, S1);
+        else if (mode == 3 && !wide)
+          st = byte ? launch(k_sort_pass8<K, V, WARPS, ITEMS, true, false, 2>, S0)
+                    : launch(k_sort_pass8<K, V, WARPS, ITEMS, false, false, 2>, S0);
+        else if (mode == 4 && !wide)
+          st = byte ? launch(k_sort_pass8<K, V, WARPS, ITEMS, true, false, 3>, S0)
+                    : launch(k_sort_pass8<K, V, WARPS, ITEMS, false, false, 3>, S0);
         else if (wide)
           st = byte ? launch(k_sort_pass8<K, V, WARPS, ITEMS, true, true, 0>, S0)
                     : launch(k_sort_pass8<K, V, WARPS, ITEMS, false, true, 0>, S0);

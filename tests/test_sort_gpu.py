@@ -228,7 +228,7 @@ def test_sort_rankings_agree(cuda, kw, vw):
                 v = rng.integers(0, 2 ** 63, size=n, dtype=np.uint64)
                 v = v.astype(np.uint32) if vw == 4 else v
                 ek, ev = oracle.sort(k, v)
-                for mode in (0, 1, 2):
+                for mode in (0, 1, 2, 3, 4):
                     L.gprtcuDebugSortRanking(mode)
                     kt = torch.from_numpy(k.view(np.int32 if kw == 4 else np.int64).copy()).cuda()
                     vt = torch.from_numpy(v.view(np.int32 if vw == 4 else np.int64).copy()).cuda()
