@@ -51,16 +51,15 @@ int grid_index(int rb, int tile, int warps) {
   return -1;
 }
 
-// Shapes used until the tuner or the caller picks others, from a sweep of the
+// Shapes used until the tuner or the caller picks others, from sweeps of the
 // grid on B200 (uniform and Zipf(1.1) keys, 2^18 .. 2^28 elements): 8-bit
-// digits everywhere; 8192-key tiles for 32-bit keys (8 warps without
-// payload, 16 with), 4096-key tiles of 8 warps for 64-bit keys; 2048-key
-// tiles of 8 warps below 2^22 keys, where there are too few large tiles to
-// fill the SMs.
+// digits everywhere; 8192-key tiles of 8 warps for 32-bit keys (2^28 Zipf
+// pairs: 6.20 ms against 6.32 with 16 warps), 4096-key tiles of 8 warps for
+// 64-bit keys; 2048-key tiles of 8 warps below 2^22 keys, where there are too
+// few large tiles to fill the SMs.
 int default_index(int slot, uint64_t n) {
   if (n < (1ull << 22)) return grid_index(8, 2048, 8);
-  if (slot == 0) return grid_index(8, 8192, 8);
-  if (slot == 1) return grid_index(8, 8192, 16);
+  if (slot == 0 || slot == 1 || slot == 5) return grid_index(8, 8192, 8);
   return grid_index(8, 4096, 8);
 }
 

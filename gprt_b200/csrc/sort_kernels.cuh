@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(WARPS * 32, (PassCfg<K, V, RB, WARPS, ITEMS>::
   for (int i = 0; i < ITEMS; ++i) {
     k[i] = s_keys[warp * WK + i * 32 + lane];
     const uint32_t d = digit_of(k[i], shift, mask);
-    const unsigned peers = warp_peers<RB>(d);
+    const unsigned peers = warp_peers_p<RB>(d);
     const uint32_t base = wh[d];
     __syncwarp();
     if (lane == 31 - __clz(peers)) wh[d] = base + __popc(peers);
@@ -663,10 +663,10 @@ __global__ void __launch_bounds__(WARPS * 32, (Pass8Cfg<K, V, WARPS, ITEMS, RANK
       peers = __match_any_sync(FULL_MASK, d);
       __syncwarp();
     } else if constexpr (RANK == 3) {
-      peers = warp_peers_p<8>(d);
+      peers = warp_peers<8>(d);  // the plain form of the votes, for comparison
       __syncwarp();
     } else {
-      peers = warp_peers<8>(d);
+      peers = warp_peers_p<8>(d);
       __syncwarp();
     }
     wc[d] = base + __popc(peers);  // every peer stores the same count
@@ -797,10 +797,10 @@ __global__ void k_sort_final_copy(K *keys, const K *keys_alt, V *vals, const V *
 }
 
 // Shared memory a pass kernel of this shape needs.
-// Kernel of the 8-bit passes: 0 = k_sort_pass8 with vote ranking, 1 = the
-// original k_sort_pass, 2 = k_sort_pass8 with shared-memory OR ranking, 3 =
-// k_sort_pass8 with match.any ranking, 4 = k_sort_pass8 with the predicated
-// vote ranking; a test and measurement switch (sort.cu).
+// Kernel of the 8-bit passes: 0 = k_sort_pass8 (predicated votes), 1 = the
+// original k_sort_pass, 2 = k_sort_pass8 ranking by shared-memory OR words,
+// 3 = k_sort_pass8 ranking by match.any, 4 = k_sort_pass8 with the plain
+// votes; a test and measurement switch (sort.cu).
 int gprtcu_sort_ranking();
 
 template <typename K, typename V, int RB, int WARPS, int ITEMS>
