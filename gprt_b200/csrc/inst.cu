@@ -121,17 +121,9 @@ constexpr int kInstRefill = 4;
 // One lane per ray from a global counter, warp-uniform visit loop; lanes
 // whose rays finished take new rays once kInstRefill of the 32 are idle
 // (16,384 instances, 16.8M rays: 32 rays per warp without refill 147 ms,
-// refill at 16 / 8 / 4 idle lanes 119.6 / 109.5 / 105.7 ms).  Both levels
-// share one node step: the top level's nodes and every mesh's nodes have the
-// same two-box layout, so a lane walks whichever level it is in with the same
-// instructions (world ray at the top, the instance's object-space ray below)
-// and only entering an instance and testing triangles are level-specific.
-// (Separate top- and bottom-level steps made the warp run both whenever its
-// lanes were split between the levels.)  One stack holds references of both
-// levels with their entry distances (a bit per entry says which level), so a
-// popped reference behind the best hit is dropped at either level; a mesh's
-// entries lie above the top-level entries pushed before the instance was
-// entered, so popping past them returns the lane to the world ray.
+// refill at 16 / 8 / 4 idle lanes 119.6 / 109.5 / 105.7 ms).  The top-level stack holds references (inner node >= 0, leaf
+// ~slot) with their entry distances, so a popped reference behind the best hit
+// is dropped; the bottom-level stack holds node indices.
 template <bool ANY>
 __global__ void __launch_bounds__(kInstThreads) k_trace_inst(const Bvh2Node *tnodes, const uint32_t *tids, uint32_t ninst,
                                                              const float *troot, const InstanceRec *inst,
@@ -140,20 +132,20 @@ __global__ void __launch_bounds__(kInstThreads) k_trace_inst(const Bvh2Node *tno
                                                              uint64_t nrays, uint32_t ray_mask, Hit *hits,
                                                              uint32_t *hit_inst, unsigned long long *counter,
                                                              uint32_t *err) {
-  static_assert(kInstStack <= 64, "one bit per stack entry in a 64-bit word");
   const int lane = threadIdx.x & 31;
   const uint32_t lt = (1u << lane) - 1u;
   bool active = false, drained = false, done = true;
   uint64_t r = 0;
-  Ray W, C;  // world ray; current ray (W at the top level, object space inside an instance)
+  Ray W, O;
   uint32_t best = kMiss, binst = kMiss, bslot = 0;
   float bt = 0.0f;
-  int sref[kInstStack];
-  float stn[kInstStack];
-  uint64_t slev = 0;  // bit k: entry k belongs to a mesh (bottom level)
-  int sp = 0;
-  int level = 0, node = 0;  // top level: node >= 0 inner, < 0 instance leaf ~slot; bottom level: inner node
-  uint32_t ci = 0;          // instance being walked
+  int tref[kInstStack];
+  float ttn[kInstStack];
+  int tsp = 0;
+  int bstack[kInstStack];
+  int bsp = 0;
+  int level = 0, cur = 0, bnode = 0;
+  uint32_t ci = 0;  // instance being walked
   const Bvh2Node *bvh = blas_all;
   const float4 *leaf = leaf_all;
   auto tri_test = [&](uint32_t slot) {
@@ -162,7 +154,7 @@ __global__ void __launch_bounds__(kInstThreads) k_trace_inst(const Bvh2Node *tno
     const float v0[3] = {a.x, a.y, a.z}, v1[3] = {b.x, b.y, b.z}, v2[3] = {c.x, c.y, c.z};
     const uint32_t id = __float_as_uint(a.w);
     float t;
-    if (isect_tri(C, v0, v1, v2, t) &&
+    if (isect_tri(O, v0, v1, v2, t) &&
         (best == kMiss || t < bt || (t == bt && (ci < binst || (ci == binst && id < best))))) {
       best = id;
       binst = ci;
@@ -170,36 +162,19 @@ __global__ void __launch_bounds__(kInstThreads) k_trace_inst(const Bvh2Node *tno
       bt = t;
     }
   };
-  // next reference from the stack (entries behind the best hit dropped),
-  // back to the world ray when it is a top-level one
-  auto pop = [&]() {
-    while (sp > 0) {
-      --sp;
-      if (stn[sp] <= bt) {
-        node = sref[sp];
-        const int lev = (int)((slev >> sp) & 1ull);
-        if (lev != level) {
-          level = lev;
-          C = W;
-        }
+  auto pop_top = [&]() {
+    while (tsp > 0) {
+      --tsp;
+      if (ttn[tsp] <= bt) {
+        cur = tref[tsp];
         return;
       }
     }
     done = true;
   };
-  auto push = [&](int ref, float tn) {
-    if (sp < kInstStack) {
-      sref[sp] = ref;
-      stn[sp] = tn;
-      slev = (slev & ~(1ull << sp)) | ((uint64_t)level << sp);
-      ++sp;
-      return true;
-    }
-    atomicCAS(err, 0u, 5u);  // traversal stack overflow
-    done = true;
-    return false;
-  };
   while (true) {
+    // Lanes whose rays finished take new ones once kInstRefill of the warp's
+    // 32 are idle (rays differ widely in how many instances they enter).
     const unsigned idle = __ballot_sync(FULL_MASK, !active);
     const int n_idle = __popc(idle);
     if (!drained && (n_idle >= kInstRefill || n_idle == 32)) {
@@ -214,17 +189,18 @@ __global__ void __launch_bounds__(kInstThreads) k_trace_inst(const Bvh2Node *tno
           active = true;
           done = false;
           ray_setup(__ldg(rays + 2 * r), __ldg(rays + 2 * r + 1), W);
-          C = W;
+          O = W;
           best = kMiss;
           binst = kMiss;
           bslot = 0;
           bt = W.tmax;
-          sp = 0;
+          tsp = 0;
+          bsp = 0;
           level = 0;
-          node = 0;
+          cur = 0;
           if (ninst == 1) {
             float tn;
-            node = ~0;  // the single instance is the root leaf
+            cur = ~0;  // the single instance is the root leaf
             if (!ray_box(W, troot[0], troot[1], troot[2], troot[3], troot[4], troot[5], bt, tn)) done = true;
           }
         }
@@ -235,49 +211,80 @@ __global__ void __launch_bounds__(kInstThreads) k_trace_inst(const Bvh2Node *tno
       continue;
     }
     if (active && !done) {
-      if (level == 1 || node >= 0) {
-        // ---- an inner node of either level
-        const float4 *np = reinterpret_cast<const float4 *>((level ? bvh : tnodes) + node);
+      if (level == 1) {
+        // ---- bottom level: the instance's mesh in object space
+        const float4 *np = reinterpret_cast<const float4 *>(bvh + bnode);
         const float4 f0 = __ldg(np), f1 = __ldg(np + 1), f2 = __ldg(np + 2);
         const int4 rf = __ldg(reinterpret_cast<const int4 *>(np + 3));
         float tn0, tn1;
-        bool h0 = ray_box(C, f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, bt, tn0) && tn0 <= bt;
-        bool h1 = ray_box(C, f1.z, f1.w, f2.x, f2.y, f2.z, f2.w, bt, tn1) && tn1 <= bt;
-        if (level == 1) {
-          // a mesh's leaves are triangles, tested at once; the top level's
-          // leaves are instances, entered when visited
-          if (h0 && rf.x < 0) {
-            tri_test((uint32_t)~rf.x);
-            h0 = false;
-          }
-          if (h1 && rf.y < 0) {
-            if (tn1 <= bt) tri_test((uint32_t)~rf.y);
-            h1 = false;
-          }
-          if (h1 && tn1 > bt) h1 = false;
+        bool h0 = ray_box(O, f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, bt, tn0) && tn0 <= bt;
+        bool h1 = ray_box(O, f1.z, f1.w, f2.x, f2.y, f2.z, f2.w, bt, tn1) && tn1 <= bt;
+        if (h0 && rf.x < 0) {
+          tri_test((uint32_t)~rf.x);
+          h0 = false;
         }
+        if (h1 && rf.y < 0) {
+          if (tn1 <= bt) tri_test((uint32_t)~rf.y);
+          h1 = false;
+        }
+        if (h1 && tn1 > bt) h1 = false;
         if (ANY && best != kMiss) {
           done = true;
         } else if (h0 && h1) {
           const bool first0 = tn0 <= tn1;
-          if (push(first0 ? rf.y : rf.x, first0 ? tn1 : tn0)) node = first0 ? rf.x : rf.y;
+          if (bsp < kInstStack) {
+            bstack[bsp++] = first0 ? rf.y : rf.x;
+            bnode = first0 ? rf.x : rf.y;
+          } else {
+            atomicCAS(err, 0u, 5u);  // traversal stack overflow
+            done = true;
+          }
         } else if (h0) {
-          node = rf.x;
+          bnode = rf.x;
         } else if (h1) {
-          node = rf.y;
+          bnode = rf.y;
+        } else if (bsp > 0) {
+          bnode = bstack[--bsp];
         } else {
-          pop();
+          level = 0;  // back to the top level
+          pop_top();
+        }
+      } else if (cur >= 0) {
+        // ---- top level, inner node
+        const float4 *np = reinterpret_cast<const float4 *>(tnodes + cur);
+        const float4 f0 = __ldg(np), f1 = __ldg(np + 1), f2 = __ldg(np + 2);
+        const int4 rf = __ldg(reinterpret_cast<const int4 *>(np + 3));
+        float tn0, tn1;
+        const bool h0 = ray_box(W, f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, bt, tn0) && tn0 <= bt;
+        const bool h1 = ray_box(W, f1.z, f1.w, f2.x, f2.y, f2.z, f2.w, bt, tn1) && tn1 <= bt;
+        if (h0 && h1) {
+          const bool first0 = tn0 <= tn1;
+          if (tsp < kInstStack) {
+            tref[tsp] = first0 ? rf.y : rf.x;
+            ttn[tsp] = first0 ? tn1 : tn0;
+            ++tsp;
+            cur = first0 ? rf.x : rf.y;
+          } else {
+            atomicCAS(err, 0u, 5u);
+            done = true;
+          }
+        } else if (h0) {
+          cur = rf.x;
+        } else if (h1) {
+          cur = rf.y;
+        } else {
+          pop_top();
         }
       } else {
-        // ---- a top-level leaf: enter the instance's mesh in object space
-        ci = __ldg(tids + (uint32_t)~node);
+        // ---- top level, an instance: enter its mesh in object space
+        ci = __ldg(tids + (uint32_t)~cur);
         const uint32_t cm = __ldg(&inst[ci].custom_mask);
         const uint32_t mesh = (uint32_t)__ldg(&inst[ci].blas);
         bool entered = false;
         if (((cm >> 24) & ray_mask) && mesh < im.meshes) {
           const float *w = w2o + 12 * (size_t)ci;
           if (__ldg(w) != 0.0f || __ldg(w + 1) != 0.0f || __ldg(w + 2) != 0.0f) {  // singular: all zero
-            ray_to_object(w, W, C);
+            ray_to_object(w, W, O);
             const uint32_t b = im.tri_off ? __ldg(im.tri_off + mesh) : 0u;
             const uint32_t cnt = im.tri_off ? __ldg(im.tri_off + mesh + 1) - b : im.n_all;
             bvh = blas_all + (b - mesh);
@@ -285,21 +292,21 @@ __global__ void __launch_bounds__(kInstThreads) k_trace_inst(const Bvh2Node *tno
             if (cnt == 1) {
               const float4 a = __ldg(leaf), bb = __ldg(leaf + 1), c = __ldg(leaf + 2);
               float tn;
-              if (ray_box(C, fminf(a.x, fminf(bb.x, c.x)), fminf(a.y, fminf(bb.y, c.y)), fminf(a.z, fminf(bb.z, c.z)),
+              if (ray_box(O, fminf(a.x, fminf(bb.x, c.x)), fminf(a.y, fminf(bb.y, c.y)), fminf(a.z, fminf(bb.z, c.z)),
                           fmaxf(a.x, fmaxf(bb.x, c.x)), fmaxf(a.y, fmaxf(bb.y, c.y)), fmaxf(a.z, fmaxf(bb.z, c.z)), bt,
                           tn) &&
                   tn <= bt)
                 tri_test(0);
               if (ANY && best != kMiss) done = true;
-              C = W;  // still at the top level
             } else {
               level = 1;
-              node = 0;
+              bnode = 0;
+              bsp = 0;
               entered = true;
             }
           }
         }
-        if (!entered && !done) pop();
+        if (!entered && !done) pop_top();
       }
     }
     if (active && done) {
@@ -308,7 +315,6 @@ __global__ void __launch_bounds__(kInstThreads) k_trace_inst(const Bvh2Node *tno
       h.t = __int_as_float(0x7f800000);
       if (best != kMiss) {
         // the winner's object-space ray again (same operations, same bits)
-        Ray O;
         ray_to_object(w2o + 12 * (size_t)binst, W, O);
         const uint32_t mesh = (uint32_t)__ldg(&inst[binst].blas);
         const uint32_t b = im.tri_off ? __ldg(im.tri_off + mesh) : 0u;
