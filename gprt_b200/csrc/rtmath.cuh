@@ -52,10 +52,11 @@ __device__ __forceinline__ void ray_setup(const float4 a, const float4 b, Ray &r
   r.kx = kx; r.ky = ky; r.kz = kz;
   r.Sx = __fdiv_rn(pick3(b.x, b.y, b.z, kx), dkz);
   r.Sy = __fdiv_rn(pick3(b.x, b.y, b.z, ky), dkz);
-  r.Sz = __fdiv_rn(1.0f, dkz);
-  r.ix = __fdiv_rn(1.0f, b.x);
-  r.iy = __fdiv_rn(1.0f, b.y);
-  r.iz = __fdiv_rn(1.0f, b.z);
+  // correctly rounded reciprocals: the values of 1.0f / x, without a division
+  r.Sz = __frcp_rn(dkz);
+  r.ix = __frcp_rn(b.x);
+  r.iy = __frcp_rn(b.y);
+  r.iz = __frcp_rn(b.z);
 }
 
 // a*d - b*c, Kahan's algorithm (one FMA-corrected product).

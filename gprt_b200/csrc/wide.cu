@@ -348,30 +348,6 @@ __device__ __forceinline__ void wide_leaf_test(const float4 *leaf, uint32_t i, c
   }
 }
 
-// One lane per ray.  Per node: the ray is moved into the node's quantised
-// frame once, the eight child boxes are tested two at a time with packed
-// f32x2 arithmetic (byte decode, directed-rounding slab FMAs, the 2^-18
-// widening) and three-input min/max, and only then are the hit leaf
-// children's triangles tested (the lanes with leaf hits run those tests
-// together, whatever slots they are in; testing them inside the child loop
-// ran each slot's test separately with few lanes active).  Absent children
-// are inverted boxes and need no test of their own.  The nearest hit inner
-// child is found inside the box loop and entered; the other hit inner
-// children are pushed as one entry {child_base, slot mask | inner mask << 8}
-// and a popped slot's node is child_base + the inner children below it.
-// Lanes are refilled as their rays finish: when at least kWideRefill lanes of
-// a warp are idle, the warp takes that many new rays from the global counter
-// (waiting for the whole warp to finish left most lanes idle behind the
-// longest ray); a refilled ray's mesh is found by galloping forward from the
-// warp's previous mesh (the ray counter only grows) instead of bisecting all
-// ray offsets (59.2 -> 57.5 ms).  On 16.7M rays of one 16.7M-triangle mesh and on 134M rays
-// over 16,384 meshes, thresholds of 4, 8, 16 and 32 (no refill) idle lanes
-// measured 33.6 / 34.7 / 38.5 / 63.7 ms and 71.3 / 69.0 / 74.8 / 155.5 ms;
-// testing leaf triangles inside the child loop instead measured 174.7 ms on
-// the second.  The packed box loop took the second from 68.7 to 59.2 ms.
-// Keeping a lane's leaf tests pending across nodes until enough lanes had
-// some measured 76.4 ms: lanes finishing with tests pending forced most
-// flushes, and the extra state spilled.
 // Largest m < meshes with off[m] <= r, given off[m0] <= r: gallop upward
 // from m0, then bisect.  off has meshes + 1 entries, off[meshes] > r.
 __device__ __forceinline__ uint32_t mesh_from(const uint32_t *off, uint32_t meshes, uint32_t m0, uint64_t r) {
@@ -390,13 +366,229 @@ __device__ __forceinline__ uint32_t mesh_from(const uint32_t *off, uint32_t mesh
   return lo;
 }
 
-template <bool ANY, bool BATCHED>
-__global__ void __launch_bounds__(kWideThreads, 8)
-    k_trace_wide(const WideNode *nodes, const float4 *leaf, const uint32_t *roots, const uint32_t *ray_off,
-                    uint32_t meshes, const float4 *rays, uint64_t nrays, Hit *hits, unsigned long long *counter,
-                    uint32_t *err) {
+// Lane refill.  When at least kWideRefill lanes of a warp are idle (or all
+// are), the warp takes that many new rays from the global counter (waiting
+// for the whole warp to finish left most lanes idle behind the longest ray).
+// On 16.7M rays of one 16.7M-triangle mesh and on 134M rays over 16,384
+// meshes, thresholds of 4, 8, 16 and 32 (no refill) idle lanes measured
+// 33.6 / 34.7 / 38.5 / 63.7 ms and 71.3 / 69.0 / 74.8 / 155.5 ms.  The
+// counter only grows, so the mesh of the first new ray is at or after the
+// warp's previous mesh: the 32 lanes probe the next 32 mesh offsets at once
+// (one load latency instead of a serial gallop), and a lane whose ray lies
+// before the end of that mesh needs no search of its own.  Called by all 32
+// lanes; returns true on the lanes that took a ray (their traversal state is
+// then reset by the caller).
+template <bool BATCHED>
+__device__ __forceinline__ bool wide_take_ray(bool &active, bool &drained, uint32_t &warp_mesh, uint64_t &r,
+                                              Ray &R, uint32_t &node, const uint32_t *roots,
+                                              const uint32_t *ray_off, uint32_t meshes, const float4 *rays,
+                                              uint64_t nrays, unsigned long long *counter) {
   const int lane = threadIdx.x & 31;
-  const uint32_t lt = (1u << lane) - 1u;
+  const unsigned idle = __ballot_sync(FULL_MASK, !active);
+  const int n_idle = __popc(idle);
+  if (drained || (n_idle < kWideRefill && n_idle != 32)) return false;
+  unsigned long long base = 0;
+  if (lane == 0) base = atomicAdd(counter, (unsigned long long)n_idle);
+  base = __shfl_sync(FULL_MASK, base, 0);
+  if (base + n_idle >= nrays) drained = true;
+  uint64_t mesh_end = 0;  // first ray after warp_mesh
+  if (BATCHED && base < nrays) {
+    while (true) {
+      const uint32_t j = warp_mesh + 1 + lane;
+      const uint32_t v = j <= meshes ? __ldg(ray_off + j) : 0xFFFFFFFFu;
+      const int k = __popc(__ballot_sync(FULL_MASK, j < meshes && v <= base));  // a prefix of the lanes
+      warp_mesh += k;
+      if (k < 32) {
+        mesh_end = __shfl_sync(FULL_MASK, v, k);
+        break;
+      }
+    }
+  }
+  if (active) return false;
+  const uint64_t mine = base + __popc(idle & ((1u << lane) - 1u));
+  if (mine >= nrays) return false;
+  r = mine;
+  active = true;
+  ray_setup(__ldg(rays + 2 * r), __ldg(rays + 2 * r + 1), R);
+  uint32_t m = 0;
+  if (BATCHED) m = mine < mesh_end ? warp_mesh : mesh_from(ray_off, meshes, warp_mesh, r);
+  node = __ldg(roots + m);
+  return true;
+}
+
+// One node step: the ray is moved into the node's quantised frame once, the
+// eight child boxes are tested two at a time with packed f32x2 arithmetic
+// (byte decode, directed-rounding slab FMAs, the 2^-18 widening) and
+// three-input min/max (68.7 -> 60.7 ms on the 134M-ray workload against the
+// scalar loop).  Absent children are inverted boxes and need no test of their
+// own.  The nearest hit inner child is found inside the box loop.
+struct WideStep {
+  uint32_t hm;  // slots whose box is hit
+  uint32_t imask, child_base, leaf_base, meta_lo, meta_hi;
+  int ns;  // nearest hit inner slot, -1 if none
+};
+
+__device__ __forceinline__ WideStep wide_node_step(const WideNode *nodes, uint32_t node, const Ray &R, float bt) {
+  WideStep S;
+  const uint4 *np = reinterpret_cast<const uint4 *>(nodes + node);
+  const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+  const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
+  const float sx = scale_of((int8_t)(w0.w & 0xFF)), sy = scale_of((int8_t)((w0.w >> 8) & 0xFF)),
+              sz = scale_of((int8_t)((w0.w >> 16) & 0xFF));
+  S.imask = w0.w >> 24;
+  S.child_base = w1.x;
+  S.leaf_base = w1.y;
+  S.meta_lo = w1.z;
+  S.meta_hi = w1.w;
+  float An[3], Af[3], Bq[3];
+  uint32_t qn[3][2], qf[3][2];
+  {
+    const float pa[3] = {px, py, pz}, oa[3] = {R.ox, R.oy, R.oz}, ia[3] = {R.ix, R.iy, R.iz};
+    const float sa[3] = {sx, sy, sz};
+    const uint32_t ql[3][2] = {{w2.x, w2.y}, {w2.z, w2.w}, {w3.x, w3.y}};
+    const uint32_t qh[3][2] = {{w3.z, w3.w}, {w4.x, w4.y}, {w4.z, w4.w}};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float dlo = __fsub_rd(pa[a], oa[a]), dhi = __fsub_ru(pa[a], oa[a]);
+      const bool pos = !(ia[a] < 0.0f);
+      An[a] = __fmul_rd(pos ? dlo : dhi, ia[a]);
+      Af[a] = __fmul_ru(pos ? dhi : dlo, ia[a]);
+      Bq[a] = __fmul_rn(sa[a], ia[a]);
+      qn[a][0] = pos ? ql[a][0] : qh[a][0];
+      qn[a][1] = pos ? ql[a][1] : qh[a][1];
+      qf[a][0] = pos ? qh[a][0] : ql[a][0];
+      qf[a][1] = pos ? qh[a][1] : ql[a][1];
+    }
+  }
+  uint32_t hm = 0;
+  float nt = __int_as_float(0x7f800000);
+  int ns = -1;
+  {
+    const unsigned long long bias = pk2(-8388608.0f, -8388608.0f);
+    const unsigned long long lo2 = pk2(kBoxLo, kBoxLo), hi2 = pk2(kBoxHi, kBoxHi);
+    unsigned long long B2[3], N2[3], F2[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      B2[a] = pk2(Bq[a], Bq[a]);
+      N2[a] = pk2(An[a], An[a]);
+      F2[a] = pk2(Af[a], Af[a]);
+    }
+#pragma unroll
+    for (int cp = 0; cp < 4; ++cp) {
+      const int h = cp >> 1;
+      const uint32_t s0 = 0x7540u | (uint32_t)((2 * cp) & 3), s1 = 0x7540u | (uint32_t)((2 * cp + 1) & 3);
+      float n[2][3], f[2][3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const unsigned long long qn2 = pk2(__uint_as_float(__byte_perm(qn[a][h], 0x4B000000u, s0)),
+                                           __uint_as_float(__byte_perm(qn[a][h], 0x4B000000u, s1)));
+        const unsigned long long qf2 = pk2(__uint_as_float(__byte_perm(qf[a][h], 0x4B000000u, s0)),
+                                           __uint_as_float(__byte_perm(qf[a][h], 0x4B000000u, s1)));
+        up2(fma2_rd(add2_rn(qn2, bias), B2[a], N2[a]), n[0][a], n[1][a]);
+        up2(fma2_ru(add2_rn(qf2, bias), B2[a], F2[a]), f[0][a], f[1][a]);
+      }
+      float tn[2], tf[2];
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        tn[k] = fmaxf(max3f(n[k][0], n[k][1], n[k][2]), R.tmin);
+        tf[k] = fminf(min3f(f[k][0], f[k][1], f[k][2]), bt);
+      }
+      up2(mul2_rn(pk2(tn[0], tn[1]), lo2), tn[0], tn[1]);
+      up2(mul2_rn(pk2(tf[0], tf[1]), hi2), tf[0], tf[1]);
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const int c = 2 * cp + k;
+        const bool hit = tn[k] <= tf[k] && tn[k] <= bt;
+        hm |= (uint32_t)hit << c;
+        if (hit && ((S.imask >> c) & 1u) && tn[k] < nt) {
+          nt = tn[k];
+          ns = c;
+        }
+      }
+    }
+  }
+  S.hm = hm;
+  S.ns = ns;
+  return S;
+}
+
+// The next node: the nearest hit inner child is entered and the other hit
+// inner children are pushed as one entry {child_base, slot mask | inner mask
+// << 8} (a popped slot's node is child_base + the inner children below it);
+// with no inner child hit, the top entry's lowest slot is popped.  Returns
+// false when the traversal is over (or the stack overflowed: status 5).
+__device__ __forceinline__ bool wide_next(const WideStep &S, uint2 *stack, int &sp, uint32_t &node, uint32_t *err) {
+  if (S.ns >= 0) {
+    const uint32_t rest = S.hm & S.imask & ~(1u << S.ns);
+    if (rest) {
+      if (sp >= kWideStack) {
+        atomicCAS(err, 0u, 5u);  // traversal stack overflow
+        return false;
+      }
+      stack[sp++] = make_uint2(S.child_base, rest | (S.imask << 8));
+    }
+    node = S.child_base + (uint32_t)__popc(S.imask & ((1u << S.ns) - 1u));
+    return true;
+  }
+  if (sp > 0) {
+    uint2 &top = stack[sp - 1];
+    const uint32_t c = __ffs(top.y & 0xFFu) - 1;
+    top.y &= ~(1u << c);
+    node = top.x + (uint32_t)__popc((top.y >> 8) & ((1u << c) - 1u));
+    if ((top.y & 0xFFu) == 0) --sp;
+    return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ uint32_t wide_leaf_meta(const WideStep &S, int c) {
+  return ((c < 4 ? S.meta_lo : S.meta_hi) >> (8 * (c & 3))) & 0xFF;
+}
+
+// A finished ray's record: the primitive id and, until k_wide_refine
+// replaces it by t, the leaf slot of the triangle hit.
+__device__ __forceinline__ Hit wide_result(uint32_t best, uint32_t best_leaf) {
+  Hit out;
+  out.prim = best;
+  out.t = best != kMiss ? __uint_as_float(best_leaf) : __int_as_float(0x7f800000);
+  return out;
+}
+
+// t of every hit: the plane-equation distance of the hit triangle in
+// double-float, rounded once.  Run after the traversal over all rays at once
+// (coalesced, every lane busy) instead of by each lane as its ray finished,
+// when few lanes of the warp ran it and the rest waited.
+__global__ void __launch_bounds__(256) k_wide_refine(const float4 *leaf, const float4 *rays, uint64_t nrays,
+                                                     Hit *hits) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nrays;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const Hit h = hits[i];
+    if (h.prim == kMiss) continue;
+    const uint32_t slot = __float_as_uint(h.t);
+    const float4 o = __ldg(rays + 2 * i), d = __ldg(rays + 2 * i + 1);
+    Ray R;
+    R.ox = o.x;
+    R.oy = o.y;
+    R.oz = o.z;
+    R.dx = d.x;
+    R.dy = d.y;
+    R.dz = d.z;
+    const float4 a = __ldg(leaf + 3 * (size_t)slot), b = __ldg(leaf + 3 * (size_t)slot + 1),
+                 c = __ldg(leaf + 3 * (size_t)slot + 2);
+    const float v0[3] = {a.x, a.y, a.z}, v1[3] = {b.x, b.y, b.z}, v2[3] = {c.x, c.y, c.z};
+    hits[i].t = refine_t(R, v0, v1, v2);
+  }
+}
+
+// Any hit: one lane per ray; after a node's box loop the lanes with hit leaf
+// children test those triangles together, whatever slots they are in (testing
+// them inside the child loop ran each slot's test separately with few lanes
+// active), and the first hit ends the ray.
+template <bool BATCHED>
+__global__ void __launch_bounds__(kWideThreads, 8)
+    k_trace_wide_any(const WideNode *nodes, const float4 *leaf, const uint32_t *roots, const uint32_t *ray_off,
+                     uint32_t meshes, const float4 *rays, uint64_t nrays, Hit *hits, unsigned long long *counter,
+                     uint32_t *err) {
   bool active = false, drained = false;
   uint64_t r = 0;
   Ray R;
@@ -406,183 +598,190 @@ __global__ void __launch_bounds__(kWideThreads, 8)
   uint32_t warp_mesh = 0;  // a mesh at or below every ray this warp will still take
   int sp = 0;
   while (true) {
-    const unsigned idle = __ballot_sync(FULL_MASK, !active);
-    const int n_idle = __popc(idle);
-    if (!drained && (n_idle >= kWideRefill || n_idle == 32)) {
-      unsigned long long base = 0;
-      if (lane == 0) base = atomicAdd(counter, (unsigned long long)n_idle);
-      base = __shfl_sync(FULL_MASK, base, 0);
-      if (base + n_idle >= nrays) drained = true;
-      if (BATCHED && base < nrays) {
-        // the counter only grows: search forward from this warp's last mesh
-        if (lane == 0) warp_mesh = mesh_from(ray_off, meshes, warp_mesh, base);
-        warp_mesh = __shfl_sync(FULL_MASK, warp_mesh, 0);
-      }
-      if (!active) {
-        const uint64_t mine = base + __popc(idle & lt);
-        if (mine < nrays) {
-          r = mine;
-          active = true;
-          ray_setup(__ldg(rays + 2 * r), __ldg(rays + 2 * r + 1), R);
-          uint32_t m = 0;
-          if (BATCHED) m = mesh_from(ray_off, meshes, warp_mesh, r);
-          node = __ldg(roots + m);
-          best = kMiss;
-          best_leaf = 0;
-          bt = R.tmax;
-          sp = 0;
-        }
-      }
+    if (wide_take_ray<BATCHED>(active, drained, warp_mesh, r, R, node, roots, ray_off, meshes, rays, nrays,
+                               counter)) {
+      best = kMiss;
+      best_leaf = 0;
+      bt = R.tmax;
+      sp = 0;
     }
     if (!__any_sync(FULL_MASK, active)) {
       if (drained) break;
       continue;
     }
     if (!active) continue;
-
-    const uint4 *np = reinterpret_cast<const uint4 *>(nodes + node);
-    const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
-    const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
-    const float sx = scale_of((int8_t)(w0.w & 0xFF)), sy = scale_of((int8_t)((w0.w >> 8) & 0xFF)),
-                sz = scale_of((int8_t)((w0.w >> 16) & 0xFF));
-    const uint32_t imask = w0.w >> 24;
-    const uint32_t child_base = w1.x, leaf_base = w1.y;
-    const uint32_t meta_lo = w1.z, meta_hi = w1.w;
-    float An[3], Af[3], Bq[3];
-    uint32_t qn[3][2], qf[3][2];
-    {
-      const float pa[3] = {px, py, pz}, oa[3] = {R.ox, R.oy, R.oz}, ia[3] = {R.ix, R.iy, R.iz};
-      const float sa[3] = {sx, sy, sz};
-      const uint32_t ql[3][2] = {{w2.x, w2.y}, {w2.z, w2.w}, {w3.x, w3.y}};
-      const uint32_t qh[3][2] = {{w3.z, w3.w}, {w4.x, w4.y}, {w4.z, w4.w}};
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const float dlo = __fsub_rd(pa[a], oa[a]), dhi = __fsub_ru(pa[a], oa[a]);
-        const bool pos = !(ia[a] < 0.0f);
-        An[a] = __fmul_rd(pos ? dlo : dhi, ia[a]);
-        Af[a] = __fmul_ru(pos ? dhi : dlo, ia[a]);
-        Bq[a] = __fmul_rn(sa[a], ia[a]);
-        qn[a][0] = pos ? ql[a][0] : qh[a][0];
-        qn[a][1] = pos ? ql[a][1] : qh[a][1];
-        qf[a][0] = pos ? qh[a][0] : ql[a][0];
-        qf[a][1] = pos ? qh[a][1] : ql[a][1];
-      }
-    }
-    float ctn[8];
-    uint32_t hm = 0;  // slots whose box is hit
-    float nt = __int_as_float(0x7f800000);
-    int ns = -1;  // nearest hit inner slot
-    {
-      const unsigned long long bias = pk2(-8388608.0f, -8388608.0f);
-      const unsigned long long lo2 = pk2(kBoxLo, kBoxLo), hi2 = pk2(kBoxHi, kBoxHi);
-      unsigned long long B2[3], N2[3], F2[3];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        B2[a] = pk2(Bq[a], Bq[a]);
-        N2[a] = pk2(An[a], An[a]);
-        F2[a] = pk2(Af[a], Af[a]);
-      }
-#pragma unroll
-      for (int cp = 0; cp < 4; ++cp) {
-        const int h = cp >> 1;
-        const uint32_t s0 = 0x7540u | (uint32_t)((2 * cp) & 3), s1 = 0x7540u | (uint32_t)((2 * cp + 1) & 3);
-        float n[2][3], f[2][3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          const unsigned long long qn2 = pk2(__uint_as_float(__byte_perm(qn[a][h], 0x4B000000u, s0)),
-                                             __uint_as_float(__byte_perm(qn[a][h], 0x4B000000u, s1)));
-          const unsigned long long qf2 = pk2(__uint_as_float(__byte_perm(qf[a][h], 0x4B000000u, s0)),
-                                             __uint_as_float(__byte_perm(qf[a][h], 0x4B000000u, s1)));
-          up2(fma2_rd(add2_rn(qn2, bias), B2[a], N2[a]), n[0][a], n[1][a]);
-          up2(fma2_ru(add2_rn(qf2, bias), B2[a], F2[a]), f[0][a], f[1][a]);
-        }
-        float tn[2], tf[2];
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          tn[k] = fmaxf(max3f(n[k][0], n[k][1], n[k][2]), R.tmin);
-          tf[k] = fminf(min3f(f[k][0], f[k][1], f[k][2]), bt);
-        }
-        up2(mul2_rn(pk2(tn[0], tn[1]), lo2), tn[0], tn[1]);
-        up2(mul2_rn(pk2(tf[0], tf[1]), hi2), tf[0], tf[1]);
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          const int c = 2 * cp + k;
-          ctn[c] = tn[k];
-          const bool hit = tn[k] <= tf[k] && tn[k] <= bt;
-          hm |= (uint32_t)hit << c;
-          if (hit && ((imask >> c) & 1u) && tn[k] < nt) {
-            nt = tn[k];
-            ns = c;
-          }
-        }
-      }
-    }
-    const uint32_t inner_hit = hm & imask;
-    uint32_t leaf_hit = hm & ~imask;
-    const float bt_before = bt;
-    // deferred triangle tests: lanes with leaf hits run them together
+    const WideStep S = wide_node_step(nodes, node, R, bt);
+    uint32_t leaf_hit = S.hm & ~S.imask;
     while (leaf_hit) {
       const int c = __ffs(leaf_hit) - 1;
       leaf_hit &= leaf_hit - 1u;
-      const uint32_t meta = ((c < 4 ? meta_lo : meta_hi) >> (8 * (c & 3))) & 0xFF;
-      if (meta != 0xFF) wide_leaf_test(leaf, leaf_base + meta, R, best, best_leaf, bt);
+      const uint32_t meta = wide_leaf_meta(S, c);
+      if (meta != 0xFF) wide_leaf_test(leaf, S.leaf_base + meta, R, best, best_leaf, bt);
     }
-    bool finished = false;
-    if (ANY && best != kMiss) {
-      finished = true;
-    } else {
-      uint32_t rest = inner_hit;  // inner slots still to visit
-      if (bt < bt_before) {
-        // a triangle of this node moved the best distance: drop the inner
-        // children now behind it and pick the nearest again
-        ns = -1;
-#pragma unroll
-        for (int c = 0; c < 8; ++c)
-          if (((rest >> c) & 1u) && ctn[c] > bt) rest &= ~(1u << c);
-#pragma unroll
-        for (int c = 0; c < 8; ++c)
-          if (((rest >> c) & 1u) && (ns < 0 || ctn[c] < nt)) {
-            ns = c;
-            nt = ctn[c];
-          }
-      }
-      if (ns >= 0) {
-        rest &= ~(1u << ns);
-        if (rest) {
-          if (sp < kWideStack) {
-            stack[sp++] = make_uint2(child_base, rest | (imask << 8));
-          } else {
-            atomicCAS(err, 0u, 5u);  // traversal stack overflow
-            finished = true;
-          }
-        }
-        node = child_base + (uint32_t)__popc(imask & ((1u << ns) - 1u));
-      } else if (sp > 0) {
-        uint2 &top = stack[sp - 1];
-        const uint32_t c = __ffs(top.y & 0xFFu) - 1;
-        top.y &= ~(1u << c);
-        node = top.x + (uint32_t)__popc((top.y >> 8) & ((1u << c) - 1u));
-        if ((top.y & 0xFFu) == 0) --sp;
-      } else {
-        finished = true;
-      }
-    }
-    if (finished) {
-      Hit out;
-      out.prim = best;
-      out.t = __int_as_float(0x7f800000);
-      if (best != kMiss) {
-        const float4 a = __ldg(leaf + 3 * (size_t)best_leaf), b = __ldg(leaf + 3 * (size_t)best_leaf + 1),
-                     c = __ldg(leaf + 3 * (size_t)best_leaf + 2);
-        const float v0[3] = {a.x, a.y, a.z}, v1[3] = {b.x, b.y, b.z}, v2[3] = {c.x, c.y, c.z};
-        out.t = refine_t(R, v0, v1, v2);
-      }
-      hits[r] = out;
+    if (best != kMiss || !wide_next(S, stack, sp, node, err)) {
+      hits[r] = wide_result(best, best_leaf);
       active = false;
     }
   }
 }
 
+// Order-preserving unsigned image of a distance with -0 and +0 merged:
+// comparing (t_order(t) << 32 | id) as 64-bit unsigned integers compares
+// (t, id) as the immediate test does (smaller t first, then the lower id).
+__device__ __forceinline__ uint32_t t_order(float t) {
+  const uint32_t u = t == 0.0f ? 0u : __float_as_uint(t);
+  return u ^ ((uint32_t)((int32_t)u >> 31) | 0x80000000u);
+}
+__device__ __forceinline__ float t_from_order(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k ^ 0x80000000u) : ~k);
+}
+
+constexpr int kLeafFlush = 24;  // queued triangle tests that trigger a flush
+constexpr int kLeafQueue = 288;  // per warp: fewer than kLeafFlush + up to 8 per lane from one node step
+
+// Closest hit: one lane per ray, and the triangle tests of the hit leaf
+// children are queued per warp in shared memory as (triangle slot, lane)
+// pairs instead of being run at once.  A node step hits about one leaf
+// triangle per 14 lanes, so running the tests at once kept ~2 of 32 lanes
+// busy for the length of a triangle test in most steps.  When kLeafFlush
+// tests are queued, all 32 lanes run them (the owner's ray comes by
+// shuffles) and fold each hit into the owner's best (t, id) key with one
+// shared-memory atomicMin; the owners then take the key's t as their culling
+// distance.  A lane whose traversal is over while tests of its ray are still
+// queued waits for the flush, which also runs when no lane of the warp
+// traverses any more, or when the waiting lanes and the idle ones add up to a
+// refill.  The closest (t, id) over all tested triangles is the same in any
+// order of tests, so the hits equal the immediate test's; the culling
+// distance only lags.
+template <bool BATCHED>
+__global__ void __launch_bounds__(kWideThreads, 8)
+    k_trace_wide_closest(const WideNode *nodes, const float4 *leaf, const uint32_t *roots, const uint32_t *ray_off,
+                         uint32_t meshes, const float4 *rays, uint64_t nrays, Hit *hits,
+                         unsigned long long *counter, uint32_t *err) {
+  __shared__ uint32_t s_qslot[kWideThreads / 32][kLeafQueue];
+  __shared__ uint8_t s_qlane[kWideThreads / 32][kLeafQueue];
+  __shared__ unsigned long long s_best[kWideThreads / 32][32];
+  __shared__ uint32_t s_bslot[kWideThreads / 32][32];
+  const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+  uint32_t *qslot = s_qslot[wq];
+  uint8_t *qlane = s_qlane[wq];
+  unsigned long long *sbest = s_best[wq];
+  uint32_t *sbslot = s_bslot[wq];
+  bool active = false, drained = false, done = false, pending = false;
+  uint64_t r = 0;
+  Ray R;
+  uint32_t node = 0, best = kMiss, best_leaf = 0;
+  float bt = 0.0f;
+  uint2 stack[kWideStack];
+  uint32_t warp_mesh = 0;
+  int sp = 0, nq = 0;  // nq: queued tests, the same on every lane
+
+  // Runs the queued tests with all lanes (warp-uniform call).
+  auto flush = [&]() {
+    __syncwarp();
+    const int kk = R.kx | (R.ky << 2) | (R.kz << 4);
+    for (int b = 0; b < nq; b += 32) {
+      const int e = b + lane;
+      const uint32_t slot = e < nq ? qslot[e] : kMiss;
+      const int o = e < nq ? qlane[e] : lane;
+      Ray Q;
+      Q.ox = __shfl_sync(FULL_MASK, R.ox, o);
+      Q.oy = __shfl_sync(FULL_MASK, R.oy, o);
+      Q.oz = __shfl_sync(FULL_MASK, R.oz, o);
+      Q.tmin = __shfl_sync(FULL_MASK, R.tmin, o);
+      Q.tmax = __shfl_sync(FULL_MASK, R.tmax, o);
+      Q.Sx = __shfl_sync(FULL_MASK, R.Sx, o);
+      Q.Sy = __shfl_sync(FULL_MASK, R.Sy, o);
+      Q.Sz = __shfl_sync(FULL_MASK, R.Sz, o);
+      const int k = __shfl_sync(FULL_MASK, kk, o);
+      Q.kx = k & 3;
+      Q.ky = (k >> 2) & 3;
+      Q.kz = k >> 4;
+      unsigned long long key = ~0ull;
+      if (slot != kMiss) {
+        const float4 a = __ldg(leaf + 3 * (size_t)slot), bb = __ldg(leaf + 3 * (size_t)slot + 1),
+                     c = __ldg(leaf + 3 * (size_t)slot + 2);
+        const float v0[3] = {a.x, a.y, a.z}, v1[3] = {bb.x, bb.y, bb.z}, v2[3] = {c.x, c.y, c.z};
+        float t;
+        if (isect_tri(Q, v0, v1, v2, t)) {
+          key = ((unsigned long long)t_order(t) << 32) | __float_as_uint(a.w);
+          atomicMin(&sbest[o], key);
+        }
+      }
+      __syncwarp();
+      if (key != ~0ull && sbest[o] == key) sbslot[o] = slot;  // one winner per owner
+      __syncwarp();
+    }
+    if (pending) {
+      const unsigned long long k = sbest[lane];
+      best = (uint32_t)k;
+      bt = t_from_order((uint32_t)(k >> 32));
+      best_leaf = sbslot[lane];
+      pending = false;
+    }
+    nq = 0;
+  };
+
+  while (true) {
+    if (wide_take_ray<BATCHED>(active, drained, warp_mesh, r, R, node, roots, ray_off, meshes, rays, nrays,
+                               counter)) {
+      best = kMiss;
+      best_leaf = 0;
+      bt = R.tmax;
+      sp = 0;
+      done = false;
+      sbest[lane] = ((unsigned long long)t_order(R.tmax) << 32) | kMiss;
+    }
+    if (!__any_sync(FULL_MASK, active)) {
+      if (drained) break;
+      continue;
+    }
+    uint32_t lh = 0, lbase = 0, mlo = 0, mhi = 0;
+    if (active && !done) {
+      const WideStep S = wide_node_step(nodes, node, R, bt);
+      lh = S.hm & ~S.imask;
+      lbase = S.leaf_base;
+      mlo = S.meta_lo;
+      mhi = S.meta_hi;
+      done = !wide_next(S, stack, sp, node, err);
+    }
+    const int cnt = __popc(lh);
+    const int total = (int)__reduce_add_sync(FULL_MASK, (unsigned)cnt);
+    if (total) {
+      if (nq + total > kLeafQueue) flush();
+      int pos;
+      if (!__any_sync(FULL_MASK, cnt > 1)) {
+        pos = nq + __popc(__ballot_sync(FULL_MASK, cnt) & ((1u << lane) - 1u));
+      } else {
+        int inc = cnt;  // inclusive prefix of the counts over the lanes
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const int v = __shfl_up_sync(FULL_MASK, inc, d);
+          if (lane >= d) inc += v;
+        }
+        pos = nq + inc - cnt;
+      }
+      while (lh) {
+        const int c = __ffs(lh) - 1;
+        lh &= lh - 1u;
+        const uint32_t meta = ((c < 4 ? mlo : mhi) >> (8 * (c & 3))) & 0xFF;
+        qslot[pos] = meta == 0xFF ? kMiss : lbase + meta;
+        qlane[pos] = (uint8_t)lane;
+        ++pos;
+      }
+      if (cnt) pending = true;
+      nq += total;
+    }
+    const unsigned waiting = __ballot_sync(FULL_MASK, done && pending);
+    const unsigned running = __ballot_sync(FULL_MASK, active && !done);
+    const unsigned idle = __ballot_sync(FULL_MASK, !active);
+    if (nq >= kLeafFlush || (waiting && (!running || __popc(waiting) + __popc(idle) >= kWideRefill))) flush();
+    if (active && done && !pending) {
+      hits[r] = wide_result(best, best_leaf);
+      active = false;
+    }
+  }
+}
 }  // namespace gprtcu
 
 using namespace gprtcu;
@@ -662,18 +861,23 @@ extern "C" GPRTCU_API gprtcuStatus gprtcuWideTrace(const gprtcuWideBvh *bvh, con
   const int blocks = gprtcu_num_sms() * 8;  // 64 registers: 8 CTAs of 128 threads per SM
   const uint64_t need = (numRays + kWideThreads - 1) / kWideThreads;
   const int grid = (int)(need < (uint64_t)blocks ? need : blocks);
-#define GPRTCU_WTRACE(A, B)                                                                                       \
-  k_trace_wide<A, B><<<grid, kWideThreads, 0, stream>>>((const WideNode *)bvh->nodes, (const float4 *)bvh->leafTris, \
-                                                        bvh->roots, rayOffsets, numMeshes, (const float4 *)rays,   \
-                                                        numRays, (Hit *)hits, counter, &hdr->status)
+#define GPRTCU_WTRACE(K, B)                                                                                 \
+  K<B><<<grid, kWideThreads, 0, stream>>>((const WideNode *)bvh->nodes, (const float4 *)bvh->leafTris, bvh->roots, \
+                                          rayOffsets, numMeshes, (const float4 *)rays, numRays, (Hit *)hits,      \
+                                          counter, &hdr->status)
   if (numMeshes > 1) {
-    if (anyHit) GPRTCU_WTRACE(true, true);
-    else GPRTCU_WTRACE(false, true);
+    if (anyHit) GPRTCU_WTRACE(k_trace_wide_any, true);
+    else GPRTCU_WTRACE(k_trace_wide_closest, true);
   } else {
-    if (anyHit) GPRTCU_WTRACE(true, false);
-    else GPRTCU_WTRACE(false, false);
+    if (anyHit) GPRTCU_WTRACE(k_trace_wide_any, false);
+    else GPRTCU_WTRACE(k_trace_wide_closest, false);
   }
 #undef GPRTCU_WTRACE
+  GPRTCU_TRY(cudaGetLastError());
+  const uint64_t need_r = (numRays + 255) / 256;
+  const int grid_r = (int)(need_r < (uint64_t)gprtcu_num_sms() * 4 ? need_r : gprtcu_num_sms() * 4);
+  k_wide_refine<<<grid_r, 256, 0, stream>>>((const float4 *)bvh->leafTris, (const float4 *)rays, numRays,
+                                            (Hit *)hits);
   GPRTCU_TRY(cudaGetLastError());
   return GPRTCU_OK;
 }
