@@ -293,6 +293,9 @@ constexpr int kWideStack = 64;
 constexpr int kWideRefill = 8;
 
 __device__ __forceinline__ float scale_of(int8_t e) { return __int_as_float(((int)e + 127) << 23); }
+// 2^15 x the node's quantisation step (infinity past the float range: the
+// axis then gives NaN and drops out of the box test, which stays conservative)
+__device__ __forceinline__ float scale15_of(int8_t e) { return __int_as_float(min((int)e + 142, 255) << 23); }
 
 // Packed pairs of fp32 (sm_100 f32x2 arithmetic; each half rounds as the
 // scalar instruction would) and three-input min / max.
@@ -420,7 +423,11 @@ __device__ __forceinline__ bool wide_take_ray(bool &active, bool &drained, uint3
 // eight child boxes are tested two at a time with packed f32x2 arithmetic
 // (byte decode, directed-rounding slab FMAs, the 2^-18 widening) and
 // three-input min/max (68.7 -> 60.7 ms on the 134M-ray workload against the
-// scalar loop).  Absent children are inverted boxes and need no test of their
+// scalar loop).  A plane byte q is decoded by one byte permute into the float
+// v = 1 + q 2^-15; with M = 2^15 x the step in t and the plane offset moved
+// down (near planes) or up (far planes) by M in that direction of rounding,
+// one directed-rounding FMA v M + (offset - M) gives a value never inside
+// q x step + offset, without a separate bias subtraction (47.8 -> 47.2 ms).  Absent children are inverted boxes and need no test of their
 // own.  The nearest hit inner child is found inside the box loop.
 struct WideStep {
   uint32_t hm;  // slots whose box is hit
@@ -433,8 +440,8 @@ __device__ __forceinline__ WideStep wide_node_step(const WideNode *nodes, uint32
   const uint4 *np = reinterpret_cast<const uint4 *>(nodes + node);
   const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
   const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
-  const float sx = scale_of((int8_t)(w0.w & 0xFF)), sy = scale_of((int8_t)((w0.w >> 8) & 0xFF)),
-              sz = scale_of((int8_t)((w0.w >> 16) & 0xFF));
+  const float sx = scale15_of((int8_t)(w0.w & 0xFF)), sy = scale15_of((int8_t)((w0.w >> 8) & 0xFF)),
+              sz = scale15_of((int8_t)((w0.w >> 16) & 0xFF));
   S.imask = w0.w >> 24;
   S.child_base = w1.x;
   S.leaf_base = w1.y;
@@ -453,7 +460,9 @@ __device__ __forceinline__ WideStep wide_node_step(const WideNode *nodes, uint32
       const bool pos = !(ia[a] < 0.0f);
       An[a] = __fmul_rd(pos ? dlo : dhi, ia[a]);
       Af[a] = __fmul_ru(pos ? dhi : dlo, ia[a]);
-      Bq[a] = __fmul_rn(sa[a], ia[a]);
+      Bq[a] = __fmul_rn(sa[a], ia[a]);  // M: 2^15 x the step in t (exactly 2^15 x the rounded step)
+      An[a] = __fsub_rd(An[a], Bq[a]);
+      Af[a] = __fsub_ru(Af[a], Bq[a]);
       qn[a][0] = pos ? ql[a][0] : qh[a][0];
       qn[a][1] = pos ? ql[a][1] : qh[a][1];
       qf[a][0] = pos ? qh[a][0] : ql[a][0];
@@ -464,7 +473,6 @@ __device__ __forceinline__ WideStep wide_node_step(const WideNode *nodes, uint32
   float nt = __int_as_float(0x7f800000);
   int ns = -1;
   {
-    const unsigned long long bias = pk2(-8388608.0f, -8388608.0f);
     const unsigned long long lo2 = pk2(kBoxLo, kBoxLo), hi2 = pk2(kBoxHi, kBoxHi);
     unsigned long long B2[3], N2[3], F2[3];
 #pragma unroll
@@ -476,16 +484,16 @@ __device__ __forceinline__ WideStep wide_node_step(const WideNode *nodes, uint32
 #pragma unroll
     for (int cp = 0; cp < 4; ++cp) {
       const int h = cp >> 1;
-      const uint32_t s0 = 0x7540u | (uint32_t)((2 * cp) & 3), s1 = 0x7540u | (uint32_t)((2 * cp + 1) & 3);
+      const uint32_t s0 = 0x7604u | ((uint32_t)((2 * cp) & 3) << 4), s1 = 0x7604u | ((uint32_t)((2 * cp + 1) & 3) << 4);
       float n[2][3], f[2][3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        const unsigned long long qn2 = pk2(__uint_as_float(__byte_perm(qn[a][h], 0x4B000000u, s0)),
-                                           __uint_as_float(__byte_perm(qn[a][h], 0x4B000000u, s1)));
-        const unsigned long long qf2 = pk2(__uint_as_float(__byte_perm(qf[a][h], 0x4B000000u, s0)),
-                                           __uint_as_float(__byte_perm(qf[a][h], 0x4B000000u, s1)));
-        up2(fma2_rd(add2_rn(qn2, bias), B2[a], N2[a]), n[0][a], n[1][a]);
-        up2(fma2_ru(add2_rn(qf2, bias), B2[a], F2[a]), f[0][a], f[1][a]);
+        const unsigned long long qn2 = pk2(__uint_as_float(__byte_perm(qn[a][h], 0x3F800000u, s0)),
+                                           __uint_as_float(__byte_perm(qn[a][h], 0x3F800000u, s1)));
+        const unsigned long long qf2 = pk2(__uint_as_float(__byte_perm(qf[a][h], 0x3F800000u, s0)),
+                                           __uint_as_float(__byte_perm(qf[a][h], 0x3F800000u, s1)));
+        up2(fma2_rd(qn2, B2[a], N2[a]), n[0][a], n[1][a]);
+        up2(fma2_ru(qf2, B2[a], F2[a]), f[0][a], f[1][a]);
       }
       float tn[2], tf[2];
 #pragma unroll
@@ -637,7 +645,7 @@ __device__ __forceinline__ float t_from_order(uint32_t k) {
 }
 
 constexpr int kLeafFlush = 24;  // queued triangle tests that trigger a flush
-constexpr int kLeafQueue = 288;  // per warp: fewer than kLeafFlush + up to 8 per lane from one node step
+constexpr int kLeafQueue = 256;  // per warp: one node step adds at most 8 per lane; a step that would overflow flushes first
 
 // Closest hit: one lane per ray, and the triangle tests of the hit leaf
 // children are queued per warp in shared memory as (triangle slot, lane)
@@ -645,16 +653,19 @@ constexpr int kLeafQueue = 288;  // per warp: fewer than kLeafFlush + up to 8 pe
 // triangle per 14 lanes, so running the tests at once kept ~2 of 32 lanes
 // busy for the length of a triangle test in most steps.  When kLeafFlush
 // tests are queued, all 32 lanes run them (the owner's ray comes by
-// shuffles) and fold each hit into the owner's best (t, id) key with one
-// shared-memory atomicMin; the owners then take the key's t as their culling
-// distance.  A lane whose traversal is over while tests of its ray are still
+// shuffles and from shared memory) and fold each hit into the owner's best
+// (t, id) key with one shared-memory atomicMin; the owners then take the
+// key's t as their culling distance.  A lane whose traversal is over while tests of its ray are still
 // queued waits for the flush, which also runs when no lane of the warp
 // traverses any more, or when the waiting lanes and the idle ones add up to a
 // refill.  The closest (t, id) over all tested triangles is the same in any
 // order of tests, so the hits equal the immediate test's; the culling
-// distance only lags.
+// distance only lags.  On the 134M-ray workload flush thresholds of 8, 12,
+// 16, 24, 32 and 64 tests measured 56.2 / 55.4 / 55.1 / 54.8 / 55.1 / 55.2
+// ms against 57.6 ms for the immediate tests (t still refined in the
+// traversal then).
 template <bool BATCHED>
-__global__ void __launch_bounds__(kWideThreads, 8)
+__global__ void __launch_bounds__(kWideThreads, 9)
     k_trace_wide_closest(const WideNode *nodes, const float4 *leaf, const uint32_t *roots, const uint32_t *ray_off,
                          uint32_t meshes, const float4 *rays, uint64_t nrays, Hit *hits,
                          unsigned long long *counter, uint32_t *err) {
@@ -662,6 +673,11 @@ __global__ void __launch_bounds__(kWideThreads, 8)
   __shared__ uint8_t s_qlane[kWideThreads / 32][kLeafQueue];
   __shared__ unsigned long long s_best[kWideThreads / 32][32];
   __shared__ uint32_t s_bslot[kWideThreads / 32][32];
+  // what only the flush and the final store read stays in shared memory, not
+  // in registers: 56 registers let 9 CTAs share an SM (47.8 -> 46.6 ms)
+  __shared__ float s_rs[kWideThreads / 32][4][32];  // Sx, Sy, Sz, tmax of each lane's ray
+  __shared__ int s_rk[kWideThreads / 32][32];        // kx | ky << 2 | kz << 4
+  __shared__ unsigned long long s_rid[kWideThreads / 32][32];  // ray index
   const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
   uint32_t *qslot = s_qslot[wq];
   uint8_t *qlane = s_qlane[wq];
@@ -670,7 +686,7 @@ __global__ void __launch_bounds__(kWideThreads, 8)
   bool active = false, drained = false, done = false, pending = false;
   uint64_t r = 0;
   Ray R;
-  uint32_t node = 0, best = kMiss, best_leaf = 0;
+  uint32_t node = 0;
   float bt = 0.0f;
   uint2 stack[kWideStack];
   uint32_t warp_mesh = 0;
@@ -679,7 +695,6 @@ __global__ void __launch_bounds__(kWideThreads, 8)
   // Runs the queued tests with all lanes (warp-uniform call).
   auto flush = [&]() {
     __syncwarp();
-    const int kk = R.kx | (R.ky << 2) | (R.kz << 4);
     for (int b = 0; b < nq; b += 32) {
       const int e = b + lane;
       const uint32_t slot = e < nq ? qslot[e] : kMiss;
@@ -689,11 +704,11 @@ __global__ void __launch_bounds__(kWideThreads, 8)
       Q.oy = __shfl_sync(FULL_MASK, R.oy, o);
       Q.oz = __shfl_sync(FULL_MASK, R.oz, o);
       Q.tmin = __shfl_sync(FULL_MASK, R.tmin, o);
-      Q.tmax = __shfl_sync(FULL_MASK, R.tmax, o);
-      Q.Sx = __shfl_sync(FULL_MASK, R.Sx, o);
-      Q.Sy = __shfl_sync(FULL_MASK, R.Sy, o);
-      Q.Sz = __shfl_sync(FULL_MASK, R.Sz, o);
-      const int k = __shfl_sync(FULL_MASK, kk, o);
+      Q.Sx = s_rs[wq][0][o];
+      Q.Sy = s_rs[wq][1][o];
+      Q.Sz = s_rs[wq][2][o];
+      Q.tmax = s_rs[wq][3][o];
+      const int k = s_rk[wq][o];
       Q.kx = k & 3;
       Q.ky = (k >> 2) & 3;
       Q.kz = k >> 4;
@@ -713,10 +728,7 @@ __global__ void __launch_bounds__(kWideThreads, 8)
       __syncwarp();
     }
     if (pending) {
-      const unsigned long long k = sbest[lane];
-      best = (uint32_t)k;
-      bt = t_from_order((uint32_t)(k >> 32));
-      best_leaf = sbslot[lane];
+      bt = t_from_order((uint32_t)(sbest[lane] >> 32));
       pending = false;
     }
     nq = 0;
@@ -725,12 +737,16 @@ __global__ void __launch_bounds__(kWideThreads, 8)
   while (true) {
     if (wide_take_ray<BATCHED>(active, drained, warp_mesh, r, R, node, roots, ray_off, meshes, rays, nrays,
                                counter)) {
-      best = kMiss;
-      best_leaf = 0;
       bt = R.tmax;
       sp = 0;
       done = false;
       sbest[lane] = ((unsigned long long)t_order(R.tmax) << 32) | kMiss;
+      s_rs[wq][0][lane] = R.Sx;
+      s_rs[wq][1][lane] = R.Sy;
+      s_rs[wq][2][lane] = R.Sz;
+      s_rs[wq][3][lane] = R.tmax;
+      s_rk[wq][lane] = R.kx | (R.ky << 2) | (R.kz << 4);
+      s_rid[wq][lane] = r;
     }
     if (!__any_sync(FULL_MASK, active)) {
       if (drained) break;
@@ -777,7 +793,7 @@ __global__ void __launch_bounds__(kWideThreads, 8)
     const unsigned idle = __ballot_sync(FULL_MASK, !active);
     if (nq >= kLeafFlush || (waiting && (!running || __popc(waiting) + __popc(idle) >= kWideRefill))) flush();
     if (active && done && !pending) {
-      hits[r] = wide_result(best, best_leaf);
+      hits[s_rid[wq][lane]] = wide_result((uint32_t)sbest[lane], sbslot[lane]);
       active = false;
     }
   }
@@ -858,7 +874,8 @@ extern "C" GPRTCU_API gprtcuStatus gprtcuWideTrace(const gprtcuWideBvh *bvh, con
   ScratchHeader *hdr = (ScratchHeader *)scratch;
   unsigned long long *counter = reinterpret_cast<unsigned long long *>(&hdr->ticket[0]);
   GPRTCU_TRY(cudaMemsetAsync(scratch, 0, sizeof(ScratchHeader), stream));
-  const int blocks = gprtcu_num_sms() * 8;  // 64 registers: 8 CTAs of 128 threads per SM
+  // any hit: 64 registers, 8 CTAs of 128 threads per SM; closest hit: 56, 9
+  const int blocks = gprtcu_num_sms() * (anyHit ? 8 : 9);
   const uint64_t need = (numRays + kWideThreads - 1) / kWideThreads;
   const int grid = (int)(need < (uint64_t)blocks ? need : blocks);
 #define GPRTCU_WTRACE(K, B)                                                                                 \
