@@ -499,14 +499,18 @@ __device__ __forceinline__ WideStep wide_node_step(const WideNode *nodes, uint32
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
         tn[k] = fmaxf(max3f(n[k][0], n[k][1], n[k][2]), R.tmin);
-        tf[k] = fminf(min3f(f[k][0], f[k][1], f[k][2]), bt);
+        tf[k] = min3f(f[k][0], f[k][1], f[k][2]);
       }
       up2(mul2_rn(pk2(tn[0], tn[1]), lo2), tn[0], tn[1]);
       up2(mul2_rn(pk2(tf[0], tf[1]), hi2), tf[0], tf[1]);
+      // the widened exit clamped by the best distance: one compare per child
+      // tests both (45.4 against 46.6 ms for two compares, exit clamped first)
+      tf[0] = fminf(tf[0], bt);
+      tf[1] = fminf(tf[1], bt);
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
         const int c = 2 * cp + k;
-        const bool hit = tn[k] <= tf[k] && tn[k] <= bt;
+        const bool hit = tn[k] <= tf[k];
         hm |= (uint32_t)hit << c;
         if (hit && ((S.imask >> c) & 1u) && tn[k] < nt) {
           nt = tn[k];
