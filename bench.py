@@ -677,7 +677,8 @@ def run_b200(args, world, rank, local):
                        "triangles_per_gpu": ntri, "meshes_per_gpu": meshes,
                        "rays_per_gpu": nrays, "l2": "flushed (256 MB write) between timed steps",
                        "parallelism": "independent scene per GPU" if world > 1 else "single GPU"},
-            "roofline": {"kernel": "k_trace_wide (closest hit, batched)", "bound": "hbm",
+            "roofline": {"kernel": "k_trace_wide_closest + k_wide_refine (closest hit, batched: the two kernels "
+                                   "of one gprtcuWideTrace call, timed together)", "bound": "hbm",
                          "limiter": "instruction issue (divergent per-ray traversal), not DRAM bandwidth: the HBM "
                                     "roofline is the denominator of frac, not what limits the kernel",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind + " hbm_gbs (copy)",

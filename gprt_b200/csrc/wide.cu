@@ -573,28 +573,56 @@ __device__ __forceinline__ Hit wide_result(uint32_t best, uint32_t best_leaf) {
 
 // t of every hit: the plane-equation distance of the hit triangle in
 // double-float, rounded once.  Run after the traversal over all rays at once
-// (coalesced, every lane busy) instead of by each lane as its ray finished,
-// when few lanes of the warp ran it and the rest waited.
-__global__ void __launch_bounds__(256) k_wide_refine(const float4 *leaf, const float4 *rays, uint64_t nrays,
-                                                     Hit *hits) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nrays;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    const Hit h = hits[i];
-    if (h.prim == kMiss) continue;
-    const uint32_t slot = __float_as_uint(h.t);
-    const float4 o = __ldg(rays + 2 * i), d = __ldg(rays + 2 * i + 1);
-    Ray R;
-    R.ox = o.x;
-    R.oy = o.y;
-    R.oz = o.z;
-    R.dx = d.x;
-    R.dy = d.y;
-    R.dz = d.z;
-    const float4 a = __ldg(leaf + 3 * (size_t)slot), b = __ldg(leaf + 3 * (size_t)slot + 1),
-                 c = __ldg(leaf + 3 * (size_t)slot + 2);
-    const float v0[3] = {a.x, a.y, a.z}, v1[3] = {b.x, b.y, b.z}, v2[3] = {c.x, c.y, c.z};
-    hits[i].t = refine_t(R, v0, v1, v2);
+// instead of by each lane as its ray finished (when few lanes of the warp ran
+// it and the rest waited).  A warp reads 32 records at a time (coalesced)
+// and queues the indices of the hits in shared memory; every 32 queued hits
+// are refined with all lanes busy (a lane per record left ~1 in 5 busy: 2.0
+// ms cold for 134M rays, 18 % of them hits).
+constexpr int kRefineThreads = 256;
+
+__global__ void __launch_bounds__(kRefineThreads) k_wide_refine(const float4 *leaf, const float4 *rays,
+                                                                uint64_t nrays, Hit *hits) {
+  __shared__ uint64_t s_q[kRefineThreads / 32][64];
+  const int lane = threadIdx.x & 31;
+  uint64_t *q = s_q[threadIdx.x >> 5];
+  auto refine = [&](int count) {
+    __syncwarp();
+    if (lane < count) {
+      const uint64_t i = q[lane];
+      const uint32_t slot = __float_as_uint(hits[i].t);
+      const float4 o = __ldg(rays + 2 * i), d = __ldg(rays + 2 * i + 1);
+      Ray R;
+      R.ox = o.x;
+      R.oy = o.y;
+      R.oz = o.z;
+      R.dx = d.x;
+      R.dy = d.y;
+      R.dz = d.z;
+      const float4 a = __ldg(leaf + 3 * (size_t)slot), b = __ldg(leaf + 3 * (size_t)slot + 1),
+                   c = __ldg(leaf + 3 * (size_t)slot + 2);
+      const float v0[3] = {a.x, a.y, a.z}, v1[3] = {b.x, b.y, b.z}, v2[3] = {c.x, c.y, c.z};
+      hits[i].t = refine_t(R, v0, v1, v2);
+    }
+    __syncwarp();
+  };
+  int nq = 0;  // queued hits, the same on every lane
+  const uint64_t warps = (uint64_t)gridDim.x * (kRefineThreads / 32);
+  for (uint64_t base = (blockIdx.x * (uint64_t)(kRefineThreads / 32) + (threadIdx.x >> 5)) * 32; base < nrays;
+       base += warps * 32) {
+    const uint64_t i = base + lane;
+    const bool hit = i < nrays && hits[i].prim != kMiss;
+    const unsigned m = __ballot_sync(FULL_MASK, hit);
+    if (hit) q[nq + __popc(m & ((1u << lane) - 1u))] = i;
+    nq += __popc(m);
+    if (nq >= 32) {
+      refine(32);
+      const uint64_t v = lane < nq - 32 ? q[32 + lane] : 0;
+      __syncwarp();
+      if (lane < nq - 32) q[lane] = v;
+      nq -= 32;
+    }
   }
+  refine(nq);
 }
 
 // Any hit: one lane per ray; after a node's box loop the lanes with hit leaf
@@ -900,10 +928,10 @@ extern "C" GPRTCU_API gprtcuStatus gprtcuWideTrace(const gprtcuWideBvh *bvh, con
   }
 #undef GPRTCU_WTRACE
   GPRTCU_TRY(cudaGetLastError());
-  const uint64_t need_r = (numRays + 255) / 256;
+  const uint64_t need_r = (numRays + kRefineThreads - 1) / kRefineThreads;
   const int grid_r = (int)(need_r < (uint64_t)gprtcu_num_sms() * 4 ? need_r : gprtcu_num_sms() * 4);
-  k_wide_refine<<<grid_r, 256, 0, stream>>>((const float4 *)bvh->leafTris, (const float4 *)rays, numRays,
-                                            (Hit *)hits);
+  k_wide_refine<<<grid_r, kRefineThreads, 0, stream>>>((const float4 *)bvh->leafTris, (const float4 *)rays,
+                                                       numRays, (Hit *)hits);
   GPRTCU_TRY(cudaGetLastError());
   return GPRTCU_OK;
 }
