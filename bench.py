@@ -618,6 +618,18 @@ def run_b200(args, world, rank, local):
             "triangles": ps.n, "rays": ps.nrays, "build_ms": float(np.mean(pb)), "trace_ms": float(np.mean(pt)),
             "build_mprims_s": ps.n / np.mean(pb) / 1e3, "trace_mrays_s": ps.nrays / np.mean(pt) / 1e3,
             "step_mrays_s": ps.nrays / (np.mean(pb) + np.mean(pt)) / 1e3}
+        # the same scene through the quantised wide BVH, beside the plain path
+        ps.wide_setup()
+        ps.build()
+        wc = workloads.time_steps(ps.collapse, args.steps, args.warmup, flush)
+        wt = workloads.time_steps(ps.wide_trace, args.steps, args.warmup, flush)
+        ps.trace()
+        torch.cuda.synchronize()
+        extra["small_lbvh"]["quantised"] = {
+            "collapse_ms": float(np.mean(wc)), "trace_ms": float(np.mean(wt)),
+            "trace_mrays_s": ps.nrays / np.mean(wt) / 1e3,
+            "step_mrays_s": ps.nrays / (np.mean(pb) + np.mean(wc) + np.mean(wt)) / 1e3,
+            "hits_identical": bool(torch.equal(ps.hits, ps.hw))}
         del ps
         ws = workloads.WideScene(device=dev)
         extra["wide_bvh"] = ws.run(steps=2, warmup=1, flush=flush)

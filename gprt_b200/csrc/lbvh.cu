@@ -443,7 +443,8 @@ __global__ void __launch_bounds__(256, 8) k_refit(const float *pos, const uint32
                                                const uint64_t *keys, MeshMap mm, int4 *nodes, float *aabbs,
                                                Bvh2Node *bvh, float4 *leaf_tris, uint32_t *codes_out,
                                                uint32_t *arrivals, float *root_box, const uint32_t *sort_status) {
-  const uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  // 32-bit indices throughout: n < 2^30, so node indices stay below 2^31
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= mm.n) return;
   // The scratch header sits a fixed distance before the arrival counters.
   auto lbvh_header = [&]() {
@@ -465,36 +466,37 @@ __global__ void __launch_bounds__(256, 8) k_refit(const float *pos, const uint32
       m = mm.mesh_of_prim(s);  // refit of an existing batch: no keys
     }
   }
-  const uint64_t b = BATCHED ? mm.begin(m) : 0;
-  const int64_t N = BATCHED ? mm.count(m) : mm.n;
-  const uint64_t inner_base = b - m, node_base = 2 * b - m;
-  const int64_t i = (int64_t)(s - b);
+  const uint32_t b = BATCHED ? mm.begin(m) : 0u;
+  const int N = BATCHED ? (int)mm.count(m) : (int)mm.n;
+  const uint32_t inner_base = b - m, node_base = 2 * b - m;
+  const int i = (int)(s - b);
   const uint32_t id = sort_err ? (uint32_t)i : ids[s];
   const bool hooked = (int64_t)s == c_refit_skip;
   // The parent (written by the topology kernel) and its node are loaded
   // before the primitive's gather, so the two chains of dependent loads
   // overlap instead of following each other (67M triangles in 16,384 meshes:
   // batched build 16.2 -> 15.9 ms; capped at 32 registers for full occupancy,
-  // 14.9 ms, and the topology kernel likewise, 14.5 ms).  Counting the
-  // arrival before the gather as well measured no faster (14.6 ms).
-  const int64_t leaf = (N - 1) + i;
+  // 14.9 ms, and the topology kernel likewise, 14.5 ms; 32-bit indices, no
+  // spills at 32 registers, 14.0 ms).  Counting the arrival before the gather
+  // as well measured no faster (14.6 ms).
+  const int leaf = (N - 1) + i;
   int4 *nl = &nodes[node_base + leaf];
-  int64_t p = N == 1 ? -1 : (int64_t)reinterpret_cast<const int *>(nl)[2];
+  int p = N == 1 ? -1 : reinterpret_cast<const int *>(nl)[2];
   int4 pn = make_int4(0, 0, -1, -1);
   if (p >= 0) pn = nodes[node_base + p];
   float v[9], bx[6];
-  prim_box<KIND>(pos, tri, b + id, v, bx);
+  prim_box<KIND>(pos, tri, (uint64_t)b + id, v, bx);
   if (leaf_tris) {
-    leaf_tris[3 * s + 0] = make_float4(v[0], v[1], v[2], __uint_as_float(id));
-    leaf_tris[3 * s + 1] = make_float4(v[3], v[4], v[5], 0.0f);
-    leaf_tris[3 * s + 2] = make_float4(v[6], v[7], v[8], 0.0f);
+    leaf_tris[3 * (size_t)s + 0] = make_float4(v[0], v[1], v[2], __uint_as_float(id));
+    leaf_tris[3 * (size_t)s + 1] = make_float4(v[3], v[4], v[5], 0.0f);
+    leaf_tris[3 * (size_t)s + 2] = make_float4(v[6], v[7], v[8], 0.0f);
   }
-  *nl = make_int4(-1, -1, (int)p, (int)id);
+  *nl = make_int4(-1, -1, p, (int)id);
   if (aabbs)
-    for (int k = 0; k < 6; ++k) aabbs[6 * (node_base + leaf) + k] = bx[k];
-  int64_t child = leaf;
+    for (int k = 0; k < 6; ++k) aabbs[6 * (size_t)(node_base + leaf) + k] = bx[k];
+  int child = leaf;
   while (p >= 0) {
-    const int side = pn.x == (int)child ? 0 : 1;
+    const int side = pn.x == child ? 0 : 1;
     // This child's box goes into its slot of the parent's traversal node (or
     // is already in the reference-layout array); the release half of the
     // arrival count publishes it.
@@ -516,12 +518,12 @@ __global__ void __launch_bounds__(256, 8) k_refit(const float *pos, const uint32
     // starting from +-1e38 exactly as MakeNodes initialises inner boxes.
     // (A hooked leaf arriving second waits on its own unwritten slot, so the
     // wait below runs out whichever child arrives first.)
-    const int64_t sib = side == 0 ? pn.y : pn.x;
+    const int sib = side == 0 ? pn.y : pn.x;
     const int rd = skip_store ? side : 1 - side;
     // the next parent's node, loaded while the sibling's box is read
     int4 gpn = make_int4(0, 0, -1, -1);
     if (pn.z >= 0) gpn = nodes[node_base + pn.z];
-    const float *ob = bvh ? bvh[inner_base + p].box + 6 * rd : aabbs + 6 * (node_base + sib);
+    const float *ob = bvh ? bvh[inner_base + p].box + 6 * rd : aabbs + 6 * (size_t)(node_base + sib);
     float sb[6];
     if (bvh) {
       // bounded wait for the sibling's stores; a wait that runs out records
@@ -541,7 +543,7 @@ __global__ void __launch_bounds__(256, 8) k_refit(const float *pos, const uint32
       bx[3 + k] = fmaxf(-1e38f, fmaxf(bx[3 + k], sb[3 + k]));
     }
     if (aabbs)
-      for (int k = 0; k < 6; ++k) aabbs[6 * (node_base + p) + k] = bx[k];
+      for (int k = 0; k < 6; ++k) aabbs[6 * (size_t)(node_base + p) + k] = bx[k];
     child = p;
     p = pn.z;
     pn = gpn;

@@ -73,6 +73,18 @@ class PlainScene:
         self.build()
         self.trace()
 
+    # the same scene through the 8-wide quantised BVH (collapse of the binary
+    # LBVH just built, then the wide traversal)
+    def wide_setup(self):
+        self.wide = api.WideBvh(self.n, 1, self.rays.device)
+        self.hw = torch.empty_like(self.hits)
+
+    def collapse(self):
+        api.wide_build(self.bvh, wide=self.wide)
+
+    def wide_trace(self):
+        api.wide_trace(self.wide, self.rays, hits=self.hw, scr=self.tscr)
+
 
 class WideScene:
     def __init__(self, n=16_777_216, nrays=16_777_216, clusters=64, device="cuda"):
