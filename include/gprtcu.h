@@ -230,7 +230,10 @@ GPRTCU_API gprtcuStatus gprtcuLbvhRefitTriangles(const float *positions, const u
  * TraceRay (gprt/gprt_builtins.slang:105-124; RayDesc use
  * samples/s2-hitPrograms/s2-0-triangles/deviceCode.slang:52-57), whose
  * reference path is Vulkan hardware ray tracing (gprt/gprt.cpp:9404).
- * rays: float[8] per ray {org.xyz, tmin, dir.xyz, tmax} (32 B, 16-B aligned).
+ * rays: float[8] per ray {org.xyz, tmin, dir.xyz, tmax} (32 B, 16-B aligned),
+ * 0 <= tmin <= tmax as a Vulkan RayDesc requires (the box tests widen their
+ * entry / exit distances for non-negative values; a negative tmin is not
+ * supported).
  * hits: {uint32 prim (0xFFFFFFFF = miss), float t} per ray.
  * Closest hit: smallest fp32 watertight distance in [tmin, tmax], ties to the
  * lowest primitive id; the reported t is the plane-equation distance of that

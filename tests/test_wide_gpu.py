@@ -169,3 +169,59 @@ def test_wide_trace_axis_parallel_rays(cuda, anyhit):
         hit = gw["prim"] != 0xFFFFFFFF
         assert hit.sum() > 500
         assert np.array_equal(_bits(gw["t"][hit]), _bits(gb["t"][hit]))
+
+
+def _layer_scene(k=16, zs=(0.25, 0.5, 0.75), dup_every=7):
+    """Stacked grids of quads split into triangles sharing edges and
+    vertices, with every dup_every-th triangle duplicated (coplanar copies:
+    the lower id must win a tie)."""
+    xs = np.linspace(0, 1, k + 1, dtype=np.float32)
+    X, Y = np.meshgrid(xs, xs, indexing="ij")
+    verts, tris = [], []
+    for li, z in enumerate(zs):
+        base = li * X.size
+        verts.append(np.stack([X.ravel(), Y.ravel(), np.full(X.size, z, np.float32)], 1))
+        for i in range(k):
+            for j in range(k):
+                a, b = i * (k + 1) + j, (i + 1) * (k + 1) + j
+                c, d = (i + 1) * (k + 1) + j + 1, i * (k + 1) + j + 1
+                tris += [[base + a, base + b, base + c], [base + a, base + c, base + d]]
+    tris = np.array(tris, np.uint32)
+    return np.concatenate(verts).astype(np.float32), np.concatenate([tris, tris[::dup_every]]), xs
+
+
+def test_wide_closest_ties_and_zero_t(cuda):
+    # The closest-hit kernel folds queued triangle tests into a (t, id) key:
+    # ties (coplanar copies, shared vertices and edges) must still go to the
+    # lowest id, and t = 0 (origin on a triangle) must count, whether the
+    # triangle test returns +0 or -0.
+    import torch
+    from gprt_b200 import api
+    verts, tris, xs = _layer_scene()
+    rng = np.random.default_rng(5)
+    m = 6000
+    rays = np.zeros((m, 8), np.float32)
+    rays[:, :3] = rng.random((m, 3))
+    rays[:, 4:7] = rng.normal(size=(m, 3))
+    rays[:, 7] = np.inf
+    extra = []
+    for x in xs[1:-1:3]:
+        for y in xs[1:-1:3]:
+            extra.append([x, y, 0.5, 0.0, 0.0, 0.0, -1.0, np.inf])  # starts on a layer, through a vertex: t = 0
+            extra.append([x, y, 0.5, 0.0, 0.0, 0.0, 1.0, np.inf])  # the other way: t = 0 as well
+            extra.append([x, y, 0.9, 0.0, 0.0, 0.0, -1.0, np.inf])  # through three layers' vertices
+    rays = np.concatenate([rays, np.array(extra, np.float32)])
+    rt = torch.from_numpy(rays).cuda()
+    b = api.lbvh_build_triangles(torch.from_numpy(verts).cuda(), torch.from_numpy(tris.view(np.int32)).cuda())
+    w = api.wide_build(b)
+    gw = api.hits_numpy(api.wide_trace(w, rt))
+    gb = api.hits_numpy(api.trace(b, rt))
+    exp = oracle.trace_brute(verts, tris, rays)
+    assert np.array_equal(gw["prim"], exp["prim"])
+    assert np.array_equal(gw["prim"], gb["prim"])
+    hit = gw["prim"] != 0xFFFFFFFF
+    assert np.array_equal(_bits(gw["t"][hit]), _bits(gb["t"][hit]))
+    assert hit.mean() > 0.4
+    n_extra = len(extra)
+    assert (gw["prim"][-n_extra:] != 0xFFFFFFFF).all()
+    assert (gw["t"][-n_extra::3] == 0.0).all() and (gw["t"][-n_extra + 1::3] == 0.0).all()
