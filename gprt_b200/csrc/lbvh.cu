@@ -120,13 +120,14 @@ struct MeshMap {
     }
     return lo;
   }
-  // Warp-cooperative form of the two lookups above, for the 32 consecutive
-  // elements e0 + lane (e0 the same on every lane; all 32 lanes call): the
-  // largest m with off(m) <= e0 + lane, off(m) non-decreasing.  The warp
-  // brackets the mesh of e0 with 32 probes a round (three rounds for 16,384
-  // meshes, against a 14-load bisection per element), then every lane counts
-  // the meshes that start within its reach by bisecting the next 32 offsets
-  // with shuffles (one load per lane).
+  // Warp-cooperative form of that lookup, for primitives or inner nodes
+  // (inner node g of mesh m: (b_m - m) <= g < (b_{m+1} - m - 1)), for the 32
+  // consecutive elements e0 + lane (e0 the same on every lane; all 32 lanes
+  // call): the largest m with off(m) <= e0 + lane, off(m) non-decreasing.
+  // The warp brackets the mesh of e0 with 32 probes a round (three rounds
+  // for 16,384 meshes, against a 14-load bisection per element), then every
+  // lane counts the meshes that start within its reach by bisecting the next
+  // 32 offsets with shuffles (one load per lane).
   template <class Off>
   __device__ __forceinline__ uint32_t warp_mesh_of(uint64_t e0, Off off) const {
     if (!prim_off) return 0;
@@ -158,17 +159,6 @@ struct MeshMap {
   }
   __device__ __forceinline__ uint32_t warp_mesh_of_inner(uint64_t g0) const {
     return warp_mesh_of(g0, [&](uint32_t m) -> uint64_t { return (uint64_t)__ldg(prim_off + m) - m; });
-  }
-  // Mesh holding global inner node g: (b_m - m) <= g < (b_{m+1} - m - 1).
-  __device__ __forceinline__ uint32_t mesh_of_inner(uint64_t g) const {
-    if (!prim_off) return 0;
-    uint32_t lo = 0, hi = meshes;
-    while (hi - lo > 1) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (__ldg(prim_off + mid) - mid <= g) lo = mid;
-      else hi = mid;
-    }
-    return lo;
   }
 };
 
