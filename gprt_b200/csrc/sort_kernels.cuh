@@ -24,6 +24,7 @@
 // Traffic per pass: read + write of keys and payloads; plus one read of the
 // keys for the histograms.
 #pragma once
+#include <algorithm>
 #include <array>
 #include <type_traits>
 #include <utility>
@@ -490,17 +491,29 @@ __global__ void __launch_bounds__(WARPS * 32, (PassCfg<K, V, RB, WARPS, ITEMS>::
 // ---------------------------------------------------------------------------
 // The pass above executes ~130 warp instructions per 32 keys on B200 (2^26
 // pairs; ALU pipe 59 %, issue 59 %), about 40 of them in the eight votes of
-// its ranking.  This one ranks the same way but trims the rest: digits are
-// one byte-permute when they are whole bytes (instead of a shift and a mask,
-// four times per key), every lane of a digit's peers writes the warp's count
-// (no leader election), no key is held in registers (the tile-sorted order
-// is a 16-bit index per slot, and the scatter gathers keys and payloads from
-// their untouched tiles, so payloads need no reorder round), full tiles
-// skip bounds tests, and keys and payloads leave the tile in one loop.
-// RANK 1 finds a key's peers with a 32-bit shared-memory OR of its lane bit
-// into the digit's word instead of votes (measured against the votes; a
-// 64-bit OR word carrying the count as well was 2.5x slower on Zipf keys:
-// same-word atomics serialise).
+// its ranking.  This one trims the rest: digits are one byte-permute when
+// they are whole bytes (instead of a shift and a mask, four times per key),
+// every lane of a digit's peers writes the warp's count (no leader
+// election), no key is held in registers (the tile-sorted order is a 16-bit
+// index per slot, and the scatter gathers keys and payloads from their
+// untouched tiles, so payloads need no reorder round), full tiles skip bounds
+// tests, and keys and payloads leave the tile in one loop.  The look-back's
+// first window of loads is issued before the tile-local order is written and
+// resolved after it, so its L2 round trip overlaps that work (2^28 Zipf
+// pairs: 6.14 -> 5.95 ms).
+//
+// RANK picks how a lane finds the lanes of its row with the same digit:
+//   0  leader tables (the default): every lane stores its lane number into
+//      its digit's byte of a per-warp table; after the warp barrier all
+//      lanes of a digit read back the same number (one of theirs), and
+//      different digits read different numbers, so five votes on that
+//      number replace eight on the digit (6.29 -> 6.14 ms, 2^28 Zipf pairs;
+//      the same on uniform keys);
+//   2  a 32-bit shared-memory OR of the lane bit into the digit's word (a
+//      64-bit word carrying the count as well was 2.5x slower on Zipf keys:
+//      same-word atomics serialise);
+//   3  match.any;  4  eight plain votes;  5  eight predicated votes.
+// All give the same bits; 2-5 stay for measurement.
 template <typename K, typename V, int WARPS, int ITEMS, int RANK> struct Pass8Cfg {
   static constexpr int RADIX = 256;
   static constexpr int THREADS = WARPS * 32;
@@ -510,10 +523,11 @@ template <typename K, typename V, int WARPS, int ITEMS, int RANK> struct Pass8Cf
   static constexpr size_t KEY_BYTES = (size_t)TILE * sizeof(K);
   static constexpr size_t VAL_BYTES = HAS_V ? (size_t)TILE * sizeof(V) : 0;
   static constexpr size_t TBL_BYTES = (size_t)WARPS * RADIX * 4;  // per-warp counts, then first slots
-  static constexpr size_t MSK_BYTES = RANK == 1 ? (size_t)WARPS * RADIX * 4 : 0;  // per-warp lane masks
+  static constexpr size_t MSK_BYTES = RANK == 2 ? (size_t)WARPS * RADIX * 4 : 0;  // per-warp lane masks
   static constexpr size_t PERM_BYTES = (size_t)TILE * 2;
-  static constexpr size_t SMEM =
-      KEY_BYTES + VAL_BYTES + TBL_BYTES + MSK_BYTES + PERM_BYTES + RADIX * 4 /*goff*/ + 16 /*barriers*/;
+  static constexpr size_t LEAD_BYTES = RANK == 0 ? (size_t)WARPS * 2 * RADIX : 0;  // two leader tables per warp
+  static constexpr size_t SMEM = KEY_BYTES + VAL_BYTES + TBL_BYTES + MSK_BYTES + PERM_BYTES + LEAD_BYTES +
+                                 RADIX * 4 /*goff*/ + 16 /*barriers*/;
   static_assert(TILE <= 65536, "16-bit slot indices");
   static constexpr int SMEM_CTAS = (int)((228 * 1024) / (SMEM + 1024));
   static constexpr int THREAD_CTAS = 2048 / THREADS;
@@ -573,8 +587,9 @@ __global__ void __launch_bounds__(WARPS * 32, (Pass8Cfg<K, V, WARPS, ITEMS, RANK
   uint32_t *s_cnt = reinterpret_cast<uint32_t *>(smem + C::KEY_BYTES + C::VAL_BYTES);  // [WARPS][RADIX]
   uint32_t *s_msk = reinterpret_cast<uint32_t *>(smem + C::KEY_BYTES + C::VAL_BYTES + C::TBL_BYTES);
   uint16_t *s_perm = reinterpret_cast<uint16_t *>(smem + C::KEY_BYTES + C::VAL_BYTES + C::TBL_BYTES + C::MSK_BYTES);
+  uint8_t *s_lead = smem + C::KEY_BYTES + C::VAL_BYTES + C::TBL_BYTES + C::MSK_BYTES + C::PERM_BYTES;
   uint32_t *s_goff = reinterpret_cast<uint32_t *>(smem + C::KEY_BYTES + C::VAL_BYTES + C::TBL_BYTES + C::MSK_BYTES +
-                                                  C::PERM_BYTES);
+                                                  C::PERM_BYTES + C::LEAD_BYTES);
   uint64_t *bars = reinterpret_cast<uint64_t *>(s_goff + RADIX);
   __shared__ uint32_t s_tile, s_abort;
   __shared__ uint32_t s_tmp[32];
@@ -648,30 +663,55 @@ __global__ void __launch_bounds__(WARPS * 32, (Pass8Cfg<K, V, WARPS, ITEMS, RANK
   uint32_t *wc = s_cnt + warp * RADIX;
   uint32_t *wm = s_msk + warp * RADIX;
   const uint32_t lanebit = 1u << lane, lt = lanebit - 1u;
-#pragma unroll
-  for (int i = 0; i < ITEMS; ++i) {
-    const uint32_t d = digit8<BYTE>(s_keys[warp * WK + i * 32 + lane], shift, mask, bsel);
-    uint32_t peers;
-    const uint32_t base = wc[d];
-    if constexpr (RANK == 1) {
-      atomicOr(wm + d, lanebit);
-      __syncwarp();
-      peers = *reinterpret_cast<volatile uint32_t *>(wm + d);
-      __syncwarp();
-      wm[d] = 0u;
-    } else if constexpr (RANK == 2) {
-      peers = __match_any_sync(FULL_MASK, d);
-      __syncwarp();
-    } else if constexpr (RANK == 3) {
-      peers = warp_peers<8>(d);  // the plain form of the votes, for comparison
-      __syncwarp();
-    } else {
-      peers = warp_peers_p<8>(d);
-      __syncwarp();
-    }
-    wc[d] = base + __popc(peers);  // every peer stores the same count
+  if constexpr (RANK == 0) {
+    // Two leader tables alternate by row, so the next row's stores are
+    // issued before this row's votes (the table they overwrite was read a
+    // row earlier, before the barriers that end that row).
+    uint8_t *wl = s_lead + warp * 2 * RADIX;
+    uint32_t dn = digit8<BYTE>(s_keys[warp * WK + lane], shift, mask, bsel);
+    wl[dn] = (uint8_t)lane;
     __syncwarp();
-    rank[i] = base + __popc(peers & lt);
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      const uint32_t d = dn;
+      const uint32_t ld = wl[(i & 1) * RADIX + d];
+      const uint32_t base = wc[d];
+      if (i + 1 < ITEMS) {
+        dn = digit8<BYTE>(s_keys[warp * WK + (i + 1) * 32 + lane], shift, mask, bsel);
+        wl[((i + 1) & 1) * RADIX + dn] = (uint8_t)lane;
+      }
+      const uint32_t peers = warp_peers_p<5>(ld);
+      __syncwarp();
+      wc[d] = base + __popc(peers);  // every peer stores the same count
+      __syncwarp();
+      rank[i] = base + __popc(peers & lt);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      const uint32_t d = digit8<BYTE>(s_keys[warp * WK + i * 32 + lane], shift, mask, bsel);
+      uint32_t peers;
+      const uint32_t base = wc[d];
+      if constexpr (RANK == 2) {
+        atomicOr(wm + d, lanebit);
+        __syncwarp();
+        peers = *reinterpret_cast<volatile uint32_t *>(wm + d);
+        __syncwarp();
+        wm[d] = 0u;
+      } else if constexpr (RANK == 3) {
+        peers = __match_any_sync(FULL_MASK, d);
+        __syncwarp();
+      } else if constexpr (RANK == 4) {
+        peers = warp_peers<8>(d);
+        __syncwarp();
+      } else {
+        peers = warp_peers_p<8>(d);
+        __syncwarp();
+      }
+      wc[d] = base + __popc(peers);  // every peer stores the same count
+      __syncwarp();
+      rank[i] = base + __popc(peers & lt);
+    }
   }
   __syncthreads();
 
@@ -687,66 +727,79 @@ __global__ void __launch_bounds__(WARPS * 32, (Pass8Cfg<K, V, WARPS, ITEMS, RANK
     if (!hooked) LB::store(status + (uint64_t)tile * RADIX + tid, (tile == 0 ? LB::INC : LB::AGG) | (SW)tcount);
   }
   const uint32_t tstart = block_excl_scan_digits<RADIX>(tcount, s_tmp);
-  if (tid < RADIX) {
-    uint32_t excl = 0;  // below 2^32: the count of keys before this tile's digit run
-    bool ok = true;
-    if (hooked) {
-      s_abort = 1;
-    } else if (tile > 0) {
-      int64_t j = (int64_t)tile - 1;
-      uint32_t spins = 0;
-      bool done = false;
-      while (!done && ok) {
-        SW sw[8];
+
+  // Look-back of this thread's digit: eight predecessors per probe (loads
+  // issued together), nearest first.  excl stays below 2^32: the count of
+  // keys before this tile's digit run.
+  uint32_t excl = 0;
+  SW sw[8];
+  int64_t j = (int64_t)tile - 1;
+  auto probe = [&]() {
 #pragma unroll
-        for (int c = 0; c < 8; ++c)
-          sw[c] = j - c >= 0 ? LB::load(status + (uint64_t)(j - c) * RADIX + tid) : LB::INC;
+    for (int c = 0; c < 8; ++c) sw[c] = j - c >= 0 ? LB::load(status + (uint64_t)(j - c) * RADIX + tid) : LB::INC;
+  };
+  // Resolves the probed window (and further ones) into excl, publishes the
+  // inclusive count or the poison word; false when a wait gave up.
+  auto resolve = [&]() -> bool {
+    uint32_t spins = 0;
+    bool done = false, ok = true;
+    while (true) {
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          if (done || !ok) break;
-          SW x = sw[c];
-          while ((x & ~LB::VALUE) == 0) {
-            if (++spins > a.budget) {
-              ok = false;
-              break;
-            }
-            x = LB::load(status + (uint64_t)(j - c) * RADIX + tid);
-          }
-          if (!ok) break;
-          const SW f = x & ~LB::VALUE;
-          if (f == LB::POISON) {
+      for (int c = 0; c < 8; ++c) {
+        if (done || !ok) break;
+        SW x = sw[c];
+        while ((x & ~LB::VALUE) == 0) {
+          if (++spins > a.budget) {
             ok = false;
             break;
           }
-          excl += (uint32_t)(x & LB::VALUE);
-          if (f == LB::INC) done = true;
+          x = LB::load(status + (uint64_t)(j - c) * RADIX + tid);
         }
-        j -= 8;
+        if (!ok) break;
+        const SW f = x & ~LB::VALUE;
+        if (f == LB::POISON) {
+          ok = false;
+          break;
+        }
+        excl += (uint32_t)(x & LB::VALUE);
+        if (f == LB::INC) done = true;
       }
-      LB::store(status + (uint64_t)tile * RADIX + tid, ok ? (LB::INC | (SW)(excl + tcount)) : LB::POISON);
-      if (!ok) s_abort = 1;
+      if (done || !ok) break;
+      j -= 8;
+      probe();
     }
-    s_goff[tid] = a.hist[pass * RADIX + tid] + excl - tstart;
+    LB::store(status + (uint64_t)tile * RADIX + tid, ok ? (LB::INC | (SW)(excl + tcount)) : LB::POISON);
+    return ok;
+  };
+  // Each warp's first slot of the digit in the tile-sorted order.
+  auto first_slots = [&]() {
     uint32_t run = tstart;
 #pragma unroll 4
     for (int w = 0; w < WARPS; ++w) {
       const uint32_t c = s_cnt[w * RADIX + tid];
-      s_cnt[w * RADIX + tid] = run;  // the warp's first slot of the digit
+      s_cnt[w * RADIX + tid] = run;
       run += c;
     }
+  };
+  // The first probe's loads are in flight while the tile-local order is
+  // written (and the predecessors have had that long to publish as well).
+  if (tid < RADIX) {
+    if (!hooked && tile > 0) probe();
+    first_slots();
   }
   __syncthreads();
-  if (s_abort) {
-    leave();
-    return;
-  }
-
-  // ---- tile-sorted order: slot (warp's first slot of the digit + rank)
+  // Tile-sorted order: slot (the warp's first slot of the digit + rank)
   // holds the key at this position.
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
     const uint32_t pos = warp * WK + i * 32 + lane;
     s_perm[wc[digit8<BYTE>(s_keys[pos], shift, mask, bsel)] + rank[i]] = (uint16_t)pos;
+  }
+  if (tid < RADIX) {
+    if (hooked) s_abort = 1;
+    else if (tile > 0 && !resolve()) s_abort = 1;
+    // global position of tile-sorted slot p of this digit = s_goff[d] + p
+    s_goff[tid] = a.hist[pass * RADIX + tid] + excl - tstart;
   }
   if constexpr (C::HAS_V)
     if (bulk && !mbar_wait(&bars[1], 0, mbar_budget_of(a.budget))) s_abort = 1;
@@ -796,11 +849,10 @@ __global__ void k_sort_final_copy(K *keys, const K *keys_alt, V *vals, const V *
   }
 }
 
-// Shared memory a pass kernel of this shape needs.
-// Kernel of the 8-bit passes: 0 = k_sort_pass8 (predicated votes), 1 = the
-// original k_sort_pass, 2 = k_sort_pass8 ranking by shared-memory OR words,
-// 3 = k_sort_pass8 ranking by match.any, 4 = k_sort_pass8 with the plain
-// votes; a test and measurement switch (sort.cu).
+// Kernel of the 8-bit passes: 0 = k_sort_pass8 ranking by leader tables
+// (default), 1 = the original k_sort_pass, 2-5 = k_sort_pass8 ranking by
+// shared-memory OR words, match.any, plain votes, predicated votes; a test
+// and measurement switch (sort.cu).
 int gprtcu_sort_ranking();
 
 template <typename K, typename V, int RB, int WARPS, int ITEMS>
@@ -814,7 +866,8 @@ gprtcuStatus sort_run(const SortArgs &a, cudaStream_t stream) {
   bool match = false;
   if constexpr (RB == 8) {
     using C8 = Pass8Cfg<K, V, WARPS, ITEMS, 0>;
-    static_assert(C8::SMEM <= 227 * 1024, "shared memory per CTA");
+    static_assert(Pass8Cfg<K, V, WARPS, ITEMS, 2>::SMEM <= 227 * 1024, "shared memory per CTA");
+    static_assert(Pass8Cfg<K, V, WARPS, ITEMS, 0>::SMEM <= 227 * 1024, "shared memory per CTA");
     // more keys than 30-bit look-back values can count need the wide words,
     // which only the 8-bit kernel has
     const bool wide = a.n > (uint64_t)LB_VALUE;
@@ -831,23 +884,25 @@ gprtcuStatus sort_run(const SortArgs &a, cudaStream_t stream) {
           GPRTCU_TRY(cudaGetLastError());
           return GPRTCU_OK;
         };
-        constexpr size_t S0 = Pass8Cfg<K, V, WARPS, ITEMS, 0>::SMEM, S1 = Pass8Cfg<K, V, WARPS, ITEMS, 1>::SMEM;
+        // mode m runs RANK m (1 is the original pass, below); the wide
+        // look-back words exist for the default ranking only
+        auto go = [&](auto rank_tag) -> gprtcuStatus {
+          constexpr int R = decltype(rank_tag)::value;
+          constexpr size_t S = Pass8Cfg<K, V, WARPS, ITEMS, R>::SMEM;
+          if constexpr (R == 0) {
+            if (wide)
+              return byte ? launch(k_sort_pass8<K, V, WARPS, ITEMS, true, true, 0>, S)
+                          : launch(k_sort_pass8<K, V, WARPS, ITEMS, false, true, 0>, S);
+          }
+          return byte ? launch(k_sort_pass8<K, V, WARPS, ITEMS, true, false, R>, S)
+                      : launch(k_sort_pass8<K, V, WARPS, ITEMS, false, false, R>, S);
+        };
         gprtcuStatus st;
-        if (mode == 2 && !wide)
-          st = byte ? launch(k_sort_pass8<K, V, WARPS, ITEMS, true, false, 1>, S1)
-                    : launch(k_sort_pass8<K, V, WARPS, ITEMS, false, false, 1>, S1);
-        else if (mode == 3 && !wide)
-          st = byte ? launch(k_sort_pass8<K, V, WARPS, ITEMS, true, false, 2>, S0)
-                    : launch(k_sort_pass8<K, V, WARPS, ITEMS, false, false, 2>, S0);
-        else if (mode == 4 && !wide)
-          st = byte ? launch(k_sort_pass8<K, V, WARPS, ITEMS, true, false, 3>, S0)
-                    : launch(k_sort_pass8<K, V, WARPS, ITEMS, false, false, 3>, S0);
-        else if (wide)
-          st = byte ? launch(k_sort_pass8<K, V, WARPS, ITEMS, true, true, 0>, S0)
-                    : launch(k_sort_pass8<K, V, WARPS, ITEMS, false, true, 0>, S0);
-        else
-          st = byte ? launch(k_sort_pass8<K, V, WARPS, ITEMS, true, false, 0>, S0)
-                    : launch(k_sort_pass8<K, V, WARPS, ITEMS, false, false, 0>, S0);
+        if (wide || mode == 0) st = go(std::integral_constant<int, 0>());
+        else if (mode == 2) st = go(std::integral_constant<int, 2>());
+        else if (mode == 3) st = go(std::integral_constant<int, 3>());
+        else if (mode == 4) st = go(std::integral_constant<int, 4>());
+        else st = go(std::integral_constant<int, 5>());
         if (st != GPRTCU_OK) return st;
       }
     }

@@ -478,9 +478,10 @@ GPRTCU_API void gprtcuDebugScanSkipTile(int64_t tile);
 GPRTCU_API void gprtcuDebugScanSkipStage(int64_t tile);
 GPRTCU_API void gprtcuDebugSortSkipTile(int64_t tile);
 /* Kernel of the 8-bit sort passes, for tests and measurements: 0 (default)
- * the trimmed pass ranking by predicated votes, 1 the original pass, 2 the
- * trimmed pass ranking by shared-memory OR words, 3 by match.any, 4 by the
- * plain votes.  All give the same bits. */
+ * the trimmed pass ranking by per-warp leader tables and five votes, 1 the
+ * original pass, 2-5 the trimmed pass ranking by shared-memory OR words,
+ * match.any, eight plain votes, eight predicated votes.  All give the same
+ * bits. */
 GPRTCU_API void gprtcuDebugSortRanking(int mode);
 GPRTCU_API gprtcuStatus gprtcuDebugRefitSkipLeaf(int64_t slot);
 /* Scan kernel selection for tests: 0 = automatic (default: the persistent

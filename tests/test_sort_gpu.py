@@ -210,9 +210,10 @@ def test_sort_autotune_installs_a_shape(cuda):
 
 @pytest.mark.parametrize("kw,vw", [(4, 4), (4, 8), (8, 4)])
 def test_sort_rankings_agree(cuda, kw, vw):
-    # the 8-bit passes have three kernels (test switch): the trimmed pass with
-    # vote ranking (default), the original pass, and the trimmed pass ranking
-    # by shared-memory OR words; all must give the oracle's bits
+    # the 8-bit passes have several kernels (test switch): the trimmed pass
+    # ranking by leader tables (default), the original pass, and the trimmed
+    # pass ranking by shared-memory OR words, match.any, plain votes and
+    # predicated votes; all must give the oracle's bits
     import torch
     import gprt_b200
     from gprt_b200 import api
@@ -228,7 +229,7 @@ def test_sort_rankings_agree(cuda, kw, vw):
                 v = rng.integers(0, 2 ** 63, size=n, dtype=np.uint64)
                 v = v.astype(np.uint32) if vw == 4 else v
                 ek, ev = oracle.sort(k, v)
-                for mode in (0, 1, 2, 3, 4):
+                for mode in (0, 1, 2, 3, 4, 5):
                     L.gprtcuDebugSortRanking(mode)
                     kt = torch.from_numpy(k.view(np.int32 if kw == 4 else np.int64).copy()).cuda()
                     vt = torch.from_numpy(v.view(np.int32 if vw == 4 else np.int64).copy()).cuda()
