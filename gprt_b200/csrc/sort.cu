@@ -53,13 +53,19 @@ int grid_index(int rb, int tile, int warps) {
 
 // Shapes used until the tuner or the caller picks others, from sweeps of the
 // grid on B200 (uniform and Zipf(1.1) keys, 2^18 .. 2^28 elements): 8-bit
-// digits everywhere; 8192-key tiles of 8 warps for 32-bit keys (2^28 Zipf
-// pairs: 6.20 ms against 6.32 with 16 warps), 4096-key tiles of 8 warps for
-// 64-bit keys; 2048-key tiles of 8 warps below 2^22 keys, where there are too
-// few large tiles to fill the SMs.
+// digits everywhere; for 32-bit keys with 32-bit payloads 6144-key tiles of 8
+// warps (73 KB of shared memory and 80 registers: three CTAs per SM; 2^28
+// Zipf pairs 5.76 ms against 5.95 for 8192-key tiles, which fit two); 32-bit
+// keys alone or with 64-bit payloads 8192-key tiles of 8 warps (2^28 Zipf
+// keys 4.66 ms against 4.81 at 6144); 64-bit keys with 32-bit payloads
+// 6144-key tiles of 8 warps (2^26 segmented (mesh, code) pairs of 44 bits:
+// 3.09 ms against 3.14 at 4096 and 3.80 at 8192), other 64-bit keys
+// 4096-key tiles of 8 warps; 2048-key tiles of 8 warps below 2^22 keys, where
+// there are too few large tiles to fill the SMs.
 int default_index(int slot, uint64_t n) {
   if (n < (1ull << 22)) return grid_index(8, 2048, 8);
-  if (slot == 0 || slot == 1 || slot == 5) return grid_index(8, 8192, 8);
+  if (slot == 1 || slot == 3) return grid_index(8, 6144, 8);
+  if (slot == 0 || slot == 5) return grid_index(8, 8192, 8);
   return grid_index(8, 4096, 8);
 }
 

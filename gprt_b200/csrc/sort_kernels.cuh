@@ -63,9 +63,11 @@ struct SortShape {
 
 // The tuning grid: digit bits {4, 6, 8} x tile {1024 .. 8192} x warps {4, 8,
 // 16}, keeping shapes with 1..32 keys per thread and at least one thread per
-// digit (so 8-bit digits need 8 or 16 warps).
+// digit (so 8-bit digits need 8 or 16 warps); plus 6144-key tiles of 8 warps
+// at 8-bit digits (the largest tile of which three CTAs share an SM with
+// 32-bit keys and payloads).
 inline constexpr SortShape kSortGrid[] = {
-    {8, 1024, 8}, {8, 2048, 8}, {8, 4096, 8}, {8, 8192, 8},                   //
+    {8, 1024, 8}, {8, 2048, 8}, {8, 4096, 8}, {8, 6144, 8}, {8, 8192, 8},     //
     {8, 1024, 16}, {8, 2048, 16}, {8, 4096, 16}, {8, 8192, 16},               //
     {6, 1024, 4}, {6, 2048, 4}, {6, 4096, 4},                                 //
     {6, 1024, 8}, {6, 2048, 8}, {6, 4096, 8}, {6, 8192, 8},                   //

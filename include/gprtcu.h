@@ -131,8 +131,8 @@ GPRTCU_API gprtcuStatus gprtcuSortPairsU64U64(uint64_t *keys, uint64_t *values, 
  * FidelityFX sort is fixed at 4-bit digits and 256-thread groups).  A shape is
  * the digit width (4, 6 or 8 bits), the keys per tile (1024 .. 8192, one
  * thread block per tile) and the warps per block (4, 8 or 16); the grid holds
- * the combinations with 1..32 keys per thread and at least one thread per
- * digit.  Each key/payload type pair has an active shape, used by the entry
+ * the power-of-two tiles with 1..32 keys per thread and at least one thread
+ * per digit, and 6144-key tiles of 8 warps at 8-bit digits.  Each key/payload type pair has an active shape, used by the entry
  * points above (and by the LBVH builds, which sort u32/u32 or u64/u32 pairs):
  * the one installed by gprtcuSortSetConfig or gprtcuSortAutotune, else a
  * built-in default that depends on n (gprtcuSortGetConfig reports the default

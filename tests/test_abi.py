@@ -54,7 +54,7 @@ def test_sort_tuning_grid_host_side():
     grid = api.sort_configs()
     assert len(grid) == len(set(grid))
     assert {g[0] for g in grid} == {4, 6, 8}
-    assert {g[1] for g in grid} == {1024, 2048, 4096, 8192}
+    assert {g[1] for g in grid} == {1024, 2048, 4096, 6144, 8192}
     assert {g[2] for g in grid} == {4, 8, 16}
     for rb, tile, warps in grid:
         items = tile // (32 * warps)
