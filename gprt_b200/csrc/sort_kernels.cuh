@@ -577,11 +577,22 @@ __global__ void __launch_bounds__(WARPS * 32, (Pass8Cfg<K, V, WARPS, ITEMS, RANK
   using LB = LbWord<WIDE>;
   using SW = typename LB::T;
   constexpr int RADIX = C::RADIX, THREADS = C::THREADS, TILE = C::TILE, WK = C::WARP_KEYS;
+  SortHeader *hdr = a.hdr;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // The pass's words, this thread's digit offset and (thread 0) the tile
+  // ticket are requested together, before any of them is tested: one L2
+  // round trip at the start of the CTA instead of four in a row.  A ticket
+  // taken by a pass that then returns is never used by anyone.
+  uint32_t ticket = 0;
+  if (tid == 0) ticket = atomicAdd(&hdr->ticket[1 + pass], 1u);
   const uint32_t flags = ld_relaxed_u32(&a.trivial[pass]);
+  const uint32_t err0 = ld_relaxed_u32(&hdr->h.status);
+  const uint32_t sel = ld_relaxed_u32(&hdr->sel[pass]);
+  const uint32_t ghist = tid < RADIX ? a.hist[pass * RADIX + tid] : 0u;  // global offset of the digit
   if (flags & SORT_FLAG_TRIVIAL) return;  // every key has the same digit: nothing moves
   // An earlier pass gave up on a wait: its output is not a permutation of the
   // keys, so the global digit offsets no longer bound this pass's writes.
-  if (ld_relaxed_u32(&a.hdr->h.status) != 0) return;
+  if (err0 != 0) return;
 
   extern __shared__ __align__(128) unsigned char smem[];
   K *s_keys = reinterpret_cast<K *>(smem);
@@ -596,9 +607,6 @@ __global__ void __launch_bounds__(WARPS * 32, (Pass8Cfg<K, V, WARPS, ITEMS, RANK
   __shared__ uint32_t s_tile, s_abort;
   __shared__ uint32_t s_tmp[32];
 
-  SortHeader *hdr = a.hdr;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint32_t sel = hdr->sel[pass];
   const K *src_k = static_cast<const K *>(sel ? a.keys_alt : a.keys);
   K *dst_k = static_cast<K *>(sel ? a.keys : a.keys_alt);
   const V *src_v = static_cast<const V *>(sel ? a.vals_alt : a.vals);
@@ -609,11 +617,21 @@ __global__ void __launch_bounds__(WARPS * 32, (Pass8Cfg<K, V, WARPS, ITEMS, RANK
   SW *status_next = reinterpret_cast<SW *>(a.status) + (sel ? 0 : a.tiles * RADIX);
 
   if (tid == 0) {
-    s_tile = atomicAdd(&hdr->ticket[1 + pass], 1u);
+    s_tile = ticket;
     s_abort = 0;
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     fence_mbar_init();
+    // thread 0 knows the tile: its copies start before the block barrier
+    if (a.use_bulk && ((uint64_t)ticket + 1) * TILE <= a.n) {
+      const uint64_t ts = (uint64_t)ticket * TILE;
+      mbar_arrive_expect_tx(&bars[0], (uint32_t)C::KEY_BYTES);
+      bulk_g2s(s_keys, src_k + ts, (uint32_t)C::KEY_BYTES, &bars[0]);
+      if constexpr (C::HAS_V) {
+        mbar_arrive_expect_tx(&bars[1], (uint32_t)C::VAL_BYTES);
+        bulk_g2s(s_vals, src_v + ts, (uint32_t)C::VAL_BYTES, &bars[1]);
+      }
+    }
   }
   __syncthreads();
   const uint32_t tile = s_tile;
@@ -621,16 +639,8 @@ __global__ void __launch_bounds__(WARPS * 32, (Pass8Cfg<K, V, WARPS, ITEMS, RANK
   const uint32_t tile_n = (uint32_t)min((uint64_t)TILE, a.n - tile_start);
   const bool full = tile_n == TILE;
   const bool bulk = a.use_bulk && full;
-  if (tid == 0 && bulk) {
-    mbar_arrive_expect_tx(&bars[0], (uint32_t)C::KEY_BYTES);
-    bulk_g2s(s_keys, src_k + tile_start, (uint32_t)C::KEY_BYTES, &bars[0]);
-    if constexpr (C::HAS_V) {
-      mbar_arrive_expect_tx(&bars[1], (uint32_t)C::VAL_BYTES);
-      bulk_g2s(s_vals, src_v + tile_start, (uint32_t)C::VAL_BYTES, &bars[1]);
-    }
-  }
   {
-    uint4 *t4 = reinterpret_cast<uint4 *>(s_cnt);  // counts and (RANK 1) masks are adjacent
+    uint4 *t4 = reinterpret_cast<uint4 *>(s_cnt);  // counts and (RANK 2) masks are adjacent
     for (int i = tid; i < (int)((C::TBL_BYTES + C::MSK_BYTES) / 16); i += THREADS) t4[i] = make_uint4(0u, 0u, 0u, 0u);
   }
   for (int i = tid; i < RADIX; i += THREADS) status_next[(uint64_t)tile * RADIX + i] = 0;
@@ -801,7 +811,7 @@ __global__ void __launch_bounds__(WARPS * 32, (Pass8Cfg<K, V, WARPS, ITEMS, RANK
     if (hooked) s_abort = 1;
     else if (tile > 0 && !resolve()) s_abort = 1;
     // global position of tile-sorted slot p of this digit = s_goff[d] + p
-    s_goff[tid] = a.hist[pass * RADIX + tid] + excl - tstart;
+    s_goff[tid] = ghist + excl - tstart;
   }
   if constexpr (C::HAS_V)
     if (bulk && !mbar_wait(&bars[1], 0, mbar_budget_of(a.budget))) s_abort = 1;
