@@ -413,7 +413,10 @@ struct RrPending {
 // (the dispatch requires a 16-byte aligned output).  Bulk copies instead of
 // the threads' 16-byte stores took 2^30 items from 1.85 to 1.70 ms
 // (partition) and from 1.43 to 1.36 ms (select): the scanners, the pipeline's
-// slowest stage, no longer copy the runs.
+// slowest stage, no longer copy the runs.  Taking each tile's rows, flags and
+// row-count scan before the scanners' stage barrier, which then also stands
+// for "every scanner holds its rows" (one named barrier fewer per tile):
+// 1.70 -> 1.57 ms (partition), 1.36 -> 1.29 ms (select).
 template <int MODE>
 __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *in, uint32_t *out, uint64_t n,
                                                                uint64_t ntiles, ScratchHeader *hdr, uint64_t *status,
@@ -607,6 +610,54 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
       // a warp whose wait gave up raises the flag, and after this barrier
       // all of them see the same flag and the same stage.
       if (!mbar_wait(&s_full[ss], (i / SS) & 1, mb)) s_scan_stop = 1;
+      // Partition / select: each scanner takes its rows, their selection
+      // flags and the warp's scan of the rows' counts before the barrier
+      // (the stage's tile, prefix and per-warp counts are visible once its
+      // wait has succeeded), so the barrier also means that every scanner
+      // holds its rows and the stage may be overwritten by the staging
+      // below; no second barrier before it.  (A warp whose wait gave up
+      // computes from stale words here, which nothing uses: it leaves with
+      // the others after the barrier.)
+      uint4 rows[8];
+      uint32_t fl[8], pk[2] = {0u, 0u}, own[2] = {0u, 0u}, rowtot[2] = {0u, 0u};
+      uint32_t excl = 0, tsel = 0, rowbase = 0, tc = 0;
+      if constexpr (MODE >= 2) {
+        const uint32_t tt = s_tile[ss];
+        excl = pend[q].prefix;
+#pragma unroll
+        for (int k = 0; k < SW; ++k) {
+          const uint32_t pc = pend[q].part[k];
+          rowbase += k < w ? pc : 0u;
+          tsel += pc;
+        }
+        const uint64_t tb = (uint64_t)tt * TILE;
+        tc = tt == RR_END ? 0u : (n - tb < (uint64_t)TILE ? (uint32_t)(n - tb) : TILE);
+        const uint4 *wb = reinterpret_cast<const uint4 *>(sbuf + (size_t)ss * RR_STAGE_BYTES) + w * 8 * 32;
+        const uint32_t flip = want_neg ? 0u : 15u;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          rows[r] = wb[r * 32 + lane];
+          const uint32_t l0 = (uint32_t)((w * 8 + r) * 128 + lane * 4);
+          const uint32_t rem = tc > l0 ? tc - l0 : 0u;
+          const uint32_t valid = rem >= 4 ? 15u : (1u << rem) - 1u;
+          fl[r] = (((rows[r].x >> 31) | ((rows[r].y >> 31) << 1) | ((rows[r].z >> 31) << 2) |
+                    ((rows[r].w >> 31) << 3)) ^ flip) & valid;
+          pk[r >> 2] |= (uint32_t)__popc(fl[r]) << (8 * (r & 3));
+        }
+        // Inclusive warp scan of the rows' counts, four rows to a word (a
+        // row's total is at most 128, so a byte holds it).
+        own[0] = pk[0];
+        own[1] = pk[1];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const uint32_t y = __shfl_up_sync(FULL_MASK, pk[h], o);
+            if (lane >= o) pk[h] += y;
+          }
+        rowtot[0] = __shfl_sync(FULL_MASK, pk[0], 31);
+        rowtot[1] = __shfl_sync(FULL_MASK, pk[1], 31);
+      }
       named_bar_sync(1, SW * 32);
       if (s_scan_stop) {
         if (leader) record_error(hdr, GPRTCU_ERR_TIMEOUT);
@@ -615,41 +666,8 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
       const uint32_t t = s_tile[ss];
       if (t == RR_END) break;
       if constexpr (MODE >= 2) {
-        const uint32_t excl = pend[q].prefix;
-        uint32_t tsel = 0, rowbase = 0;
-#pragma unroll
-        for (int k = 0; k < SW; ++k) {
-          const uint32_t pc = pend[q].part[k];
-          rowbase += k < w ? pc : 0u;
-          tsel += pc;
-        }
         const uint64_t base = (uint64_t)t * TILE;
-        const uint32_t tc = n - base < (uint64_t)TILE ? (uint32_t)(n - base) : TILE;
         uint32_t *sb = reinterpret_cast<uint32_t *>(sbuf + (size_t)ss * RR_STAGE_BYTES);
-        const uint4 *wb = reinterpret_cast<const uint4 *>(sb) + w * 8 * 32;
-        uint4 v[8];
-        uint32_t fl[8], pk[2] = {0u, 0u};
-        const uint32_t flip = want_neg ? 0u : 15u;
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          v[r] = wb[r * 32 + lane];
-          const uint32_t l0 = (uint32_t)((w * 8 + r) * 128 + lane * 4);
-          const uint32_t rem = tc > l0 ? tc - l0 : 0u;
-          const uint32_t valid = rem >= 4 ? 15u : (1u << rem) - 1u;
-          fl[r] = (((v[r].x >> 31) | ((v[r].y >> 31) << 1) | ((v[r].z >> 31) << 2) | ((v[r].w >> 31) << 3)) ^ flip) & valid;
-          pk[r >> 2] |= (uint32_t)__popc(fl[r]) << (8 * (r & 3));
-        }
-        // Inclusive warp scan of the rows' counts, four rows to a word (a
-        // row's total is at most 128, so a byte holds it).
-        const uint32_t own[2] = {pk[0], pk[1]};
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1)
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const uint32_t y = __shfl_up_sync(FULL_MASK, pk[h], o);
-            if (lane >= o) pk[h] += y;
-          }
-        const uint32_t rowtot[2] = {__shfl_sync(FULL_MASK, pk[0], 31), __shfl_sync(FULL_MASK, pk[1], 31)};
         // Selected rank ls goes to out[excl + ls], unselected rank lu to
         // out[top - lu].  Staged at sb[s1 + ls] and sb[u_top - lu], with the
         // shifts chosen so that shared and global indices agree modulo 4:
@@ -658,14 +676,13 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
         const uint64_t top = (n - 1) - (base - excl);
         const uint32_t s1 = (uint32_t)(excl & 3);
         const uint32_t u_top = TILE + 7 + (uint32_t)((top - (TILE + 7)) & 3);  // <= TILE + 10; u_top == top mod 4
-        named_bar_sync(1, SW * 32);  // every scanner holds its rows: the stage can be overwritten
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
           const uint32_t sh = 8 * (r & 3);
           // selected items of the tile before this lane's first in row r
           uint32_t ls = rowbase + ((pk[r >> 2] - own[r >> 2]) >> sh & 0xFFu);
           const uint32_t l0 = (uint32_t)((w * 8 + r) * 128 + lane * 4);
-          const uint32_t vals[4] = {v[r].x, v[r].y, v[r].z, v[r].w};
+          const uint32_t vals[4] = {rows[r].x, rows[r].y, rows[r].z, rows[r].w};
 #pragma unroll
           for (int c = 0; c < 4; ++c) {
             const uint32_t sel = (fl[r] >> c) & 1u;
