@@ -658,6 +658,25 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
         rowtot[0] = __shfl_sync(FULL_MASK, pk[0], 31);
         rowtot[1] = __shfl_sync(FULL_MASK, pk[1], 31);
       }
+      // Sums: the rows, their sums and the warp scans of the sums likewise
+      // come before the barrier; after it only the carry is added.
+      uint32_t sum[8], inc[8];
+      if constexpr (MODE < 2) {
+        const uint4 *wb = reinterpret_cast<const uint4 *>(sbuf + (size_t)ss * RR_STAGE_BYTES) + w * 8 * 32;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          rows[r] = wb[r * 32 + lane];
+          sum[r] = (rows[r].x + rows[r].y) + (rows[r].z + rows[r].w);
+          inc[r] = sum[r];
+        }
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+#pragma unroll
+          for (int r = 0; r < 8; ++r) {
+            const uint32_t y = __shfl_up_sync(FULL_MASK, inc[r], o);
+            if (lane >= o) inc[r] += y;
+          }
+      }
       named_bar_sync(1, SW * 32);
       if (s_scan_stop) {
         if (leader) record_error(hdr, GPRTCU_ERR_TIMEOUT);
@@ -726,21 +745,7 @@ __global__ void __launch_bounds__(RR_THREADS, 1) k_scan_reread(const uint32_t *i
       uint32_t carry = pend[q].prefix;
       for (int k = 0; k < w; ++k) carry += pend[q].part[k];
       uint4 *wb = reinterpret_cast<uint4 *>(sbuf + (size_t)ss * RR_STAGE_BYTES) + w * 8 * 32;
-      uint4 v[8];
-      uint32_t sum[8], inc[8];
-#pragma unroll
-      for (int r = 0; r < 8; ++r) {
-        v[r] = wb[r * 32 + lane];
-        sum[r] = (v[r].x + v[r].y) + (v[r].z + v[r].w);
-        inc[r] = sum[r];
-      }
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1)
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          const uint32_t y = __shfl_up_sync(FULL_MASK, inc[r], o);
-          if (lane >= o) inc[r] += y;
-        }
+      const uint4 *v = rows;
 #pragma unroll
       for (int r = 0; r < 8; ++r) {
         const uint32_t p = carry + inc[r] - sum[r];
