@@ -48,14 +48,16 @@ gprtcuStatus gprtcu_fold_status(const void *scratch, uint32_t *acc, cudaStream_t
   return GPRTCU_OK;
 }
 
+// SMs of the current device, looked up once per device (host threads may
+// race to fill the cache; they all store the same value).
 int gprtcu_num_sms() {
-  static int cached[64] = {0};
+  static std::atomic<int> cached[64];
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-  if (cached[dev] == 0) {
-    int v = 0;
+  int v = cached[dev].load(std::memory_order_relaxed);
+  if (v == 0) {
     if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
-    cached[dev] = v;
+    cached[dev].store(v, std::memory_order_relaxed);
   }
-  return cached[dev];
+  return v;
 }

@@ -952,14 +952,17 @@ extern "C" GPRTCU_API size_t gprtcuScanScratchSize(uint64_t n) {
 }
 
 // CTAs of the re-read kernel that fit on the device at once (one per SM on
-// B200); 0 if it does not fit.  Sets the shared-memory attribute once per device.
+// B200); 0 if it does not fit.  Sets the shared-memory attribute once per
+// device (host threads may race to do so; they all store the same value, and
+// a thread that finds no value yet does the set-up itself).
 static int reread_ctas() {
-  static int cached[64];
-  static bool done[64];
+  static std::atomic<int> cached[64];  // the CTA count + 1; 0 = not known yet
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
-  if (!done[dev]) {
-    int occ = 0;
+  const int known = cached[dev].load(std::memory_order_acquire);
+  if (known > 0) return known - 1;
+  {
+    int occ = 0, ctas = 0;
     if (cudaFuncSetAttribute(k_scan_reread<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RR_SMEM) ==
             cudaSuccess &&
         cudaFuncSetAttribute(k_scan_reread<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RR_SMEM) ==
@@ -969,13 +972,11 @@ static int reread_ctas() {
         cudaFuncSetAttribute(k_scan_reread<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RR_SMEM) ==
             cudaSuccess &&
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_scan_reread<0>, RR_THREADS, RR_SMEM) == cudaSuccess)
-      cached[dev] = occ * gprtcu_num_sms();
-    else
-      cached[dev] = 0;
+      ctas = occ * gprtcu_num_sms();
     cudaGetLastError();
-    done[dev] = true;
+    cached[dev].store(ctas + 1, std::memory_order_release);
+    return ctas;
   }
-  return cached[dev];
 }
 
 template <int THREADS, int VECS, int LBW>

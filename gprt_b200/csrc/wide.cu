@@ -896,11 +896,13 @@ extern "C" GPRTCU_API gprtcuStatus gprtcuWideBuild(const gprtcuLbvh *binary, con
   // grid is what fits on the GPU at once (7 CTAs of 128 threads per SM: 72
   // registers, 24 KB of shared memory): a grid-stride loop with a second wave
   // of CTAs ran the level for about twice a CTA's share (6.6 against 4.8 ms).
-  static int level_ctas = 0;
+  static std::atomic<int> level_ctas_cache{0};  // host threads may race to fill it with the same value
+  int level_ctas = level_ctas_cache.load(std::memory_order_relaxed);
   if (!level_ctas) {
     int occ = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_wide_level, 128, 0) != cudaSuccess || occ < 1) occ = 1;
     level_ctas = occ;
+    level_ctas_cache.store(occ, std::memory_order_relaxed);
   }
   const int grid = gprtcu_num_sms() * level_ctas;
   for (int level = 0; level < kWideMaxLevels; ++level) {
