@@ -38,6 +38,14 @@ __device__ __forceinline__ void load_tri(const float *pos, const uint32_t *tri, 
   }
 }
 
+// Centroid (p1 + p2 + p3) / 3 of a triangle (getTriangleCentroid,
+// gprt/development/gprt_lbvh.hlsl:139-146), each operation rounded once.
+__device__ __forceinline__ float4 tri_centroid(const float v[9]) {
+  return make_float4(__fdiv_rn(__fadd_rn(__fadd_rn(v[0], v[3]), v[6]), 3.0f),
+                     __fdiv_rn(__fadd_rn(__fadd_rn(v[1], v[4]), v[7]), 3.0f),
+                     __fdiv_rn(__fadd_rn(__fadd_rn(v[2], v[5]), v[8]), 3.0f), 0.0f);
+}
+
 // getTriangleBounds (gprt/development/gprt_lbvh.hlsl:121-129).
 __device__ __forceinline__ void tri_box(const float v[9], float b[6]) {
 #pragma unroll
@@ -205,8 +213,13 @@ __device__ __forceinline__ void prim_box(const float *pos, const uint32_t *tri, 
 // initialises both.  One mesh: block reduction, one atomic per CTA and
 // component.  Many meshes: warp reduction when the warp's primitives share a
 // mesh, per-lane atomics at mesh boundaries.
+// With cent (triangles whose build writes leaf-order triangles), each
+// triangle's centroid (p1 + p2 + p3) / 3 is stored there in primitive order
+// for k_codes, which then reads 16 coalesced bytes instead of gathering the
+// triangle again (the refit overwrites the array later).
 template <int KIND, bool BATCHED>
-__global__ void __launch_bounds__(256) k_bounds(const float *pos, const uint32_t *tri, MeshMap mm, uint32_t *slots) {
+__global__ void __launch_bounds__(256) k_bounds(const float *pos, const uint32_t *tri, MeshMap mm, uint32_t *slots,
+                                                float4 *cent) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t w[6] = {0, 0, 0, 0, 0, 0};
   const uint64_t total = ((uint64_t)mm.n + 31) & ~31ull;
@@ -222,6 +235,7 @@ __global__ void __launch_bounds__(256) k_bounds(const float *pos, const uint32_t
         tw[k] = ~f2ord(t[k]);
         tw[3 + k] = f2ord(t[3 + k]);
       }
+      if (KIND == 0 && cent) cent[i] = tri_centroid(v);
     }
     if (!BATCHED) {
 #pragma unroll
@@ -265,7 +279,7 @@ __global__ void __launch_bounds__(256) k_bounds(const float *pos, const uint32_t
 template <int KIND, bool BATCHED>
 __global__ void __launch_bounds__(256) k_codes(const float *pos, const uint32_t *tri, MeshMap mm, const uint32_t *slots,
                                                int code_kind, uint32_t *codes, uint64_t *keys, uint32_t *ids,
-                                               float *scene_out) {
+                                               float *scene_out, const float4 *cent) {
   const uint64_t total = ((uint64_t)mm.n + 31) & ~31ull;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t m = BATCHED ? mm.warp_mesh_of_prim(i - (threadIdx.x & 31)) : 0u;
@@ -285,10 +299,17 @@ __global__ void __launch_bounds__(256) k_codes(const float *pos, const uint32_t 
       }
     float c[3];
     if (KIND == 0) {
-      float v[9];
-      load_tri(pos, tri, (uint32_t)i, v);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) c[k] = __fdiv_rn(__fadd_rn(__fadd_rn(v[k], v[3 + k]), v[6 + k]), 3.0f);
+      float4 c4;
+      if (cent) {
+        c4 = cent[i];
+      } else {
+        float v[9];
+        load_tri(pos, tri, (uint32_t)i, v);
+        c4 = tri_centroid(v);
+      }
+      c[0] = c4.x;
+      c[1] = c4.y;
+      c[2] = c4.z;
     } else if (KIND == 2) {
       float v[9];
       load_edge(pos, tri, (uint32_t)i, v);
@@ -587,9 +608,12 @@ void launch_build(const float *pos, const uint32_t *tri, MeshMap mm, int codeKin
   const int g = grid_for(mm.n, 256, 8);
   int4 *nodes = (int4 *)out->nodes;
   if (stage == 0) {
-    k_bounds<KIND, BATCHED><<<g, 256, 0, stream>>>(pos, tri, mm, slots);
+    // the centroids pass through the leaf-order triangle array, which the
+    // refit overwrites afterwards
+    float4 *cent = KIND == 0 ? (float4 *)out->leafTris : nullptr;
+    k_bounds<KIND, BATCHED><<<g, 256, 0, stream>>>(pos, tri, mm, slots, cent);
     k_codes<KIND, BATCHED><<<g, 256, 0, stream>>>(pos, tri, mm, slots, codeKind, out->codes, keys, out->ids,
-                                                  out->sceneBounds);
+                                                  out->sceneBounds, cent);
   } else {
     if (mm.n > mm.meshes)
       k_karras<BATCHED><<<(unsigned)((mm.n - mm.meshes + 255) / 256), 256, 0, stream>>>(out->codes, keys, mm, nodes,
