@@ -15,12 +15,12 @@
 //      constant (skipped);
 //   2. one digit-binning kernel per pass: a tile of keys and one of payloads
 //      arrive in shared memory by bulk async copies (TMA); warps rank their
-//      keys with a ballot multisplit against per-warp shared histograms,
+//      keys against per-warp shared histograms (the 8-bit pass finds a key's
+//      equal-digit lanes through a per-warp leader table and five ballots),
 //      each digit's tile count is published to a per-(tile, digit) status
-//      word and a decoupled
-//      look-back over earlier tiles gives the digit's global position; keys,
-//      then payloads, are reordered in shared memory so the scatter leaves
-//      the tile as coalesced per-digit runs.
+//      word and a decoupled look-back over earlier tiles gives the digit's
+//      global position; the tile-sorted order is built in shared memory so
+//      the scatter leaves the tile as coalesced per-digit runs.
 // Traffic per pass: read + write of keys and payloads; plus one read of the
 // keys for the histograms.
 #pragma once
