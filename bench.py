@@ -419,6 +419,11 @@ def cpu_sample_run(sample, match=None):
             match["hits"] += int(hit.sum())
             match["id_mismatches"] += bad_id
             match["t_mismatches"] += bad_t
+            # diagnostic: the FP64 closest id through the same tree
+            d = oracle.fp64_id_diagnostic(pos, tri, e, rays, gp)
+            f = match.setdefault("fp64_ids", {})
+            for k, v in d.items():
+                f[k] = f.get(k, 0) + v
     return tb, tt, ntri, nray
 
 
@@ -433,6 +438,12 @@ def cpu_baseline(sample, meshes):
     match["match"] = match["id_mismatches"] == 0 and match["t_mismatches"] == 0 and match["rays"] > 0
     match["compared"] = ("the oracle's FP32 LBVH build + closest-hit traversal of each mesh against the "
                          "batched + quantised step's hits: primitive id of every ray, t bits of every hit")
+    if "fp64_ids" in match:
+        match["fp64_ids"]["compared"] = (
+            "diagnostic: the GPU's closest id against the FP64 closest id through the same tree (watertight test "
+            "in double precision); fp32_edge / fp64_edge: one precision's test hits a triangle the other's "
+            "misses (rays through shared edges and vertices); near_ties: both hit both triangles and their FP64 "
+            "distances agree within 1e-6 relative")
     return {"value": nray / (tb + tt) / 1e6, "unit": "Mrays/s", "cores": oracle.num_threads(), "kind": "port",
             "sample": "first %d of %d meshes of the same workload (%d triangles, %d rays), copied from the "
                       "device; per mesh a full LBVH build and a closest-hit trace of its rays"

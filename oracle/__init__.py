@@ -78,6 +78,9 @@ def lib():
         L.orc_t64.restype = ctypes.c_double
         L.orc_trace_brute.argtypes = [vp, vp, u32, vp, u64, vp]
         L.orc_trace_lbvh.argtypes = [vp, vp, u32, vp, vp, vp, u64, i32, vp]
+        L.orc_trace_lbvh64.argtypes = [vp, vp, u32, vp, vp, vp, u64, vp, vp]
+        L.orc_isect_tri64.argtypes = [vp, vp, vp, vp, vp]
+        L.orc_isect_tri64.restype = i32
         L.orc_num_threads.restype = i32
         L.orc_solid_vertex_count.argtypes = [u32]
         L.orc_solid_vertex_count.restype = i32
@@ -354,6 +357,59 @@ def trace_lbvh(pos, tri, bvh, rays, anyhit=False):
     lib().orc_trace_lbvh(_p(pos), _p(tri), tri.shape[0], _p(nodes), _p(aabbs), _p(rays), rays.shape[0],
                          1 if anyhit else 0, _p(hits))
     return hits
+
+
+def trace_lbvh64(pos, tri, bvh, rays):
+    """Closest hit through the same tree in FP64: (prim uint32[R], t float64[R])."""
+    pos = np.ascontiguousarray(pos, dtype=np.float32)
+    tri = np.ascontiguousarray(tri, dtype=np.uint32)
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    nodes = np.ascontiguousarray(bvh["nodes"], dtype=np.int32)
+    aabbs = np.ascontiguousarray(bvh["aabbs"], dtype=np.float32)
+    prim = np.zeros(rays.shape[0], np.uint32)
+    t = np.zeros(rays.shape[0], np.float64)
+    lib().orc_trace_lbvh64(_p(pos), _p(tri), tri.shape[0], _p(nodes), _p(aabbs), _p(rays), rays.shape[0], _p(prim),
+                           _p(t))
+    return prim, t
+
+
+def isect64(ray, v0, v1, v2):
+    a = [np.ascontiguousarray(v, dtype=np.float32) for v in (ray, v0, v1, v2)]
+    t = np.zeros(1, np.float64)
+    hit = lib().orc_isect_tri64(*[_p(v) for v in a], _p(t))
+    return bool(hit), float(t[0])
+
+
+def fp64_id_diagnostic(pos, tri, bvh, rays, prim32):
+    """Rays whose FP32 closest id (prim32) differs from the FP64 closest id
+    through the same tree, by kind:
+      fp32_edge   the FP32 test hits a triangle that the FP64 test misses
+                  (a ray through a shared edge or vertex; FP64 then reports
+                  a triangle behind it, or a miss);
+      fp64_edge   the FP64 test hits a triangle that the FP32 test misses;
+      near_ties   both precisions hit both triangles, and their FP64
+                  distances agree within 1e-6 relative;
+      other       anything else (none is expected)."""
+    prim32 = np.asarray(prim32, dtype=np.uint32)
+    p64, t64v = trace_lbvh64(pos, tri, bvh, rays)
+    diff = np.nonzero(p64 != prim32)[0]
+    out = {"rays": int(prim32.size), "disagreements": int(diff.size), "fp32_edge": 0, "fp64_edge": 0,
+           "near_ties": 0, "other": 0}
+    pos3 = np.ascontiguousarray(pos, dtype=np.float32).reshape(-1, 3)
+    tri3 = np.ascontiguousarray(tri, dtype=np.uint32).reshape(-1, 3)
+    rays8 = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    for r in diff:
+        a, b = int(prim32[r]), int(p64[r])
+        if a != 0xFFFFFFFF and not isect64(rays8[r], *pos3[tri3[a]])[0]:
+            out["fp32_edge"] += 1
+        elif b != 0xFFFFFFFF and not isect32(rays8[r], *pos3[tri3[b]])[0]:
+            out["fp64_edge"] += 1
+        elif a != 0xFFFFFFFF and b != 0xFFFFFFFF and \
+                abs(isect64(rays8[r], *pos3[tri3[a]])[1] - t64v[r]) <= 1e-6 * abs(t64v[r]):
+            out["near_ties"] += 1
+        else:
+            out["other"] += 1
+    return out
 
 
 def t64(ray, v0, v1, v2):

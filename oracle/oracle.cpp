@@ -634,6 +634,105 @@ extern "C" void orc_trace_lbvh(const float *pos, const uint32_t *tri, uint32_t n
   }
 }
 
+// ---- FP64 closest hit through the same tree: the accuracy reference for
+// hit ids.  The watertight test of isect32 (Woop et al. 2013, section 3)
+// carried out in double precision on the float inputs, ties to the lowest
+// id; boxes tested by ray_box as in orc_trace_lbvh (the 2^-18 widening also
+// covers double-precision hits, which lie inside the same float boxes).  Rays
+// whose FP32 and FP64 closest ids differ are the diagnostic this serves: hits
+// at shared edges and near-ties that FP32 cannot separate.
+struct RayPre64 {
+  double o[3], d[3], tmin, tmax;
+  int kx, ky, kz;
+  double Sx, Sy, Sz;
+};
+static inline void ray_pre64(const float *r, RayPre64 &p) {
+  for (int a = 0; a < 3; ++a) {
+    p.o[a] = r[a];
+    p.d[a] = r[4 + a];
+  }
+  p.tmin = r[3];
+  p.tmax = r[7];
+  double ax = std::fabs(p.d[0]), ay = std::fabs(p.d[1]), az = std::fabs(p.d[2]);
+  int kz = (ax >= ay) ? (ax >= az ? 0 : 2) : (ay >= az ? 1 : 2);
+  int kx = kz + 1 == 3 ? 0 : kz + 1;
+  int ky = kx + 1 == 3 ? 0 : kx + 1;
+  if (p.d[kz] < 0.0) std::swap(kx, ky);
+  p.kx = kx;
+  p.ky = ky;
+  p.kz = kz;
+  p.Sx = p.d[kx] / p.d[kz];
+  p.Sy = p.d[ky] / p.d[kz];
+  p.Sz = 1.0 / p.d[kz];
+}
+static inline int isect64(const RayPre64 &p, const float *v0, const float *v1, const float *v2, double *tout) {
+  double A[3], B[3], C[3];
+  for (int a = 0; a < 3; ++a) {
+    A[a] = (double)v0[a] - p.o[a];
+    B[a] = (double)v1[a] - p.o[a];
+    C[a] = (double)v2[a] - p.o[a];
+  }
+  double Ax = A[p.kx] - p.Sx * A[p.kz], Ay = A[p.ky] - p.Sy * A[p.kz];
+  double Bx = B[p.kx] - p.Sx * B[p.kz], By = B[p.ky] - p.Sy * B[p.kz];
+  double Cx = C[p.kx] - p.Sx * C[p.kz], Cy = C[p.ky] - p.Sy * C[p.kz];
+  double U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+  if ((U < 0.0 || V < 0.0 || W < 0.0) && (U > 0.0 || V > 0.0 || W > 0.0)) return 0;
+  double det = (U + V) + W;
+  if (det == 0.0) return 0;
+  double T = (U * (p.Sz * A[p.kz]) + V * (p.Sz * B[p.kz])) + W * (p.Sz * C[p.kz]);
+  double t = T / det;
+  if (!(t >= p.tmin && t <= p.tmax)) return 0;
+  *tout = t;
+  return 1;
+}
+
+extern "C" int orc_isect_tri64(const float *ray, const float *v0, const float *v1, const float *v2, double *t) {
+  RayPre64 q;
+  ray_pre64(ray, q);
+  return isect64(q, v0, v1, v2, t);
+}
+
+extern "C" void orc_trace_lbvh64(const float *pos, const uint32_t *tri, uint32_t n, const int32_t *nodes,
+                                 const float *aabbs, const float *rays, uint64_t nrays, uint32_t *prim, double *tout) {
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t r = 0; r < (int64_t)nrays; ++r) {
+    RayPre p;
+    ray_pre(rays + 8 * r, p);
+    RayPre64 q;
+    ray_pre64(rays + 8 * r, q);
+    uint32_t best = 0xFFFFFFFFu;
+    double bt = q.tmax;
+    if (n > 0) {
+      int32_t stack[128];
+      int sp = 0;
+      stack[sp++] = 0;
+      while (sp > 0) {
+        int32_t node = stack[--sp];
+        float tn;
+        // culling distance rounded up to float, so no box holding a hit at bt is pruned
+        const float btf = (float)bt < bt ? std::nextafter((float)bt, INFINITY) : (float)bt;
+        if (!ray_box(p, &aabbs[6 * (size_t)node], btf, &tn)) continue;
+        if ((double)tn > bt) continue;
+        int32_t leaf = nodes[4 * (size_t)node + 3];
+        if (leaf >= 0) {
+          const float *a, *b, *c;
+          tri_verts(pos, tri, (uint32_t)leaf, a, b, c);
+          double t;
+          if (isect64(q, a, b, c, &t) && (best == 0xFFFFFFFFu || t < bt || (t == bt && (uint32_t)leaf < best))) {
+            best = (uint32_t)leaf;
+            bt = t;
+          }
+        } else {
+          stack[sp++] = nodes[4 * (size_t)node + 1];
+          stack[sp++] = nodes[4 * (size_t)node + 0];
+        }
+      }
+    }
+    prim[r] = best;
+    tout[r] = best != 0xFFFFFFFFu ? bt : INFINITY;
+  }
+}
+
 extern "C" int orc_num_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

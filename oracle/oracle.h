@@ -115,6 +115,14 @@ void orc_trace_brute(const float *pos, const uint32_t *tri, uint32_t n, const fl
  * LBVH (nodes + aabbs).  OpenMP over rays.  Hit t is the refined t. */
 void orc_trace_lbvh(const float *pos, const uint32_t *tri, uint32_t n, const int32_t *nodes,
                     const float *aabbs, const float *rays, uint64_t nrays, int anyhit, orc_hit *hits);
+/* The watertight ray/triangle test in double precision (1 = hit, *t its
+ * distance). */
+int orc_isect_tri64(const float *ray, const float *v0, const float *v1, const float *v2, double *t);
+/* Closest hit through the same tree with the watertight test in double
+ * precision (ties to the lowest id): prim[r] and the FP64 t (INFINITY for a
+ * miss).  The accuracy reference for hit ids. */
+void orc_trace_lbvh64(const float *pos, const uint32_t *tri, uint32_t n, const int32_t *nodes, const float *aabbs,
+                      const float *rays, uint64_t nrays, uint32_t *prim, double *t);
 
 /* ---------------- solid cells ---------------- */
 /* Vertex count and hit kind of a cell type (gprt/gprt_fallbacks.slang:289-318). */

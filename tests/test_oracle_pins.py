@@ -239,3 +239,59 @@ def test_solid_cell_types_match_reference():
         h1, r1 = oracle.solid_intersect(pts[q, :3], verts[idx[c, :n]], n)
         h2, r2 = oracle.ref_solid_intersect(pts[q, :3], verts[idx[c, :n]], n)
         assert h1 == h2 and (not h1 or np.array_equal(r1.view(np.uint32), r2.view(np.uint32))), q
+
+
+def test_fp64_traversal_matches_fp64_brute_force():
+    # The FP64 closest-hit search through the tree (the accuracy reference for
+    # hit ids) against an FP64 search over every triangle, on a small scene:
+    # the tree must never prune a triangle that FP64 hits.
+    from gprt_b200 import scenes
+    pos, tri = scenes.soup(600, seed=21, sigma=0.03)
+    rays = scenes.rays(1500, seed=22)
+    e = oracle.lbvh_build_tri(pos, tri)
+    p64, t64v = oracle.trace_lbvh64(pos, tri, e, rays)
+    v = pos.reshape(-1, 3)[tri.reshape(-1)].reshape(-1, 3, 3)
+    r8 = rays.reshape(-1, 8)
+    for r in range(r8.shape[0]):
+        best, bt = 0xFFFFFFFF, np.inf
+        for i in range(v.shape[0]):
+            hit, t = _isect64(r8[r], v[i])
+            if hit and (t < bt or (t == bt and i < best)):
+                best, bt = i, t
+        assert p64[r] == best, r
+        if best != 0xFFFFFFFF:
+            assert t64v[r] == bt, r
+    # the GPU-side FP32 ids (here the FP32 oracle's) differ from FP64 only at near ties or edges
+    h32 = oracle.trace_lbvh(pos, tri, e, rays)
+    d = oracle.fp64_id_diagnostic(pos, tri, e, rays, h32["prim"])
+    assert d["other"] == 0, d
+
+
+def _isect64(ray, v):
+    """The double-precision watertight test (Woop et al. 2013, section 3) of
+    the oracle's FP64 search, restated in numpy scalars."""
+    o = ray[:3].astype(np.float64)
+    dr = ray[4:7].astype(np.float64)
+    tmin, tmax = float(ray[3]), float(ray[7])
+    a = np.abs(dr)
+    kz = (0 if a[0] >= a[2] else 2) if a[0] >= a[1] else (1 if a[1] >= a[2] else 2)
+    kx = 0 if kz + 1 == 3 else kz + 1
+    ky = 0 if kx + 1 == 3 else kx + 1
+    if dr[kz] < 0.0:
+        kx, ky = ky, kx
+    Sx, Sy, Sz = dr[kx] / dr[kz], dr[ky] / dr[kz], 1.0 / dr[kz]
+    A, B, C = (v[k].astype(np.float64) - o for k in range(3))
+    Ax, Ay = A[kx] - Sx * A[kz], A[ky] - Sy * A[kz]
+    Bx, By = B[kx] - Sx * B[kz], B[ky] - Sy * B[kz]
+    Cx, Cy = C[kx] - Sx * C[kz], C[ky] - Sy * C[kz]
+    U, V, W = Cx * By - Cy * Bx, Ax * Cy - Ay * Cx, Bx * Ay - By * Ax
+    if (U < 0.0 or V < 0.0 or W < 0.0) and (U > 0.0 or V > 0.0 or W > 0.0):
+        return False, 0.0
+    det = (U + V) + W
+    if det == 0.0:
+        return False, 0.0
+    T = (U * (Sz * A[kz]) + V * (Sz * B[kz])) + W * (Sz * C[kz])
+    t = T / det
+    if not (tmin <= t <= tmax):
+        return False, 0.0
+    return True, t
