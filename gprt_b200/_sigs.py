@@ -63,6 +63,7 @@ SIGNATURES = {
     "gprtcuDebugScanSkipStage": ([i64], None),
     "gprtcuDebugSortSkipTile": ([i64], None),
     "gprtcuDebugSortRanking": ([i32], None),
+    "gprtcuDebugSortPrefetch": ([i32], None),
     "gprtcuDebugRefitSkipLeaf": ([i64], st),
     "gprtcuDebugScanImpl": ([i32], None),
 }

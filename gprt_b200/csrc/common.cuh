@@ -154,6 +154,11 @@ __device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_gmem, u
       "l"(src_gmem), "r"(bytes), "r"(smem_addr(bar))
       : "memory");
 }
+// Fetches [src_gmem, src_gmem + bytes) into L2 without waiting for it (a
+// hint: no completion to track; both 16-byte aligned / multiples of 16).
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src_gmem, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src_gmem), "r"(bytes) : "memory");
+}
 // shared -> global, tracked by bulk groups.
 __device__ __forceinline__ void bulk_s2g(void *dst_gmem, const void *src_smem, uint32_t bytes) {
   asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst_gmem), "r"(smem_addr(src_smem)),

@@ -93,6 +93,7 @@ struct SortArgs {
   int use_bulk;
   int sms;
   int64_t skip_tile;  // test hook: this tile of every pass never publishes (-1: none)
+  uint32_t pf_tiles;  // 8-bit passes: a CTA prefetches into L2 the tile this far after its own (0: none)
 };
 
 using SortRunFn = gprtcuStatus (*)(const SortArgs &, cudaStream_t);
@@ -632,6 +633,14 @@ __global__ void __launch_bounds__(WARPS * 32, (Pass8Cfg<K, V, WARPS, ITEMS, RANK
         bulk_g2s(s_vals, src_v + ts, (uint32_t)C::VAL_BYTES, &bars[1]);
       }
     }
+    // The tile that a CTA starting about pf_tiles tickets later will take:
+    // its keys and payloads are fetched into L2 now, so that CTA's copies
+    // hit L2 instead of waiting on DRAM at its start.
+    const uint64_t pt = (uint64_t)ticket + a.pf_tiles;
+    if (a.pf_tiles && a.use_bulk && (pt + 1) * TILE <= a.n) {
+      bulk_prefetch_l2(src_k + pt * TILE, (uint32_t)C::KEY_BYTES);
+      if constexpr (C::HAS_V) bulk_prefetch_l2(src_v + pt * TILE, (uint32_t)C::VAL_BYTES);
+    }
   }
   __syncthreads();
   const uint32_t tile = s_tile;
@@ -866,6 +875,9 @@ __global__ void k_sort_final_copy(K *keys, const K *keys_alt, V *vals, const V *
 // shared-memory OR words, match.any, plain votes, predicated votes; a test
 // and measurement switch (sort.cu).
 int gprtcu_sort_ranking();
+// L2 prefetch distance of the 8-bit passes in quarters of a resident wave
+// of CTAs (0: none; sort.cu).
+int gprtcu_sort_prefetch();
 
 template <typename K, typename V, int RB, int WARPS, int ITEMS>
 gprtcuStatus sort_run(const SortArgs &a, cudaStream_t stream) {
@@ -892,7 +904,9 @@ gprtcuStatus sort_run(const SortArgs &a, cudaStream_t stream) {
         const bool byte = bits == 8 && (shift & 7) == 0;
         auto launch = [&](auto kernel, size_t smem) -> gprtcuStatus {
           GPRTCU_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-          kernel<<<(unsigned)a.tiles, C8::THREADS, smem, stream>>>(a, p, shift, bits);
+          SortArgs b = a;
+          b.pf_tiles = (uint32_t)((uint64_t)gprtcu_sort_prefetch() * a.sms * C8::MIN_CTAS / 4);
+          kernel<<<(unsigned)a.tiles, C8::THREADS, smem, stream>>>(b, p, shift, bits);
           GPRTCU_TRY(cudaGetLastError());
           return GPRTCU_OK;
         };

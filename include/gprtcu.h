@@ -483,6 +483,12 @@ GPRTCU_API void gprtcuDebugSortSkipTile(int64_t tile);
  * match.any, eight plain votes, eight predicated votes.  All give the same
  * bits. */
 GPRTCU_API void gprtcuDebugSortRanking(int mode);
+/* L2 prefetch distance of the 8-bit sort passes, in quarters of a resident
+ * wave of CTAs (SMs x CTAs per SM): each CTA fetches into L2 the keys and
+ * payloads of the tile that many tickets after its own.  Default 2; 0
+ * turns it off; clamped to 0..64.  A cache hint only: results are the same
+ * bits. */
+GPRTCU_API void gprtcuDebugSortPrefetch(int quarterWaves);
 GPRTCU_API gprtcuStatus gprtcuDebugRefitSkipLeaf(int64_t slot);
 /* Scan kernel selection for tests: 0 = automatic (default: the persistent
  * re-read kernel for n >= 2^20 and the TMA-staged tile-per-CTA kernel below,
