@@ -34,7 +34,9 @@ The JSON line's value is whole-job Mrays/s of that step.  It also carries:
                 timed region, pipelined over 16 runs of meshes on three streams
                 (copies in, build + collapse + trace, copies out); the serial
                 version (copy all, replay the graph, copy back) is reported
-                beside it
+                beside it; h2d_roofline: the bytes copied in per step over
+                the step's time against one pinned copy of the rays timed
+                alone
   gpu_launches  this library's kernels in the timed region, counted from the
                 captured graph's kernel nodes
   small_lbvh    plain LBVH build + trace, 262,144 triangles, 1,048,576 rays
@@ -614,6 +616,13 @@ def run_b200(args, world, rank, local):
     e2e_ok = bool(torch.equal(hits_p, sc.h_q.cpu())) and serial_ok
     h2d = sum(host[k][0].numel() * host[k][0].element_size() for k in ("pos", "tri", "rays")) + \
         sum(ho[0].numel() * 4 + ho[1].numel() * 4 for *_, ho in sc.e2e_runs)
+    # the host-to-device link alone, the bound of the e2e step: one pinned
+    # copy of the rays (the step's largest input) timed by itself
+    hr, dr = host["rays"]
+    link_ms = slowest(float(np.median(workloads.time_steps(lambda: dr.copy_(hr, non_blocking=True), 3, 1))))
+    link_bytes = hr.numel() * hr.element_size()
+    link_gbs = link_bytes / (link_ms * 1e-3) / 1e9
+    del hr, dr
     nrays, ntri, meshes = sc.nrays, sc.n, sc.meshes
     del host, hits_p, g
     sc.release()
@@ -726,6 +735,10 @@ def run_b200(args, world, rank, local):
             "t_check": tchk,
             "e2e": {"value": e2e_v, "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "ms_per_step": e2e_ms, "hits_match_device": e2e_ok,
+                    "h2d_roofline": {"achieved_gbs": h2d / (e2e_ms * 1e-3) / 1e9, "link_gbs": link_gbs,
+                                     "frac": h2d / (e2e_ms * 1e-3) / 1e9 / link_gbs,
+                                     "link": "one pinned host-to-device copy of the %.2f GB of rays, timed alone"
+                                             % (link_bytes / 1e9)},
                     "pipeline": "16 runs of meshes; host-to-device copies, build + collapse + trace and the hits' "
                                 "copy back overlap on three streams",
                     "serial_ms_per_step": serial_ms},
