@@ -240,6 +240,33 @@ def test_sort_rankings_agree(cuda, kw, vw):
         L.gprtcuDebugSortRanking(0)
 
 
+@pytest.mark.parametrize("kw,vw", [(4, 4), (4, 0), (8, 4)])
+def test_sort_l2_prefetch_distances_agree(cuda, kw, vw):
+    # the 8-bit passes prefetch a later tile into L2 (a cache hint); every
+    # distance, none included, must give the oracle's bits
+    import torch
+    import gprt_b200
+    from gprt_b200 import api
+    L = gprt_b200.lib()
+    rng = np.random.default_rng(7 * kw + vw)
+    kdt = np.uint32 if kw == 4 else np.uint64
+    n = (1 << 22) + 5
+    k = _zipf_u32(rng, n).astype(kdt) if kw == 4 else rng.integers(0, 2 ** 44, size=n, dtype=np.uint64)
+    v = rng.integers(0, 2 ** 32, size=n, dtype=np.uint64).astype(np.uint32) if vw else None
+    ek, ev = oracle.sort(k, v) if vw else (oracle.sort(k), None)
+    try:
+        for q in (0, 1, 2, 4, 64):
+            L.gprtcuDebugSortPrefetch(q)
+            kt = torch.from_numpy(k.view(np.int32 if kw == 4 else np.int64).copy()).cuda()
+            vt = torch.from_numpy(v.view(np.int32).copy()).cuda() if vw else None
+            api.sort(kt, vt, 0, 32 if kw == 4 else 44)
+            assert np.array_equal(kt.cpu().numpy().view(kdt), ek), q
+            if vw:
+                assert np.array_equal(vt.cpu().numpy().view(np.uint32), ev), q
+    finally:
+        L.gprtcuDebugSortPrefetch(2)
+
+
 def test_sort_beyond_2_30_keys(cuda):
     # n past 2^30 - 1 needs the wide look-back words; checked through
     # size-independent properties: keys ascending, the payload (original
